@@ -1,0 +1,211 @@
+/*
+ * mpgcr.h — C ABI of the B200 implementation of the two hot loops of the edge-based
+ * anelastic solver `lippsLFroude_implgwopks3D_unstr3.f` (the reference):
+ *
+ *   * MPDATA advection      : mpdatamper            (ref.f:3617-3941) + derivative (ref.f:3943-4022)
+ *   * GCR(k) pressure solve : gcrk (ref.f:1776-1972), precon (ref.f:482-753), laplc (ref.f:1288-1353),
+ *                             prfr (ref.f:1536-1580), div (ref.f:2096-2170), bcv (ref.f:1583-1643)
+ *
+ * and of the node loops of the time-step driver `mpsolver` (ref.f:58-479) that sit between them,
+ * so that every field stays resident on the GPU for a whole run.
+ *
+ * Conventions (they follow the Fortran caller, see the Fortran interface block in INTEGRATION.md):
+ *   * REAL is double (the reference compiled with -fdefault-real-8 -fdefault-double-8).
+ *   * INTEGER is int32; node/edge indices in mesh arrays are 1-based, as in the COMMON blocks.
+ *   * 2-D Fortran arrays arrive as base pointers with their leading dimension (npoinx, nedgex,
+ *     nfacesx): element (i, j) of `sn(nedgex,3)` is sn[(j-1)*nedgex + (i-1)].
+ *   * Every entry point returns an int status: MPG_OK or an MPG_ERR_* code; mpg_last_error()
+ *     gives a one-line message for the calling thread.  Nothing here calls exit() or stop.
+ *   * The reference keeps fields in COMMON blocks and mpsolver locals.  Here they live in a
+ *     handle on one GPU and are named by field ids (MPG_F_*); the subroutine entry points take
+ *     field ids where the reference takes arrays (same argument order and meaning).
+ *   * A handle is not re-entrant (neither is the reference): one thread drives one handle.
+ */
+#ifndef MPGCR_H
+#define MPGCR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+#define MPG_OK              0
+#define MPG_ERR_ARG         1   /* bad argument (null pointer, unknown field id, bad size) */
+#define MPG_ERR_CUDA        2   /* a CUDA call failed                                       */
+#define MPG_ERR_MESH        3   /* mesh is not a prism-column mesh, or uses an unsupported feature */
+#define MPG_ERR_NOMEM       4   /* device allocation failed                                 */
+#define MPG_ERR_UNSUPPORTED 5   /* option the implementation does not provide               */
+#define MPG_ERR_NUMERIC     6   /* NaN/Inf met in a solver reduction                        */
+
+/* GCR exit status (mpg_gcr_stats.status).  The reference leaves gcrk silently in every case
+ * (ref.f:1895-1896); the status makes the reason visible. */
+#define MPG_GCR_CONVERGED   0   /* max|r| <= eps0/dt after >= itmn restart cycles (ref.f:1895)   */
+#define MPG_GCR_STALLED     1   /* ||r||_2^2 did not decrease (ref.f:1896)                      */
+#define MPG_GCR_MAXIT       2   /* itr restart cycles done without convergence                  */
+#define MPG_GCR_NAN         3   /* NaN/Inf in the residual                                      */
+#define MPG_GCR_FALLBACK    4   /* learned preconditioner rejected, solve redone with the plain one */
+
+/* ---------------------------------------------------------------- run parameters */
+/* One struct for the three configuration layers of the reference: inputinc.d
+ * (ref.f:2293-2321), input_mg_v3.d (ref.f:2265-2276) and the constants hard-coded in
+ * mpsolver (ref.f:108-138).  Fields keep the reference names. */
+typedef struct mpg_params {
+    /* inputinc.d */
+    int32_t ntime, istst, isfera, iper;
+    double  cfl, delt;
+    double  p0inf, u0inf, v0inf, w0inf;
+    int32_t ielast;
+    double  eps0;
+    int32_t itr, lord;           /* lord: GCR order (a compile-time 9 in the reference, ref.f:1782) */
+    int32_t irl;                 /* absorbers on/off */
+    double  dxabl, dxabr, dyabd, dyabu, dzabd, dzabu;
+    double  towxl, towxr, towyd, towyu, towzd, towzu;
+    /* input_mg_v3.d */
+    int32_t mg_flag, sm_flag1;
+    double  omega;
+    int32_t itrp1, itrp2;
+    /* mpsolver constants */
+    int32_t implgw, lipps;
+    double  strat, tetbar, g;
+    /* extensions of this implementation */
+    int32_t iprc;                /* 0 identity, 1 reference smoother (ref.f:587-612), 2 vertical line */
+    int32_t nscal;               /* passive scalars advected after unk(:,1..4)                      */
+    int32_t precision;           /* MPG_PREC_FP64 or MPG_PREC_MIXED                                 */
+    int32_t itmn;                /* minimum restart cycles before the convergence test (3, ref.f:1809) */
+} mpg_params;
+
+#define MPG_PREC_FP64  0
+#define MPG_PREC_MIXED 1
+
+/* ---------------------------------------------------------------- mesh (reference COMMON layout) */
+/* /n/ npoin,nedge,nbface,nbpoin,nboun; /xyz/ coord; /volume/ vol; /edg/ iedge; /wge/ sn;
+ * /bound/ kbface,sb; /bpoints/ ibpoin,anp; /terms/ sbb; /coin/ /per2/ /per4/ periodic lists
+ * (ref.f:2182-2196, read at ref.f:2437-2501, ref.f:2562-2576). */
+typedef struct mpg_mesh_ref {
+    int32_t npoin, nedge, nbface, nboun;
+    int32_t npoinx, nedgex, nfacesx;   /* leading dimensions of the arrays below */
+    const double  *coord;              /* coord(npoinx,3)  */
+    const double  *vol;                /* vol(npoinx)      */
+    const int32_t *iedge;              /* iedge(nedgex,2)  */
+    const double  *sn;                 /* sn(nedgex,3)     */
+    const int32_t *kbface;             /* kbface(nfacesx,2) (may be NULL when nbface == 0) */
+    const double  *sb;                 /* sb(nfacesx,3)    */
+    const int32_t *ibpoin;             /* ibpoin(nfacesx,2): node, boundary type */
+    const double  *sbb;                /* sbb(nfacesx,3)   */
+    const double  *anp;                /* anp(nfacesx,3)   */
+    int32_t ncoin, ncoin2, ncoin4;
+    int32_t ldcoin;                    /* leading dimension of icoin (nfacesx*2 in the reference) */
+    const int32_t *icoin;              /* icoin(ldcoin,2)  */
+    const int32_t *icoin2;             /* icoin2(nfacesx,2) */
+    const int32_t *icoin4;             /* icoin4(nfacesx,4) */
+} mpg_mesh_ref;
+
+/* ---------------------------------------------------------------- outputs */
+typedef struct mpg_gcr_stats {         /* /itero/ (ref.f:1953-1963) plus the exit reason */
+    int32_t niter, nitsm, icount, status;
+    double  eer, eem;
+    double  dvmx;                      /* final max|r| (units of rhs, 1/s)       */
+    double  rl2;                       /* final sum r^2                          */
+    int32_t fallbacks;                 /* learned-preconditioner fallbacks taken */
+    int32_t pad;
+} mpg_gcr_stats;
+
+typedef struct mpg_diag {              /* per-step diagnostics printed by mpsolver (ref.f:456-459) */
+    double divmx, divmn, divav, divsd; /* div(...,1)        ref.f:2148-2168 */
+    double crnmx, crnmn, crnav, crnsd; /* courant(...,1)    ref.f:2076-2092 */
+    int32_t icrnmx, niter, nitav, pad; /* node of max Courant (1-based), solver stats */
+    double eer, eem;
+    double stats[16];                  /* umx,umn,uav,usd, vmx.., wmx.., tmx,tmn,tav,tsd (ref.f:2904) */
+    double mass[8];                    /* sum(vol*rh0*unk(:,k)) for the prognostic fields (FP64)  */
+    double smin[4], smax[4];           /* min/max of the first passive scalars                     */
+} mpg_diag;
+
+typedef struct mpg_info {
+    int64_t npoin, nedge, ncol, nedge2d;
+    int32_t nlev, precision;
+    int64_t device_bytes;              /* bytes allocated on the device by the handle */
+} mpg_info;
+
+/* ---------------------------------------------------------------- field ids */
+enum {
+    MPG_F_UNK    = 0,    /* unk(:,1..4+nscal) : MPG_F_UNK + k-1   (u, v, w, theta', scalars)   */
+    MPG_F_UNK1   = 16,   /* unk1(:,1..4)                                                        */
+    MPG_F_UUU    = 20,   /* uuu(:,1..3)   momentum / velocity                                   */
+    MPG_F_UUU0   = 23,   /* uuu0(:,1..3)                                                        */
+    MPG_F_FRC    = 26,   /* frc(:,1..4)                                                         */
+    MPG_F_UNKDASH= 30,   /* unkdash(:,1..3)                                                     */
+    MPG_F_PRPOT  = 33,
+    MPG_F_RHS    = 34,
+    MPG_F_COUR   = 35,
+    MPG_F_ALPHA  = 36,
+    MPG_F_COEFW  = 37,
+    MPG_F_RH0    = 38,
+    MPG_F_TH0    = 39,
+    MPG_F_THE    = 40,
+    MPG_F_DTHEDZ = 41,
+    MPG_F_D1     = 42,   /* /doperator/ d1 (compute_d_unstr)                                   */
+    MPG_F_WORK   = 48,   /* 8 caller-usable work arrays MPG_F_WORK + 0..7                       */
+    MPG_F_COUNT  = 56
+};
+
+typedef struct mpg_solver *mpg_handle;
+
+/* ---------------------------------------------------------------- lifecycle */
+/* Uploads the mesh once, detects the prism-column structure (columns of equal (x,y), the same
+ * number of levels everywhere, horizontal edges between equal levels), packs it column-major
+ * (level fastest) and allocates every field on `device`.  Replaces the mesh part of `input`
+ * (ref.f:2343-2641) and the static COMMON storage. */
+int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int device, mpg_handle *out);
+int mpg_destroy(mpg_handle h);
+const char *mpg_last_error(void);
+int mpg_get_info(mpg_handle h, mpg_info *info);
+
+/* Field exchange in reference node order: `n` = npoin values, contiguous. */
+int mpg_set_field(mpg_handle h, int fid, const double *src);
+int mpg_get_field(mpg_handle h, int fid, double *dst);
+
+/* ---------------------------------------------------------------- reference subroutines */
+/* derivative(unk, dpdxa, idx)                          ref.f:3943-4022 */
+int mpg_derivative(mpg_handle h, int unk, int out, int idx);
+/* bcv(u, v, w, flag)                                    ref.f:1583-1643 */
+int mpg_bcv(mpg_handle h, int u, int v, int w, double flag);
+/* laplc(press, alap, impfl)                             ref.f:1288-1353 */
+int mpg_laplc(mpg_handle h, int press, int alap, int impfl);
+/* prfr(press, ustr, vstr, wstr, uout, vout, wout, impfl) ref.f:1536-1580 */
+int mpg_prfr(mpg_handle h, int press, int ustr, int vstr, int wstr,
+             int uout, int vout, int wout, int impfl);
+/* div(ua, va, wa, rhs, iflg)                            ref.f:2096-2170; diag may be NULL */
+int mpg_div(mpg_handle h, int ua, int va, int wa, int rhs, int iflg, mpg_diag *diag);
+/* precon(rhs, p, r, iprc, elas, impfl)                  ref.f:482-753 (mg_flag=0) + line option */
+int mpg_precon(mpg_handle h, int rhs, int p, int r, int iprc, int impfl);
+/* gcrk(p, u1, v1, w1, u2, v2, w2, impfl)                ref.f:1776-1972 */
+int mpg_gcrk(mpg_handle h, int p, int u1, int v1, int w1, int u2, int v2, int w2,
+             int impfl, mpg_gcr_stats *stats);
+/* mpdatamper(uuu, unk(1,iflag), iflag)                  ref.f:3617-3941 (uuu = MPG_F_UUU) */
+int mpg_mpdatamper(mpg_handle h, int unk, int iflag);
+/* courant(uuu, cour, iflag) and stats(unk)              ref.f:1974-2094, ref.f:2847-2912 */
+int mpg_courant(mpg_handle h, int iflag, mpg_diag *diag);
+int mpg_stats(mpg_handle h, mpg_diag *diag);
+
+/* ---------------------------------------------------------------- mpsolver */
+/* Set-up part of mpsolver (ref.f:99-273): profiles, absorbers, metric, beta/d, ambient state,
+ * potential-flow solve, coefw, momentum and the initial diagnostics. */
+int mpg_setup(mpg_handle h, mpg_diag *diag);
+/* One pass of the DO ITIME loop (ref.f:285-463). */
+int mpg_step(mpg_handle h, mpg_diag *diag);
+/* The node loops of one pass, for a host that drives the subroutines itself. */
+int mpg_half_forcing(mpg_handle h);                 /* ref.f:290-301 */
+int mpg_explicit_forcing(mpg_handle h, int mtri);   /* ref.f:323-359 */
+int mpg_post_solve(mpg_handle h, int mtri);         /* ref.f:367-383 */
+int mpg_extrapolate(mpg_handle h);                  /* ref.f:387-439 */
+/* Last GCR statistics of the handle (/itero/). */
+int mpg_get_gcr_stats(mpg_handle h, mpg_gcr_stats *stats);
+/* Wait for all work of the handle. */
+int mpg_synchronize(mpg_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPGCR_H */

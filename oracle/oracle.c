@@ -1,0 +1,1102 @@
+/*
+ * TEST INFRASTRUCTURE — NOT PART OF THE PRODUCT.  See oracle.h.
+ *
+ * Line-by-line FP64 restatement of the hot path of lippsLFroude_implgwopks3D_unstr3.f
+ * (cited as ref.f:<line>).  Every loop keeps the reference's iteration order and every
+ * expression keeps the reference's association (Fortran evaluates left to right), so the
+ * product can be compared with it bit for bit where its own order allows.  Build with
+ * -O2 -ffp-contract=off (no FMA contraction, no fast-math).
+ *
+ * Reference options restated: isfera=0 only (the spherical variant is out of scope),
+ * iper=0 or 2, mg_flag=0, ielast=0, itraj=0.  Extensions beyond the reference are marked
+ * NEW: the vertical-line preconditioner (iprc=2), runtime lord/itmn, passive scalars and
+ * the FP64 mass sums.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define AMAX(a, b) ((a) > (b) ? (a) : (b))
+#define AMIN(a, b) ((a) < (b) ? (a) : (b))
+#define MAXUNK 16
+
+struct orc {
+    mpg_params P;
+    int npoin, nedge, nbface, nboun, ncoin, ncoin2, ncoin4;
+    double *x, *y, *z, *vol;
+    int *ie1, *ie2;
+    double *snx, *sny, *snz;
+    int *kb1, *kb2;
+    double *sbx, *sby, *sbz;
+    int *ibn, *ibt;
+    double *sbbx, *sbby, *sbbz, *anx, *any, *anz;
+    int *ic1, *ic2, *ic2a, *ic2b, *ic4[4];
+    /* COMMON state */
+    double *timestp, *cosa, *gmm, *ue, *ve, *d1;
+    double betaunstr1;
+    double rgas, cp, cap;
+    /* fields addressed by id */
+    double *f[MPG_F_COUNT];
+    /* /itero/ */
+    int niter, nitsm, icount, gstatus;
+    double eer, eem, dvmx_last, rl2_last;
+    /* vertical structure (NEW line preconditioner) */
+    int *up, *dn, *colstart, ncol;
+    int *colnodes;
+    int nvert_e;
+    int *vedge;         /* vertical edges: index into the combined edge list */
+};
+
+/* ------------------------------------------------------------------ helpers */
+static double *dz(int n) { return (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }
+static int *iz(int n) { return (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int)); }
+
+int orc_npoin(const orc *o) { return o->npoin; }
+double *orc_field(orc *o, int fid) { return (fid >= 0 && fid < MPG_F_COUNT) ? o->f[fid] : NULL; }
+double orc_beta(orc *o) { return o->betaunstr1; }
+
+/* cyclicr, cyclicr2, cyclicr4 — ref.f:4377-4446 */
+static void cyclicr(orc *o, double *u) {
+    if (!o->ncoin) return;
+    double *uc = dz(o->ncoin);
+    for (int c = 0; c < o->ncoin; ++c) uc[c] = u[o->ic1[c]] + u[o->ic2[c]];
+    for (int c = 0; c < o->ncoin; ++c) { u[o->ic1[c]] = uc[c]; u[o->ic2[c]] = uc[c]; }
+    free(uc);
+}
+static void cyclicr2(orc *o, double *u) {
+    if (!o->ncoin2) return;
+    double *uc = dz(o->ncoin2);
+    for (int c = 0; c < o->ncoin2; ++c) uc[c] = u[o->ic2a[c]] + u[o->ic2b[c]];
+    for (int c = 0; c < o->ncoin2; ++c) { u[o->ic2a[c]] = uc[c]; u[o->ic2b[c]] = uc[c]; }
+    free(uc);
+}
+static void cyclicr4(orc *o, double *u) {
+    if (!o->ncoin4) return;
+    double *uc = dz(o->ncoin4);
+    for (int c = 0; c < o->ncoin4; ++c)
+        uc[c] = u[o->ic4[0][c]] + u[o->ic4[1][c]] + u[o->ic4[2][c]] + u[o->ic4[3][c]];
+    for (int c = 0; c < o->ncoin4; ++c)
+        for (int j = 0; j < 4; ++j) u[o->ic4[j][c]] = uc[c];
+    free(uc);
+}
+
+/* ------------------------------------------------------------------ derivative ref.f:3943-4022 */
+void orc_derivative(orc *o, const double *unk, double *out, int idx) {
+    const double *s = idx == 1 ? o->snx : idx == 2 ? o->sny : o->snz;
+    const double *sb = idx == 1 ? o->sbx : idx == 2 ? o->sby : o->sbz;
+    const double *sbb = idx == 1 ? o->sbbx : idx == 2 ? o->sbby : o->sbbz;
+    for (int ip = 0; ip < o->npoin; ++ip) out[ip] = 0.;
+    for (int e = 0; e < o->nedge; ++e) {                       /* ref.f:3967-3974 */
+        int i1 = o->ie1[e], i2 = o->ie2[e];
+        double sx = s[e];
+        double u = (unk[i1] + unk[i2]) * 0.5;
+        out[i1] = out[i1] + sx * u;
+        out[i2] = out[i2] - sx * u;
+    }
+    for (int e = 0; e < o->nbface; ++e) {                      /* ref.f:3975-3985 */
+        int i1 = o->kb1[e], i2 = o->kb2[e];
+        double sx = sb[e];
+        double u = (unk[i1] + unk[i2]) * 0.5;
+        out[i1] = out[i1] + sx * u;
+        out[i2] = out[i2] - sx * u;
+    }
+    if (o->P.isfera == 0 && o->P.iper == 0) {                  /* ref.f:4007-4014 */
+        for (int b = 0; b < o->nboun; ++b) {
+            int i1 = o->ibn[b];
+            double sx = sbb[b];
+            double u = unk[i1];
+            out[i1] = out[i1] + sx * u;
+        }
+    }
+    if (o->P.iper == 2) {                                      /* ref.f:4015-4019 */
+        cyclicr(o, out);
+        cyclicr2(o, out);
+        cyclicr4(o, out);
+    }
+}
+
+/* ------------------------------------------------------------------ bcv ref.f:1583-1643 */
+void orc_bcv(orc *o, double *u, double *v, double *w, double flag) {
+    int per = (o->P.isfera == 1 || o->P.iper == 2);
+    for (int b = 0; b < o->nboun; ++b) {
+        int ii = o->ibn[b], t = o->ibt[b];
+        double a1 = o->anx[b], a2 = o->any[b], a3 = o->anz[b];
+        if (t == 11 || (!per && (t == 5 || t == 6))) {
+            double vn = u[ii] * a1 + v[ii] * a2 + w[ii] * a3;
+            u[ii] = u[ii] - a1 * vn;
+            v[ii] = v[ii] - a2 * vn;
+            w[ii] = w[ii] - a3 * vn;
+        }
+        if (!per && (t == 7 || t == 8)) u[ii] = o->ue[ii] * flag;
+    }
+}
+
+/* ------------------------------------------------------------------ laplc ref.f:1288-1353 */
+void orc_laplc(orc *o, const double *press, double *alap, int impfl) {
+    int n = o->npoin;
+    double *dx = dz(n), *dy = dz(n), *dzz = dz(n);
+    const double *rh0 = o->f[MPG_F_RH0], *coefw = o->f[MPG_F_COEFW];
+    for (int ip = 0; ip < n; ++ip) alap[ip] = 0.;
+    orc_derivative(o, press, dx, 1);
+    orc_derivative(o, press, dy, 2);
+    orc_derivative(o, press, dzz, 3);
+    for (int ip = 0; ip < n; ++ip) {
+        double gc = o->gmm[ip] * o->cosa[ip];
+        dx[ip] = o->timestp[ip] * dx[ip] / o->vol[ip];
+        dy[ip] = o->timestp[ip] * dy[ip] / o->vol[ip];
+        dzz[ip] = o->timestp[ip] * dzz[ip] / o->vol[ip];
+        dx[ip] = 0.5 * dx[ip] / (gc * gc);
+        dy[ip] = 0.5 * dy[ip] / (o->gmm[ip] * o->gmm[ip]);
+        dzz[ip] = 0.5 * dzz[ip] * (coefw[ip] * (double)impfl + (double)(1 - impfl));
+    }
+    orc_bcv(o, dx, dy, dzz, 0.);
+    for (int ip = 0; ip < n; ++ip) {
+        dx[ip] = dx[ip] * rh0[ip];
+        dy[ip] = dy[ip] * rh0[ip];
+        dzz[ip] = dzz[ip] * rh0[ip];
+    }
+    orc_derivative(o, dx, alap, 1);
+    {
+        double *t = dz(n);
+        orc_derivative(o, dy, t, 2);      /* derivative(dpdyb, dpdxb, 2) */
+        memcpy(dx, t, sizeof(double) * n);
+        orc_derivative(o, dzz, t, 3);     /* derivative(dpdzb, dpdyb, 3) */
+        memcpy(dy, t, sizeof(double) * n);
+        free(t);
+    }
+    for (int ip = 0; ip < n; ++ip)
+        alap[ip] = (alap[ip] + dx[ip] + dy[ip]) / (o->vol[ip] * rh0[ip]);
+    free(dx); free(dy); free(dzz);
+}
+
+/* ------------------------------------------------------------------ prfr ref.f:1536-1580 */
+void orc_prfr(orc *o, const double *press, const double *ustr, const double *vstr,
+              const double *wstr, double *uout, double *vout, double *wout, int impfl) {
+    int n = o->npoin;
+    double *dx = dz(n), *dy = dz(n), *dzz = dz(n);
+    const double *coefw = o->f[MPG_F_COEFW];
+    orc_derivative(o, press, dx, 1);
+    orc_derivative(o, press, dy, 2);
+    orc_derivative(o, press, dzz, 3);
+    for (int ip = 0; ip < n; ++ip) {
+        double gc = o->gmm[ip] * o->cosa[ip];
+        dx[ip] = dx[ip] / (gc * gc) / o->vol[ip];
+        dy[ip] = dy[ip] / (o->gmm[ip] * o->gmm[ip]) / o->vol[ip];
+        dzz[ip] = dzz[ip] / o->vol[ip];
+    }
+    for (int ip = 0; ip < n; ++ip) {
+        uout[ip] = ustr[ip] - 0.5 * o->timestp[ip] * dx[ip];
+        vout[ip] = vstr[ip] - 0.5 * o->timestp[ip] * dy[ip];
+        wout[ip] = wstr[ip] - 0.5 * o->timestp[ip] * dzz[ip]
+                   * (coefw[ip] * (double)impfl + (double)(1 - impfl));
+    }
+    orc_bcv(o, uout, vout, wout, 1.);
+    free(dx); free(dy); free(dzz);
+}
+
+/* ------------------------------------------------------------------ div ref.f:2096-2170 */
+void orc_div(orc *o, const double *ua, const double *va, const double *wa, double *rhs,
+             int iflg, mpg_diag *diag) {
+    int n = o->npoin;
+    const double *rh0 = o->f[MPG_F_RH0];
+    double *ub = dz(n), *vb = dz(n), *wb = dz(n);
+    double *dudx = dz(n), *dvdy = dz(n), *dwdz = dz(n);
+    for (int ip = 0; ip < n; ++ip) {
+        if (iflg == -1) {
+            ub[ip] = ua[ip] * rh0[ip]; vb[ip] = va[ip] * rh0[ip]; wb[ip] = wa[ip] * rh0[ip];
+        } else {
+            ub[ip] = ua[ip]; vb[ip] = va[ip]; wb[ip] = wa[ip];
+        }
+    }
+    orc_derivative(o, ub, dudx, 1);
+    orc_derivative(o, vb, dvdy, 2);
+    orc_derivative(o, wb, dwdz, 3);
+    for (int ip = 0; ip < n; ++ip)
+        rhs[ip] = (double)iflg * (dudx[ip] / o->vol[ip] + dvdy[ip] / o->vol[ip]
+                                  + dwdz[ip] / o->vol[ip]) / rh0[ip];
+    if (iflg == 1 && diag) {
+        double divmx = -1.e15, divmn = 1.e15, divav = 0.;
+        for (int ip = 0; ip < n; ++ip) {
+            divmx = AMAX(divmx, rhs[ip] * o->timestp[ip]);
+            divmn = AMIN(divmn, rhs[ip] * o->timestp[ip]);
+            divav = divav + rhs[ip] * o->timestp[ip];
+        }
+        divav = divav / (double)n;
+        double divsd = 0.;
+        for (int ip = 0; ip < n; ++ip) {
+            double t = rhs[ip] * o->timestp[ip] - divav;
+            divsd = divsd + t * t;
+        }
+        divsd = sqrt(divsd / n);
+        diag->divmx = divmx; diag->divmn = divmn; diag->divav = divav; diag->divsd = divsd;
+        diag->eer = o->eer; diag->eem = o->eem; diag->niter = o->niter;
+        diag->nitav = o->nitsm / (o->icount > 1 ? o->icount : 1);
+    }
+    free(ub); free(vb); free(wb); free(dudx); free(dvdy); free(dwdz);
+}
+
+/* ------------------------------------------------------------------ NEW: vertical-line preconditioner
+ * Per column, a compact tridiagonal M approximates the vertical part of laplc; its diagonal
+ * also carries the diagonal of the horizontal part (the compute_d_unstr sum, ref.f:1213-1271,
+ * restricted to non-vertical edges).  Vertical edge e from a (below) to b (above) with
+ * face vector S (oriented upward):
+ *     T_e = ((0.5*dt) * ((sx*sx + sy*sy) + (sz*sz)*cwf)) * rhof / volf
+ *     rhof = 0.5*(rh0_a+rh0_b), volf = 0.5*(vol_a+vol_b), cwf = 0.5*(cw_a+cw_b),
+ *     cw = coefw*impfl + (1-impfl)
+ * Row i:  a_i = (sum of T below)/(vol_i*rh0_i),  c_i = (sum of T above)/(vol_i*rh0_i),
+ *         Dh_i = -((0.5*dt)*((dhx+dhy)+dhz)) / ((4*vol_i)*rh0_i)   (non-vertical edges),
+ *         b_i = (Dh_i - a_i) - c_i.
+ * Thomas from the bottom: m_0=b_0, cp_k=c_k/m_k, m_k=b_k-a_k*cp_{k-1};
+ *     d_k=(r_k-a_k*d_{k-1})/m_k;  z_top=d_top;  z_k=d_k-cp_k*z_{k+1}.            */
+static int is_vertical(orc *o, int i1, int i2) {
+    return o->x[i1] == o->x[i2] && o->y[i1] == o->y[i2];
+}
+
+static void line_structure(orc *o) {
+    if (o->up) return;
+    int n = o->npoin;
+    o->up = iz(n); o->dn = iz(n);
+    for (int i = 0; i < n; ++i) { o->up[i] = -1; o->dn[i] = -1; }
+    for (int e = 0; e < o->nedge + o->nbface; ++e) {
+        int i1 = e < o->nedge ? o->ie1[e] : o->kb1[e - o->nedge];
+        int i2 = e < o->nedge ? o->ie2[e] : o->kb2[e - o->nedge];
+        if (!is_vertical(o, i1, i2)) continue;
+        int lo = o->z[i1] < o->z[i2] ? i1 : i2, hi = lo == i1 ? i2 : i1;
+        o->up[lo] = hi;
+        o->dn[hi] = lo;
+    }
+    o->colnodes = iz(n);
+    o->colstart = iz(n + 1);
+    int pos = 0, nc = 0;
+    for (int i = 0; i < n; ++i) {
+        if (o->dn[i] != -1) continue;
+        o->colstart[nc++] = pos;
+        for (int j = i; j != -1; j = o->up[j]) o->colnodes[pos++] = j;
+    }
+    o->colstart[nc] = pos;
+    o->ncol = nc;
+}
+
+static void line_coeffs(orc *o, int impfl, double *a, double *m, double *cp) {
+    int n = o->npoin;
+    const double *rh0 = o->f[MPG_F_RH0], *coefw = o->f[MPG_F_COEFW];
+    double dt = o->timestp[0];
+    double *Ta = dz(n), *Tc = dz(n), *hx = dz(n), *hy = dz(n), *hz = dz(n);
+    line_structure(o);
+    for (int e = 0; e < o->nedge + o->nbface; ++e) {
+        int in = e < o->nedge;
+        int i1 = in ? o->ie1[e] : o->kb1[e - o->nedge];
+        int i2 = in ? o->ie2[e] : o->kb2[e - o->nedge];
+        double sx = in ? o->snx[e] : o->sbx[e - o->nedge];
+        double sy = in ? o->sny[e] : o->sby[e - o->nedge];
+        double sz = in ? o->snz[e] : o->sbz[e - o->nedge];
+        if (is_vertical(o, i1, i2)) {
+            int lo = o->z[i1] < o->z[i2] ? i1 : i2, hi = lo == i1 ? i2 : i1;
+            if (lo != i1) { sx = -sx; sy = -sy; sz = -sz; }
+            double cwa = coefw[lo] * (double)impfl + (double)(1 - impfl);
+            double cwb = coefw[hi] * (double)impfl + (double)(1 - impfl);
+            double cwf = 0.5 * (cwa + cwb);
+            double rhof = 0.5 * (rh0[lo] + rh0[hi]);
+            double volf = 0.5 * (o->vol[lo] + o->vol[hi]);
+            double T = (0.5 * dt) * ((sx * sx + sy * sy) + (sz * sz) * cwf) * rhof / volf;
+            Tc[lo] = Tc[lo] + T;
+            Ta[hi] = Ta[hi] + T;
+        } else {
+            hx[i1] = hx[i1] + sx * sx * rh0[i2] / o->vol[i2];
+            hx[i2] = hx[i2] + sx * sx * rh0[i1] / o->vol[i1];
+            hy[i1] = hy[i1] + sy * sy * rh0[i2] / o->vol[i2];
+            hy[i2] = hy[i2] + sy * sy * rh0[i1] / o->vol[i1];
+            hz[i1] = hz[i1] + sz * sz * rh0[i2] / o->vol[i2];
+            hz[i2] = hz[i2] + sz * sz * rh0[i1] / o->vol[i1];
+        }
+    }
+    double *b = dz(n), *c = dz(n);
+    for (int i = 0; i < n; ++i) {
+        double vr = o->vol[i] * rh0[i];
+        double dh = -((0.5 * dt) * ((hx[i] + hy[i]) + hz[i])) / ((4. * o->vol[i]) * rh0[i]);
+        a[i] = Ta[i] / vr;
+        c[i] = Tc[i] / vr;
+        b[i] = (dh - a[i]) - c[i];
+    }
+    for (int col = 0; col < o->ncol; ++col) {
+        int s = o->colstart[col], t = o->colstart[col + 1];
+        for (int k = s; k < t; ++k) {
+            int i = o->colnodes[k];
+            if (k == s) m[i] = b[i];
+            else m[i] = b[i] - a[i] * cp[o->colnodes[k - 1]];
+            cp[i] = c[i] / m[i];
+        }
+    }
+    free(Ta); free(Tc); free(hx); free(hy); free(hz); free(b); free(c);
+}
+
+void orc_line_solve(orc *o, const double *rhs, double *zout, int impfl) {
+    int n = o->npoin;
+    double *a = dz(n), *m = dz(n), *cp = dz(n), *d = dz(n);
+    line_coeffs(o, impfl, a, m, cp);
+    for (int col = 0; col < o->ncol; ++col) {
+        int s = o->colstart[col], t = o->colstart[col + 1];
+        for (int k = s; k < t; ++k) {
+            int i = o->colnodes[k];
+            if (k == s) d[i] = rhs[i] / m[i];
+            else d[i] = (rhs[i] - a[i] * d[o->colnodes[k - 1]]) / m[i];
+        }
+        for (int k = t - 1; k >= s; --k) {
+            int i = o->colnodes[k];
+            if (k == t - 1) zout[i] = d[i];
+            else zout[i] = d[i] - cp[i] * zout[o->colnodes[k + 1]];
+        }
+    }
+    free(a); free(m); free(cp); free(d);
+}
+
+/* ------------------------------------------------------------------ precon ref.f:482-753 (mg_flag=0) */
+void orc_precon(orc *o, const double *rhs, double *p, double *r, int iprc, int impfl) {
+    int n = o->npoin;
+    if (iprc == 0) {                                           /* ref.f:543-548 */
+        for (int ip = 0; ip < n; ++ip) p[ip] = rhs[ip];
+        return;
+    }
+    for (int ip = 0; ip < n; ++ip) { p[ip] = 0.; r[ip] = 0.; }
+    if (iprc == 2) {                                           /* NEW: line relaxation */
+        double *zz = dz(n), *res = dz(n);
+        for (int it = 1; it <= o->P.itrp1; ++it) {
+            if (it == 1) {
+                orc_line_solve(o, rhs, zz, impfl);
+            } else {
+                orc_laplc(o, p, r, impfl);
+                for (int ip = 0; ip < n; ++ip) res[ip] = rhs[ip] - r[ip];
+                orc_line_solve(o, res, zz, impfl);
+            }
+            for (int ip = 0; ip < n; ++ip) p[ip] = p[ip] + o->P.omega * zz[ip];
+        }
+        free(zz); free(res);
+        return;
+    }
+    double *pstep = dz(n);                                     /* ref.f:587-600 */
+    for (int ip = 0; ip < n; ++ip) {
+        if (o->P.sm_flag1 == 1) pstep[ip] = (-1.) / o->d1[ip];
+        else if (o->P.sm_flag1 == 2) pstep[ip] = o->betaunstr1;
+        else if (o->P.sm_flag1 == 3) pstep[ip] = o->betaunstr1 / (1. - o->d1[ip] * o->betaunstr1);
+    }
+    for (int it = 1; it <= o->P.itrp1; ++it) {                 /* ref.f:607-612 */
+        orc_laplc(o, p, r, impfl);
+        for (int ip = 0; ip < n; ++ip)
+            p[ip] = p[ip] + o->P.omega * pstep[ip] * (r[ip] - rhs[ip]);
+    }
+    free(pstep);
+}
+
+/* ------------------------------------------------------------------ gcrk ref.f:1776-1972 */
+void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const double *w1,
+              double *u2, double *v2, double *w2, int impfl, mpg_gcr_stats *st) {
+    int nml = o->npoin, lord = o->P.lord, itmn = o->P.itmn > 0 ? o->P.itmn : 3;
+    double eps = o->P.eps0 / o->timestp[0];
+    double epa = 1.e-38;
+    int nlc = 0, iprc = o->P.iprc;
+    double *r = dz(nml), *qr = dz(nml), *ar = dz(nml);
+    double **x = (double **)calloc(lord, sizeof(double *));
+    double **ax = (double **)calloc(lord, sizeof(double *));
+    double *ax2 = dz(lord), *axar = dz(lord), *del = dz(lord);
+    for (int i = 0; i < lord; ++i) { x[i] = dz(nml); ax[i] = dz(nml); }
+    orc_prfr(o, p, u1, v1, w1, u2, v2, w2, impfl);
+    orc_div(o, u2, v2, w2, r, -1, NULL);
+    orc_precon(o, r, qr, ar, iprc, impfl);
+    double eer0 = 0., eem0 = -1.e15, rl20 = 0.;
+    for (int k = 0; k < nml; ++k) {
+        eer0 = eer0 + qr[k] * qr[k];
+        eem0 = AMAX(eem0, fabs(qr[k]));
+        rl20 = rl20 + r[k] * r[k];
+    }
+    eer0 = AMAX(eer0, epa);
+    eem0 = AMAX(eem0, epa);
+    rl20 = AMAX(rl20, epa);
+    for (int k = 0; k < nml; ++k) x[0][k] = qr[k];
+    orc_laplc(o, x[0], ax[0], impfl);
+    int status = MPG_GCR_MAXIT;
+    double dvmx = 0., rl2 = 0.;
+    for (int it = 1; it <= o->P.itr; ++it) {
+        for (int i = 1; i <= lord; ++i) {
+            double *xi = x[i - 1], *axi = ax[i - 1];
+            double rax = 0.;
+            ax2[i - 1] = 0.;
+            for (int k = 0; k < nml; ++k) {
+                rax = rax + r[k] * axi[k];
+                ax2[i - 1] = ax2[i - 1] + axi[k] * axi[k];
+            }
+            ax2[i - 1] = AMAX(epa, ax2[i - 1]);
+            double beta = -rax / ax2[i - 1];
+            dvmx = -1.e15;
+            rl2 = 0.;
+            for (int k = 0; k < nml; ++k) {
+                p[k] = p[k] + beta * xi[k];
+                r[k] = r[k] + beta * axi[k];
+                dvmx = AMAX(dvmx, fabs(r[k]));
+                rl2 = rl2 + r[k] * r[k];
+            }
+            if (!(dvmx == dvmx) || !(rl2 == rl2)) { status = MPG_GCR_NAN; goto done; }
+            if (dvmx <= eps && it >= itmn) { status = MPG_GCR_CONVERGED; goto done; }
+            if (rl2 >= rl20) { status = MPG_GCR_STALLED; goto done; }
+            rl20 = AMAX(rl2, epa);
+            orc_precon(o, r, qr, ar, iprc, impfl);
+            orc_laplc(o, qr, ar, impfl);
+            nlc = nlc + 1;
+            for (int ii = 1; ii <= i; ++ii) {
+                axar[ii - 1] = 0.;
+                for (int k = 0; k < nml; ++k) axar[ii - 1] = axar[ii - 1] + ax[ii - 1][k] * ar[k];
+                del[ii - 1] = -axar[ii - 1] / ax2[ii - 1];
+            }
+            if (i < lord) {
+                for (int k = 0; k < nml; ++k) { x[i][k] = qr[k]; ax[i][k] = ar[k]; }
+                for (int ii = 1; ii <= i; ++ii)
+                    for (int k = 0; k < nml; ++k) {
+                        x[i][k] = x[i][k] + del[ii - 1] * x[ii - 1][k];
+                        ax[i][k] = ax[i][k] + del[ii - 1] * ax[ii - 1][k];
+                    }
+            } else {
+                for (int k = 0; k < nml; ++k) {
+                    x[0][k] = qr[k] + del[0] * x[0][k];
+                    ax[0][k] = ar[k] + del[0] * ax[0][k];
+                }
+                for (int ii = 2; ii <= i; ++ii)
+                    for (int k = 0; k < nml; ++k) {
+                        x[0][k] = x[0][k] + del[ii - 1] * x[ii - 1][k];
+                        x[ii - 1][k] = 0.;
+                        ax[0][k] = ax[0][k] + del[ii - 1] * ax[ii - 1][k];
+                        ax[ii - 1][k] = 0.;
+                    }
+            }
+        }
+    }
+done:;
+    double eer = 0., eem = -1.e15;                             /* ref.f:1953-1963 */
+    for (int k = 0; k < nml; ++k) {
+        eer = eer + qr[k] * qr[k];
+        eem = AMAX(eem, fabs(qr[k]));
+    }
+    o->eer = eer / eer0;
+    o->eem = eem / eem0;
+    o->niter = nlc;
+    o->nitsm = o->nitsm + o->niter;
+    o->icount = o->icount + 1;
+    o->gstatus = status;
+    o->dvmx_last = dvmx;
+    o->rl2_last = rl2;
+    if (st) orc_get_gcr_stats(o, st);
+    for (int i = 0; i < lord; ++i) { free(x[i]); free(ax[i]); }
+    free(x); free(ax); free(ax2); free(axar); free(del); free(r); free(qr); free(ar);
+}
+
+void orc_get_gcr_stats(orc *o, mpg_gcr_stats *st) {
+    memset(st, 0, sizeof(*st));
+    st->niter = o->niter; st->nitsm = o->nitsm; st->icount = o->icount;
+    st->status = o->gstatus; st->eer = o->eer; st->eem = o->eem;
+    st->dvmx = o->dvmx_last; st->rl2 = o->rl2_last;
+}
+
+/* ------------------------------------------------------------------ mpdatamper ref.f:3617-3941 */
+static double partp(double y) { return AMAX(0., y); }
+static double partn(double y) { return -AMIN(0., y); }
+
+void orc_mpdatamper(orc *o, double *unk, int iflag) {
+    (void)iflag;
+    int n = o->npoin, ne = o->nedge, nb = o->nbface;
+    double *const *uuu = &o->f[MPG_F_UUU];
+    const double *rh0 = o->f[MPG_F_RH0];
+    double *aun = dz(ne), *aunb = dz(nb), *divv = dz(n);
+    double *dpdxa = dz(n), *dpdya = dz(n), *dpdza = dz(n);
+    double *unkmx = dz(n), *unkmn = dz(n), *rhin = dz(n), *rhout = dz(n);
+    double *cpp = dz(n), *cnn = dz(n), *sw = dz(n), *sw1 = dz(n), *arh2 = dz(n);
+    int iord = 2, npass = iord, ifct = 1;
+    double tol = 1.e-10;
+    for (int ip = 0; ip < n; ++ip) { sw[ip] = 1.; sw1[ip] = 1.; }   /* ref.f:3652-3658 */
+    for (int ip = 0; ip < n; ++ip) { unkmx[ip] = -1.e15; unkmn[ip] = 1.e15; }
+    for (int ipass = 1; ipass <= npass + 1; ++ipass) {
+        for (int ip = 0; ip < n; ++ip) {
+            arh2[ip] = 0.;
+            sw[ip] = ipass == 1 ? 1. : sw1[ip];
+        }
+        for (int e = 0; e < ne; ++e) {                              /* ref.f:3681-3707 */
+            int i1 = o->ie1[e], i2 = o->ie2[e];
+            double sx = o->snx[e], sy = o->sny[e], sz = o->snz[e], fl;
+            if (ipass == 1) {
+                aun[e] = (uuu[0][i1] + uuu[0][i2]) * 0.5 * sx
+                       + (uuu[1][i1] + uuu[1][i2]) * 0.5 * sy
+                       + (uuu[2][i1] + uuu[2][i2]) * 0.5 * sz;
+                fl = unk[i1] * AMAX(0., aun[e]) + unk[i2] * AMIN(0., aun[e]);
+            } else {
+                fl = aun[e];
+            }
+            arh2[i1] = arh2[i1] + fl * (sw[i1] + sw[i2]) * 0.5;
+            arh2[i2] = arh2[i2] - fl * (sw[i1] + sw[i2]) * 0.5;
+            divv[i1] = divv[i1] + aun[e];
+            divv[i2] = divv[i2] - aun[e];
+        }
+        for (int e = 0; e < nb; ++e) {                              /* ref.f:3709-3730 */
+            int i1 = o->kb1[e], i2 = o->kb2[e];
+            double sx = o->sbx[e], sy = o->sby[e], sz = o->sbz[e], fl;
+            if (ipass == 1) {
+                aunb[e] = (uuu[0][i1] + uuu[0][i2]) * 0.5 * sx
+                        + (uuu[1][i1] + uuu[1][i2]) * 0.5 * sy
+                        + (uuu[2][i1] + uuu[2][i2]) * 0.5 * sz;
+                fl = unk[i1] * AMAX(0., aunb[e]) + unk[i2] * AMIN(0., aunb[e]);
+            } else {
+                fl = aunb[e];
+            }
+            arh2[i1] = arh2[i1] + fl * (sw[i1] + sw[i2]) * 0.5;
+            arh2[i2] = arh2[i2] - fl * (sw[i1] + sw[i2]) * 0.5;
+            divv[i1] = divv[i1] + aunb[e];
+            divv[i2] = divv[i2] - aunb[e];
+        }
+        for (int b = 0; b < o->nboun; ++b) {                        /* ref.f:3732-3738 */
+            int i1 = o->ibn[b];
+            double fl1 = 0.;
+            arh2[i1] = arh2[i1] + fl1 * sw[i1];
+        }
+        cyclicr(o, arh2);
+        cyclicr2(o, arh2);
+        cyclicr4(o, arh2);
+        for (int ip = 0; ip < n; ++ip)                              /* ref.f:3745-3747 */
+            unk[ip] = unk[ip] - arh2[ip] * o->timestp[ip] / o->vol[ip] / rh0[ip];
+        if (ipass == iord) break;
+        orc_derivative(o, unk, dpdxa, 1);                           /* ref.f:3755-3757 */
+        orc_derivative(o, unk, dpdya, 2);
+        orc_derivative(o, unk, dpdza, 3);
+        double dt1 = o->timestp[0];
+        for (int e = 0; e < ne + nb; ++e) {                         /* ref.f:3760-3794 */
+            int in = e < ne;
+            int i1 = in ? o->ie1[e] : o->kb1[e - ne], i2 = in ? o->ie2[e] : o->kb2[e - ne];
+            double *a = in ? &aun[e] : &aunb[e - ne];
+            double un = fabs(*a) * (unk[i2] - unk[i1]) * 0.5;
+            double volt = 0.5 * (o->vol[i1] * rh0[i1] + o->vol[i2] * rh0[i2]);
+            double dpdx = 0.5 * (dpdxa[i1] + dpdxa[i2]) / volt;
+            double dpdy = 0.5 * (dpdya[i1] + dpdya[i2]) / volt;
+            double dpdz = 0.5 * (dpdza[i1] + dpdza[i2]) / volt;
+            double term = (uuu[0][i1] + uuu[0][i2]) * 0.5 * dpdx
+                        + (uuu[1][i1] + uuu[1][i2]) * 0.5 * dpdy
+                        + (uuu[2][i1] + uuu[2][i2]) * 0.5 * dpdz;
+            *a = un - *a * term * dt1 * 0.5;
+        }
+        if (ifct == 1) {                                            /* ref.f:3796-3932 */
+            for (int e = 0; e < ne + nb; ++e) {
+                int in = e < ne;
+                int i1 = in ? o->ie1[e] : o->kb1[e - ne], i2 = in ? o->ie2[e] : o->kb2[e - ne];
+                double p1 = unk[i1], p2 = unk[i2];
+                unkmx[i1] = AMAX(AMAX(unkmx[i1], p1), p2);
+                unkmn[i1] = AMIN(AMIN(unkmn[i1], p1), p2);
+                unkmx[i2] = AMAX(AMAX(unkmx[i2], p2), p1);
+                unkmn[i2] = AMIN(AMIN(unkmn[i2], p2), p1);
+            }
+            for (int c = 0; c < o->ncoin; ++c) {
+                int i1 = o->ic1[c], i2 = o->ic2[c];
+                double p1 = unk[i1], p2 = unk[i2];
+                unkmx[i1] = AMAX(AMAX(AMAX(unkmx[i1], p1), p2), unkmx[i2]);
+                unkmn[i1] = AMIN(AMIN(AMIN(unkmn[i1], p1), p2), unkmn[i2]);
+                unkmx[i2] = AMAX(AMAX(AMAX(unkmx[i2], p1), p2), unkmx[i1]);
+                unkmn[i2] = AMIN(AMIN(AMIN(unkmn[i2], p1), p2), unkmn[i1]);
+            }
+            for (int c = 0; c < o->ncoin2; ++c) {
+                int i1 = o->ic2a[c], i2 = o->ic2b[c];
+                double p1 = unk[i1], p2 = unk[i2];
+                unkmx[i1] = AMAX(AMAX(AMAX(unkmx[i1], p1), p2), unkmx[i2]);
+                unkmn[i1] = AMIN(AMIN(AMIN(unkmn[i1], p1), p2), unkmn[i2]);
+                unkmx[i2] = AMAX(AMAX(AMAX(unkmx[i2], p1), p2), unkmx[i1]);
+                unkmn[i2] = AMIN(AMIN(AMIN(unkmn[i2], p1), p2), unkmn[i1]);
+            }
+            for (int c = 0; c < o->ncoin4; ++c) {
+                /* ref.f:3853-3866: the minima are taken over the maxima unkmx (as written). */
+                int ii[4] = {o->ic4[0][c], o->ic4[1][c], o->ic4[2][c], o->ic4[3][c]};
+                double pp[4] = {unk[ii[0]], unk[ii[1]], unk[ii[2]], unk[ii[3]]};
+                for (int j = 0; j < 4; ++j) {
+                    double mx = unkmx[ii[0]];
+                    for (int q = 1; q < 4; ++q) mx = AMAX(mx, unkmx[ii[q]]);
+                    for (int q = 0; q < 4; ++q) mx = AMAX(mx, pp[q]);
+                    unkmx[ii[j]] = mx;
+                    double mn = unkmx[ii[0]];
+                    for (int q = 1; q < 4; ++q) mn = AMIN(mn, unkmx[ii[q]]);
+                    for (int q = 0; q < 4; ++q) mn = AMIN(mn, pp[q]);
+                    unkmn[ii[j]] = mn;
+                }
+            }
+            for (int ip = 0; ip < n; ++ip) { rhin[ip] = 0.; rhout[ip] = 0.; cpp[ip] = 0.; cnn[ip] = 0.; }
+            for (int e = 0; e < ne + nb; ++e) {
+                int in = e < ne;
+                int i1 = in ? o->ie1[e] : o->kb1[e - ne], i2 = in ? o->ie2[e] : o->kb2[e - ne];
+                double a = in ? aun[e] : aunb[e - ne];
+                rhin[i1] = rhin[i1] + partn(a);
+                rhout[i1] = rhout[i1] + partp(a);
+                rhin[i2] = rhin[i2] + partp(a);
+                rhout[i2] = rhout[i2] + partn(a);
+            }
+            cyclicr(o, rhin); cyclicr(o, rhout);
+            cyclicr2(o, rhin); cyclicr2(o, rhout);
+            cyclicr4(o, rhin); cyclicr4(o, rhout);
+            for (int ip = 0; ip < n; ++ip) {
+                cpp[ip] = (unkmx[ip] - unk[ip]) * o->vol[ip] * rh0[ip] / (rhin[ip] * o->timestp[ip] + tol);
+                cnn[ip] = (unk[ip] - unkmn[ip]) * o->vol[ip] * rh0[ip] / (rhout[ip] * o->timestp[ip] + tol);
+            }
+            for (int e = 0; e < ne + nb; ++e) {
+                int in = e < ne;
+                int i1 = in ? o->ie1[e] : o->kb1[e - ne], i2 = in ? o->ie2[e] : o->kb2[e - ne];
+                double *a = in ? &aun[e] : &aunb[e - ne];
+                if (*a > 0.) *a = *a * AMIN(AMIN(1., cpp[i2]), cnn[i1]);
+                else *a = *a * AMIN(AMIN(1., cnn[i2]), cpp[i1]);
+            }
+        }
+    }
+    free(aun); free(aunb); free(divv); free(dpdxa); free(dpdya); free(dpdza);
+    free(unkmx); free(unkmn); free(rhin); free(rhout); free(cpp); free(cnn);
+    free(sw); free(sw1); free(arh2);
+}
+
+/* ------------------------------------------------------------------ courant ref.f:1974-2094 */
+void orc_courant(orc *o, int iflag, mpg_diag *diag) {
+    int n = o->npoin;
+    double *cour = o->f[MPG_F_COUR];
+    const double *rh0 = o->f[MPG_F_RH0];
+    double *const *uuu = &o->f[MPG_F_UUU];
+    for (int ip = 0; ip < n; ++ip) cour[ip] = 0.;
+    for (int e = 0; e < o->nedge + o->nbface; ++e) {
+        int in = e < o->nedge;
+        int i1 = in ? o->ie1[e] : o->kb1[e - o->nedge], i2 = in ? o->ie2[e] : o->kb2[e - o->nedge];
+        double sx = in ? o->snx[e] : o->sbx[e - o->nedge];
+        double sy = in ? o->sny[e] : o->sby[e - o->nedge];
+        double sz = in ? o->snz[e] : o->sbz[e - o->nedge];
+        double rhav = 0.5 * (rh0[i1] + rh0[i2]);
+        double aun = (uuu[0][i1] + uuu[0][i2]) * 0.5 * sx
+                   + (uuu[1][i1] + uuu[1][i2]) * 0.5 * sy
+                   + (uuu[2][i1] + uuu[2][i2]) * 0.5 * sz;
+        aun = aun / rhav;
+        if (iflag == 1) { cour[i1] = cour[i1] + fabs(aun); cour[i2] = cour[i2] + fabs(aun); }
+        if (iflag == 2) { cour[i1] = cour[i1] + aun; cour[i2] = cour[i2] - aun; }
+        if (iflag == 3) { cour[i1] = cour[i1] + AMAX(0., aun); cour[i2] = cour[i2] - AMIN(0., aun); }
+    }
+    if (o->P.iper != 2) {
+        for (int b = 0; b < o->nboun; ++b) {
+            int i1 = o->ibn[b];
+            double aun = uuu[0][i1] * o->sbbx[b] + uuu[1][i1] * o->sbby[b] + uuu[2][i1] * o->sbbz[b];
+            aun = aun / rh0[i1];
+            if (iflag == 1) cour[i1] = cour[i1] + fabs(aun);
+            if (iflag == 2) cour[i1] = cour[i1] + aun;
+            if (iflag == 3) cour[i1] = cour[i1] + AMAX(0., aun);
+        }
+    }
+    for (int ip = 0; ip < n; ++ip) cour[ip] = cour[ip] * o->timestp[ip] / o->vol[ip] / rh0[ip];
+    double crnmx = -1.e9, crnmn = 1.e9, crnav = 0., crnsd = 0.;
+    int ic = 0;
+    for (int ip = 0; ip < n; ++ip) {
+        crnav = crnav + cour[ip];
+        crnmx = AMAX(crnmx, cour[ip]);
+        crnmn = AMIN(crnmn, cour[ip]);
+        if (crnmx == cour[ip]) ic = ip + 1;
+    }
+    crnav = crnav / n;
+    for (int ip = 0; ip < n; ++ip) crnsd = crnsd + (cour[ip] - crnav) * (cour[ip] - crnav);
+    crnsd = sqrt(crnsd / n);
+    if (diag) {
+        diag->crnmx = crnmx; diag->crnmn = crnmn; diag->crnav = crnav; diag->crnsd = crnsd;
+        diag->icrnmx = ic;
+    }
+}
+
+/* ------------------------------------------------------------------ stats ref.f:2847-2912 (+ NEW sums) */
+void orc_stats(orc *o, mpg_diag *diag) {
+    int n = o->npoin;
+    const double *rh0 = o->f[MPG_F_RH0];
+    double av[4] = {0, 0, 0, 0}, mx[4], mn[4], sd[4] = {0, 0, 0, 0}, rav = 0.;
+    for (int k = 0; k < 4; ++k) { mx[k] = -1.e10; mn[k] = 1.e10; }
+    for (int ip = 0; ip < n; ++ip) {
+        rav = rav + rh0[ip];
+        for (int k = 0; k < 4; ++k) {
+            double u = o->f[MPG_F_UNK + k][ip];
+            av[k] = av[k] + rh0[ip] * u;
+            mx[k] = AMAX(mx[k], u);
+            mn[k] = AMIN(mn[k], u);
+        }
+    }
+    for (int k = 0; k < 4; ++k) av[k] = av[k] / rav;
+    for (int ip = 0; ip < n; ++ip)
+        for (int k = 0; k < 4; ++k) {
+            double t = o->f[MPG_F_UNK + k][ip] - av[k];
+            sd[k] = sd[k] + rh0[ip] * (t * t);
+        }
+    for (int k = 0; k < 3; ++k) sd[k] = sqrt(sd[k] / rav);
+    sd[3] = sqrt(sd[3] / n);                                   /* ref.f:2903 divides by npoin */
+    if (!diag) return;
+    for (int k = 0; k < 4; ++k) {
+        diag->stats[4 * k + 0] = mx[k]; diag->stats[4 * k + 1] = mn[k];
+        diag->stats[4 * k + 2] = av[k]; diag->stats[4 * k + 3] = sd[k];
+    }
+    int nf = 4 + o->P.nscal;
+    for (int k = 0; k < nf && k < 8; ++k) {                   /* NEW: FP64 mass sums */
+        double s = 0.;
+        const double *u = o->f[MPG_F_UNK + k];
+        for (int ip = 0; ip < n; ++ip) s = s + o->vol[ip] * rh0[ip] * u[ip];
+        diag->mass[k] = s;
+    }
+    for (int s = 0; s < o->P.nscal && s < 4; ++s) {
+        const double *u = o->f[MPG_F_UNK + 4 + s];
+        double a = 1.e300, b = -1.e300;
+        for (int ip = 0; ip < n; ++ip) { a = AMIN(a, u[ip]); b = AMAX(b, u[ip]); }
+        diag->smin[s] = a; diag->smax[s] = b;
+    }
+}
+
+/* ------------------------------------------------------------------ set-up helpers */
+/* rhprof ref.f:4549-4579, thprof ref.f:4532-4547 */
+static void rhprof_thprof(orc *o) {
+    int n = o->npoin;
+    double *rh0 = o->f[MPG_F_RH0], *th0 = o->f[MPG_F_TH0];
+    double g = o->P.g, st = o->P.strat, tt00 = o->P.tetbar, th00 = o->P.tetbar;
+    double rgas = 287.04, cp = 3.5 * rgas, cap = rgas / cp, capi = 1. / cap;
+    double cs = g / (cp * tt00 * st);
+    double rh0inf = 1., rh00 = 1.;
+    o->rgas = rgas; o->cp = cp; o->cap = cap;
+    for (int ip = 0; ip < n; ++ip) {
+        rh0[ip] = rh0inf;
+        if (o->P.lipps == 1) {
+            double exs = exp(-st * o->z[ip]);
+            rh0[ip] = rh00 * exs * pow(1. - cs * (1. - exs), capi - 1.);
+        }
+    }
+    for (int ip = 0; ip < n; ++ip)
+        th0[ip] = o->P.lipps == 1 ? th00 * exp(st * o->z[ip]) : th00;
+}
+
+/* absorbers ref.f:2915-3026 */
+static void absorbers(orc *o) {
+    int n = o->npoin;
+    double *alpha = o->f[MPG_F_ALPHA];
+    const mpg_params *P = &o->P;
+    double r = 1., eps = 1.e-07;
+    if (P->irl != 1) return;
+    double abxmax = -1.e+07, abxmin = 1.e+07, abymax = -1.e+07, abymin = 1.e+07;
+    double abzmax = -1.e+07, abzmin = 1.e+07;
+    for (int ip = 0; ip < n; ++ip) {
+        abxmax = AMAX(o->x[ip], abxmax); abxmin = AMIN(o->x[ip], abxmin);
+        abymax = AMAX(o->y[ip], abymax); abymin = AMIN(o->y[ip], abymin);
+        abzmax = AMAX(o->z[ip], abzmax); abzmin = AMIN(o->z[ip], abzmin);
+    }
+    double xabr = abxmax * r - P->dxabr, xabl = abxmin * r + P->dxabl;
+    double yabu = abymax * r - P->dyabu, yabd = abymin * r + P->dyabd;
+    double zabu = abzmax - P->dzabu, zabd = abzmin + P->dzabd;
+    double tolil = P->towxl != 0. ? 1. / P->towxl : 0.;
+    double tolir = P->towxr != 0. ? 1. / P->towxr : 0.;
+    double toliu = P->towyu != 0. ? 1. / P->towyu : 0.;
+    double tolid = P->towyd != 0. ? 1. / P->towyd : 0.;
+    double toliuz = P->towzu != 0. ? 1. / P->towzu : 0.;
+    double tolidz = P->towzd != 0. ? 1. / P->towzd : 0.;
+    for (int ip = 0; ip < n; ++ip) {
+        double relx, rely, relz, r0, r1, r2, relb;
+        r0 = o->x[ip] * r; r1 = 0.; r2 = 0.; relb = 0.;
+        if (P->dxabl != 0.) r1 = AMAX(0., xabl - r0) / P->dxabl;
+        if (P->dxabr != 0.) r2 = AMAX(0., r0 - xabr) / P->dxabr;
+        if ((tolil + tolir) != 0.)
+            relb = ((tolil * r1) * (tolil * r1) + (tolir * r2) * (tolir * r2)) / (tolil * r1 + tolir * r2 + eps);
+        relx = relb;
+        r1 = 0.; r2 = 0.; relb = 0.;
+        r0 = o->y[ip] * r;
+        if (P->dyabd != 0.) r1 = AMAX(0., -r0 + yabd) / P->dyabd;
+        if (P->dyabu != 0.) r2 = AMAX(0., r0 - yabu) / P->dyabu;
+        if ((tolid + toliu) != 0.)
+            relb = ((tolid * r1) * (tolid * r1) + (toliu * r2) * (toliu * r2)) / (tolid * r1 + toliu * r2 + eps);
+        rely = relb;
+        r1 = 0.; r2 = 0.; relb = 0.;
+        r0 = o->z[ip];
+        if (P->dzabd != 0.) r1 = AMAX(0., -r0 + zabd) / P->dzabd;
+        if (P->dzabu != 0.) r2 = AMAX(0., r0 - zabu) / P->dzabu;
+        if ((tolidz + toliuz) != 0.)
+            relb = ((tolidz * r1) * (tolidz * r1) + (toliuz * r2) * (toliuz * r2)) / (tolidz * r1 + toliuz * r2 + eps);
+        relz = relb;
+        double alpha1 = (rely * rely + relx * relx) / (rely + relx + eps);
+        alpha[ip] = (alpha1 * alpha1 + relz * relz) / (alpha1 + relz + eps);
+    }
+}
+
+/* beta_timestep_unstr(1) ref.f:953-1109 — the domain box and hill height are the
+ * reference's hard-coded values (ref.f:2255-2260, ref.f:1041). */
+static void beta_timestep(orc *o) {
+    double dom_x1 = 0., dom_x2 = 15000., dom_y1 = -6000., dom_y2 = 6000., dom_z1 = 0., dom_z2 = 6000.;
+    double ddx = 10.e+06, hill_height = 1500.0;
+    for (int e = 0; e < o->nedge; ++e) {
+        int i1 = o->ie1[e], i2 = o->ie2[e];
+        if (o->x[i1] != dom_x1 && o->x[i1] != dom_x2 && o->y[i1] != dom_y1 && o->y[i1] != dom_y2
+            && o->z[i1] != dom_z1 && o->z[i1] != dom_z2 && o->x[i2] != dom_x1 && o->x[i2] != dom_x2
+            && o->y[i2] != dom_y1 && o->y[i2] != dom_y2 && o->z[i2] != dom_z1 && o->z[i2] != dom_z2
+            && o->z[i1] > hill_height && o->z[i2] > hill_height) {
+            double hx = fabs(o->snx[e]), hy = fabs(o->sny[e]), hz = fabs(o->snz[e]);
+            double h = AMAX(AMAX(hx, hy), hz);
+            ddx = AMIN(AMIN(ddx, o->vol[i1] / h), o->vol[i2] / h);
+        }
+    }
+    double safety_factor = 1;
+    o->betaunstr1 = 0.5 * ddx * ddx * safety_factor;
+}
+
+/* compute_d_unstr(1) ref.f:1112-1284 */
+static void compute_d(orc *o) {
+    int n = o->npoin;
+    const double *rh0 = o->f[MPG_F_RH0];
+    double *dix = dz(n), *diy = dz(n), *diz = dz(n);
+    for (int e = 0; e < o->nedge + o->nbface; ++e) {
+        int in = e < o->nedge;
+        int i1 = in ? o->ie1[e] : o->kb1[e - o->nedge], i2 = in ? o->ie2[e] : o->kb2[e - o->nedge];
+        double sx = in ? o->snx[e] : o->sbx[e - o->nedge];
+        double sy = in ? o->sny[e] : o->sby[e - o->nedge];
+        double sz = in ? o->snz[e] : o->sbz[e - o->nedge];
+        dix[i1] = dix[i1] + sx * sx * rh0[i2] / o->vol[i2];
+        dix[i2] = dix[i2] + sx * sx * rh0[i1] / o->vol[i1];
+        diy[i1] = diy[i1] + sy * sy * rh0[i2] / o->vol[i2];
+        diy[i2] = diy[i2] + sy * sy * rh0[i1] / o->vol[i1];
+        diz[i1] = diz[i1] + sz * sz * rh0[i2] / o->vol[i2];
+        diz[i2] = diz[i2] + sz * sz * rh0[i1] / o->vol[i1];
+    }
+    for (int ip = 0; ip < n; ++ip)
+        o->d1[ip] = -0.5 * o->timestp[ip] * (dix[ip] + diy[ip] + diz[ip]) / (4 * o->vol[ip] * rh0[ip]);
+    free(dix); free(diy); free(diz);
+}
+
+/* ------------------------------------------------------------------ mpsolver set-up ref.f:99-273 */
+void orc_setup(orc *o, mpg_diag *diag) {
+    int n = o->npoin;
+    const mpg_params *P = &o->P;
+    double **f = o->f;
+    double *rh0 = f[MPG_F_RH0], *th0 = f[MPG_F_TH0], *the = f[MPG_F_THE], *dthedz = f[MPG_F_DTHEDZ];
+    double *coefw = f[MPG_F_COEFW], *prpot = f[MPG_F_PRPOT];
+    if (P->iper == 2) { cyclicr(o, o->vol); cyclicr2(o, o->vol); cyclicr4(o, o->vol); }
+    double g = P->g, tet00 = P->tetbar, strat = P->strat;
+    int implgw = P->implgw;
+    rhprof_thprof(o);
+    absorbers(o);
+    double r = 1.;                                             /* isfera = 0 */
+    for (int ip = 0; ip < n; ++ip) {
+        o->cosa[ip] = cos(o->y[ip]) * (double)P->isfera + (1. - (double)P->isfera);
+        o->gmm[ip] = 1. + o->z[ip] / r * (double)P->isfera;
+        rh0[ip] = rh0[ip] * (o->gmm[ip] * o->gmm[ip]) * o->cosa[ip];
+    }
+    for (int ip = 0; ip < n; ++ip) o->timestp[ip] = P->delt;  /* input, ref.f:2507-2509 */
+    beta_timestep(o);
+    compute_d(o);
+    for (int ip = 0; ip < n; ++ip) {                           /* ref.f:177-207 */
+        o->ue[ip] = P->u0inf;
+        o->ve[ip] = P->v0inf;
+        if (P->lipps == 0) {
+            the[ip] = tet00 * (1. + strat * o->z[ip]);
+            dthedz[ip] = tet00 * strat * (double)implgw;
+        } else {
+            the[ip] = th0[ip];
+            dthedz[ip] = the[ip] * strat * (double)implgw;
+        }
+        f[MPG_F_UNK + 0][ip] = o->ue[ip];
+        f[MPG_F_UNK + 1][ip] = o->ve[ip];
+        f[MPG_F_UNK + 2][ip] = 0.2 * f[MPG_F_FRC + 0][ip];
+        f[MPG_F_UNK + 3][ip] = 0. + 0.001 * f[MPG_F_FRC + 0][ip];
+        f[MPG_F_UNK1 + 0][ip] = f[MPG_F_UNK + 0][ip] / (o->gmm[ip] * o->cosa[ip]);
+        f[MPG_F_UNK1 + 1][ip] = f[MPG_F_UNK + 1][ip] / o->gmm[ip];
+        f[MPG_F_UNK1 + 2][ip] = f[MPG_F_UNK + 2][ip];
+        f[MPG_F_UNK1 + 3][ip] = 0.;
+        prpot[ip] = 0.;
+    }
+    orc_gcrk(o, prpot, f[MPG_F_UNK1], f[MPG_F_UNK1 + 1], f[MPG_F_UNK1 + 2],
+             f[MPG_F_UNK], f[MPG_F_UNK + 1], f[MPG_F_UNK + 2], 0, NULL);
+    orc_prfr(o, prpot, f[MPG_F_UNK1], f[MPG_F_UNK1 + 1], f[MPG_F_UNK1 + 2],
+             f[MPG_F_UNK], f[MPG_F_UNK + 1], f[MPG_F_UNK + 2], 0);
+    for (int ip = 0; ip < n; ++ip) {
+        for (int k = 0; k < 3; ++k) f[MPG_F_UUU + k][ip] = f[MPG_F_UNK + k][ip];
+        f[MPG_F_UNK][ip] = f[MPG_F_UNK][ip] * o->gmm[ip] * o->cosa[ip];
+        f[MPG_F_UNK + 1][ip] = f[MPG_F_UNK + 1][ip] * o->gmm[ip];
+    }
+    for (int ip = 0; ip < n; ++ip) {                           /* ref.f:242-253 */
+        prpot[ip] = 0.;
+        for (int k = 0; k < 4; ++k) f[MPG_F_FRC + k][ip] = 0.;
+        double gth0 = g / th0[ip];
+        coefw[ip] = 1. + 0.25 * (o->timestp[0] * o->timestp[0]) * gth0 * dthedz[ip];
+        coefw[ip] = 1. / coefw[ip];
+    }
+    for (int ip = 0; ip < n; ++ip) {                           /* itraj = 0, ref.f:258-266 */
+        for (int k = 0; k < 3; ++k) {
+            f[MPG_F_UUU + k][ip] = f[MPG_F_UUU + k][ip] * rh0[ip];
+            f[MPG_F_UNKDASH + k][ip] = f[MPG_F_UNK + k][ip];
+        }
+    }
+    mpg_diag dd;
+    memset(&dd, 0, sizeof dd);
+    orc_div(o, f[MPG_F_UUU], f[MPG_F_UUU + 1], f[MPG_F_UUU + 2], f[MPG_F_RHS], 1, &dd);
+    orc_courant(o, 1, &dd);
+    orc_stats(o, &dd);
+    if (diag) *diag = dd;
+}
+
+/* ------------------------------------------------------------------ one DO ITIME pass ref.f:285-463 */
+void orc_step(orc *o, mpg_diag *diag) {
+    int n = o->npoin;
+    const mpg_params *P = &o->P;
+    double **f = o->f;
+    double *rh0 = f[MPG_F_RH0], *th0 = f[MPG_F_TH0], *dthedz = f[MPG_F_DTHEDZ];
+    double *coefw = f[MPG_F_COEFW], *alpha = f[MPG_F_ALPHA];
+    double *ts = o->timestp, g = P->g;
+    int implgw = P->implgw, icorio = 0, ideep = 1;
+    double f0 = 1.4584e-03, xlat = 20.;
+    double *unk[4] = {f[MPG_F_UNK], f[MPG_F_UNK + 1], f[MPG_F_UNK + 2], f[MPG_F_UNK + 3]};
+    double *frc[4] = {f[MPG_F_FRC], f[MPG_F_FRC + 1], f[MPG_F_FRC + 2], f[MPG_F_FRC + 3]};
+    double *uuu[3] = {f[MPG_F_UUU], f[MPG_F_UUU + 1], f[MPG_F_UUU + 2]};
+    double *uuu0[3] = {f[MPG_F_UUU0], f[MPG_F_UUU0 + 1], f[MPG_F_UUU0 + 2]};
+    double *ud[3] = {f[MPG_F_UNKDASH], f[MPG_F_UNKDASH + 1], f[MPG_F_UNKDASH + 2]};
+    double *unk1[3] = {f[MPG_F_UNK1], f[MPG_F_UNK1 + 1], f[MPG_F_UNK1 + 2]};
+    for (int ip = 0; ip < n; ++ip) {                           /* ref.f:290-301 */
+        for (int k = 0; k < 3; ++k) uuu0[k][ip] = uuu[k][ip];
+        for (int k = 0; k < 4; ++k) unk[k][ip] = unk[k][ip] + 0.5 * frc[k][ip] * ts[ip];
+        if (implgw == 0) unk[3][ip] = unk[3][ip] + f[MPG_F_THE][ip];
+    }
+    for (int k = 0; k < 4 + P->nscal; ++k)                     /* ref.f:314-319 */
+        orc_mpdatamper(o, f[MPG_F_UNK + k], k + 1);
+    int mtrimx = 2;
+    for (int mtri = 1; mtri <= mtrimx; ++mtri) {
+        for (int ip = 0; ip < n; ++ip) {                       /* ref.f:323-359 */
+            double frm1 = 0., frm2 = 0., frm3 = 0.;
+            double fcr3 = f0 * sin(xlat) * (double)icorio;
+            double fcr2 = f0 * cos(xlat) * (double)icorio;
+            if (mtri == 1 && implgw == 0) unk[3][ip] = unk[3][ip] - f[MPG_F_THE][ip];
+            double we = 0.;
+            frm1 = frm1 + fcr3 * (ud[1][ip] - o->ve[ip]) - fcr2 * (ud[2][ip] - we) * (double)ideep
+                   - alpha[ip] * (ud[0][ip] - o->ue[ip]);
+            frm2 = frm2 - fcr3 * (ud[0][ip] - o->ue[ip]) - alpha[ip] * (ud[1][ip] - o->ve[ip]);
+            frm3 = frm3 + fcr2 * (ud[0][ip] - o->ue[ip]) * (double)ideep - alpha[ip] * ud[2][ip]
+                   + g * unk[3][ip] / th0[ip];
+            frc[0][ip] = unk[0][ip] + 0.5 * ts[ip] * frm1;
+            frc[1][ip] = unk[1][ip] + 0.5 * ts[ip] * frm2;
+            frc[2][ip] = (unk[2][ip] + 0.5 * ts[ip] * frm3) * coefw[ip];
+            unk1[0][ip] = frc[0][ip] / (o->gmm[ip] * o->cosa[ip]);
+            unk1[1][ip] = frc[1][ip] / o->gmm[ip];
+            unk1[2][ip] = frc[2][ip];
+        }
+        int imp = implgw;                                      /* ref.f:361-365 */
+        orc_gcrk(o, f[MPG_F_PRPOT], unk1[0], unk1[1], unk1[2], uuu[0], uuu[1], uuu[2], imp, NULL);
+        orc_prfr(o, f[MPG_F_PRPOT], unk1[0], unk1[1], unk1[2], uuu[0], uuu[1], uuu[2], imp);
+        for (int ip = 0; ip < n; ++ip) {                       /* ref.f:367-383 */
+            ud[0][ip] = uuu[0][ip] * o->gmm[ip] * o->cosa[ip];
+            ud[1][ip] = uuu[1][ip] * o->gmm[ip];
+            ud[2][ip] = uuu[2][ip];
+            if (mtri == mtrimx) {
+                frc[0][ip] = (ud[0][ip] - frc[0][ip]) * 2. / ts[ip];
+                frc[1][ip] = (ud[1][ip] - frc[1][ip]) * 2. / ts[ip];
+                double frc33 = frc[2][ip] / coefw[ip] - (g * unk[3][ip] / th0[ip]) * 0.5 * ts[ip];
+                frc[2][ip] = (ud[2][ip] - frc33) * 2. / ts[ip];
+                unk[0][ip] = ud[0][ip];
+                unk[1][ip] = ud[1][ip];
+                unk[2][ip] = ud[2][ip];
+                frc[3][ip] = -unk[2][ip] * dthedz[ip];
+                unk[3][ip] = unk[3][ip] + 0.5 * ts[0] * frc[3][ip];
+            }
+        }
+    }
+    for (int ip = 0; ip < n; ++ip) {                           /* ref.f:387-439 */
+        double frm1 = 0., frm2 = 0., frm3 = 0.;
+        double fcr3 = f0 * sin(xlat) * (double)icorio;
+        double fcr2 = f0 * cos(xlat) * (double)icorio;
+        frm1 = frm1 + fcr3 * (unk[1][ip] - o->ve[ip]) - fcr2 * (unk[2][ip] - 0.) * (double)ideep
+               - alpha[ip] * (unk[0][ip] - o->ue[ip]);
+        frm2 = frm2 - fcr3 * (unk[0][ip] - o->ue[ip]) - alpha[ip] * (unk[1][ip] - o->ve[ip]);
+        frm3 = frm3 + fcr2 * (unk[0][ip] - o->ue[ip]) * (double)ideep - alpha[ip] * (unk[2][ip]);
+        double frm4 = -alpha[ip] * (unk[3][ip]);
+        frc[0][ip] = frc[0][ip] + frm1;
+        frc[1][ip] = frc[1][ip] + frm2;
+        frc[2][ip] = frc[2][ip] + frm3;
+        frc[3][ip] = frc[3][ip] + frm4;
+        for (int k = 0; k < 3; ++k) uuu[k][ip] = 1.5 * uuu[k][ip] * rh0[ip] - 0.5 * uuu0[k][ip];
+        double rhoi = 1. / rh0[ip];
+        uuu0[0][ip] = uuu0[0][ip] * rhoi * o->gmm[ip] * o->cosa[ip];
+        uuu0[1][ip] = uuu0[1][ip] * rhoi * o->gmm[ip];
+        uuu0[2][ip] = uuu0[2][ip] * rhoi;
+        for (int k = 0; k < 3; ++k) ud[k][ip] = 2. * unk[k][ip] - uuu0[k][ip];
+    }
+    mpg_diag dd;                                               /* ref.f:456-459 */
+    memset(&dd, 0, sizeof dd);
+    orc_div(o, uuu[0], uuu[1], uuu[2], f[MPG_F_RHS], 1, &dd);
+    orc_courant(o, 1, &dd);
+    orc_stats(o, &dd);
+    if (diag) *diag = dd;
+}
+
+/* ------------------------------------------------------------------ construction */
+orc *orc_create(const mpg_params *prm, const mpg_mesh_ref *m) {
+    if (!prm || !m || prm->isfera != 0 || prm->mg_flag != 0 || prm->nscal < 0
+        || 4 + prm->nscal > MAXUNK || prm->lord < 1)
+        return NULL;
+    orc *o = (orc *)calloc(1, sizeof(orc));
+    o->P = *prm;
+    int n = m->npoin;
+    o->npoin = n; o->nedge = m->nedge; o->nbface = m->nbface; o->nboun = m->nboun;
+    o->ncoin = m->ncoin; o->ncoin2 = m->ncoin2; o->ncoin4 = m->ncoin4;
+    o->x = dz(n); o->y = dz(n); o->z = dz(n); o->vol = dz(n);
+    for (int i = 0; i < n; ++i) {
+        o->x[i] = m->coord[i];
+        o->y[i] = m->coord[(size_t)m->npoinx + i];
+        o->z[i] = m->coord[2 * (size_t)m->npoinx + i];
+        o->vol[i] = m->vol[i];
+    }
+    int ne = m->nedge;
+    o->ie1 = iz(ne); o->ie2 = iz(ne); o->snx = dz(ne); o->sny = dz(ne); o->snz = dz(ne);
+    for (int e = 0; e < ne; ++e) {
+        o->ie1[e] = m->iedge[e] - 1;
+        o->ie2[e] = m->iedge[(size_t)m->nedgex + e] - 1;
+        o->snx[e] = m->sn[e];
+        o->sny[e] = m->sn[(size_t)m->nedgex + e];
+        o->snz[e] = m->sn[2 * (size_t)m->nedgex + e];
+    }
+    int nb = m->nbface, nf = m->nfacesx;
+    o->kb1 = iz(nb); o->kb2 = iz(nb); o->sbx = dz(nb); o->sby = dz(nb); o->sbz = dz(nb);
+    for (int e = 0; e < nb; ++e) {
+        o->kb1[e] = m->kbface[e] - 1;
+        o->kb2[e] = m->kbface[(size_t)nf + e] - 1;
+        o->sbx[e] = m->sb[e]; o->sby[e] = m->sb[(size_t)nf + e]; o->sbz[e] = m->sb[2 * (size_t)nf + e];
+    }
+    int nbo = m->nboun;
+    o->ibn = iz(nbo); o->ibt = iz(nbo);
+    o->sbbx = dz(nbo); o->sbby = dz(nbo); o->sbbz = dz(nbo);
+    o->anx = dz(nbo); o->any = dz(nbo); o->anz = dz(nbo);
+    for (int b = 0; b < nbo; ++b) {
+        o->ibn[b] = m->ibpoin[b] - 1;
+        o->ibt[b] = m->ibpoin[(size_t)nf + b];
+        o->sbbx[b] = m->sbb[b]; o->sbby[b] = m->sbb[(size_t)nf + b]; o->sbbz[b] = m->sbb[2 * (size_t)nf + b];
+        o->anx[b] = m->anp[b]; o->any[b] = m->anp[(size_t)nf + b]; o->anz[b] = m->anp[2 * (size_t)nf + b];
+    }
+    o->ic1 = iz(o->ncoin); o->ic2 = iz(o->ncoin);
+    for (int c = 0; c < o->ncoin; ++c) {
+        o->ic1[c] = m->icoin[c] - 1;
+        o->ic2[c] = m->icoin[(size_t)m->ldcoin + c] - 1;
+    }
+    o->ic2a = iz(o->ncoin2); o->ic2b = iz(o->ncoin2);
+    for (int c = 0; c < o->ncoin2; ++c) {
+        o->ic2a[c] = m->icoin2[c] - 1;
+        o->ic2b[c] = m->icoin2[(size_t)nf + c] - 1;
+    }
+    for (int j = 0; j < 4; ++j) {
+        o->ic4[j] = iz(o->ncoin4);
+        for (int c = 0; c < o->ncoin4; ++c) o->ic4[j][c] = m->icoin4[(size_t)j * nf + c] - 1;
+    }
+    o->timestp = dz(n); o->cosa = dz(n); o->gmm = dz(n); o->ue = dz(n); o->ve = dz(n); o->d1 = dz(n);
+    for (int i = 0; i < n; ++i) { o->timestp[i] = prm->delt; o->cosa[i] = 1.; o->gmm[i] = 1.; }
+    for (int k = 0; k < MPG_F_COUNT; ++k) {
+        if (k >= MPG_F_UNK + 4 + prm->nscal && k < MPG_F_UNK1) continue;
+        o->f[k] = dz(n);
+    }
+    /* d1 lives in o->d1; expose it by id too */
+    free(o->f[MPG_F_D1]);
+    o->f[MPG_F_D1] = o->d1;
+    for (int i = 0; i < n; ++i) o->f[MPG_F_RH0][i] = 1., o->f[MPG_F_COEFW][i] = 1., o->f[MPG_F_TH0][i] = prm->tetbar;
+    return o;
+}
+
+void orc_destroy(orc *o) {
+    if (!o) return;
+    void *ptrs[] = {o->x, o->y, o->z, o->vol, o->ie1, o->ie2, o->snx, o->sny, o->snz, o->kb1, o->kb2,
+                    o->sbx, o->sby, o->sbz, o->ibn, o->ibt, o->sbbx, o->sbby, o->sbbz, o->anx, o->any,
+                    o->anz, o->ic1, o->ic2, o->ic2a, o->ic2b, o->ic4[0], o->ic4[1], o->ic4[2], o->ic4[3],
+                    o->timestp, o->cosa, o->gmm, o->ue, o->ve, o->up, o->dn, o->colstart, o->colnodes};
+    for (size_t i = 0; i < sizeof ptrs / sizeof ptrs[0]; ++i) free(ptrs[i]);
+    for (int k = 0; k < MPG_F_COUNT; ++k) free(o->f[k]);
+    free(o);
+}
