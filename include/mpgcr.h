@@ -159,6 +159,10 @@ typedef struct mpg_solver *mpg_handle;
  * (ref.f:2343-2641) and the static COMMON storage. */
 int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int device, mpg_handle *out);
 int mpg_destroy(mpg_handle h);
+/* Host-only check of a mesh: runs the prism-column detection of mpg_create without touching a
+ * GPU and fills npoin, nedge, ncol, nedge2d and nlev of `info` (device_bytes = 0; precision =
+ * 1 when per-node sums can follow the reference's edge order exactly, else 0). */
+int mpg_analyze_mesh(const mpg_mesh_ref *mesh, mpg_info *info);
 const char *mpg_last_error(void);
 int mpg_get_info(mpg_handle h, mpg_info *info);
 

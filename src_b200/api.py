@@ -1,0 +1,200 @@
+"""Python host side of the C ABI (include/mpgcr.h): one `Solver` per GPU-resident run.
+
+Method names and argument meaning follow the reference subroutines of
+lippsLFroude_implgwopks3D_unstr3.f: ``gcrk`` (ref.f:1776), ``prfr`` (ref.f:1536),
+``laplc`` (ref.f:1288), ``div`` (ref.f:2096), ``derivative`` (ref.f:3943), ``precon``
+(ref.f:482), ``bcv`` (ref.f:1583), ``mpdatamper`` (ref.f:3617), ``courant`` (ref.f:1974),
+``stats`` (ref.f:2847), and the driver ``mpsolver`` split into ``setup`` (ref.f:99-273) and
+``step`` (one DO ITIME pass, ref.f:285-463).  Arrays passed in or out are in the reference
+node order.  The CUDA library must be built (``__graft_entry__.build()``); there is no CPU
+fallback — a missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import cabi
+from .cabi import MeshMarshal, MpgDiag, MpgGcrStats, MpgInfo, RunParams
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libmpgcr.so")
+_lib = None
+
+EXPORTS = [
+    "mpg_create", "mpg_destroy", "mpg_last_error", "mpg_get_info", "mpg_set_field", "mpg_get_field",
+    "mpg_derivative", "mpg_bcv", "mpg_laplc", "mpg_prfr", "mpg_div", "mpg_precon", "mpg_gcrk",
+    "mpg_mpdatamper", "mpg_courant", "mpg_stats", "mpg_setup", "mpg_step", "mpg_half_forcing",
+    "mpg_explicit_forcing", "mpg_post_solve", "mpg_extrapolate", "mpg_get_gcr_stats",
+    "mpg_synchronize", "mpg_analyze_mesh",
+]
+
+
+class MpgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"mpgcr error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load libmpgcr.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise RuntimeError(f"CUDA library {LIBPATH} not built; run __graft_entry__.build()")
+        L = C.CDLL(LIBPATH)
+        vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+        L.mpg_last_error.restype = C.c_char_p
+        L.mpg_create.argtypes = [vp, vp, ip, C.POINTER(vp)]
+        L.mpg_destroy.argtypes = [vp]
+        L.mpg_get_info.argtypes = [vp, vp]
+        L.mpg_set_field.argtypes = [vp, ip, vp]
+        L.mpg_get_field.argtypes = [vp, ip, vp]
+        L.mpg_derivative.argtypes = [vp, ip, ip, ip]
+        L.mpg_bcv.argtypes = [vp, ip, ip, ip, dp]
+        L.mpg_laplc.argtypes = [vp, ip, ip, ip]
+        L.mpg_prfr.argtypes = [vp] + [ip] * 8
+        L.mpg_div.argtypes = [vp, ip, ip, ip, ip, ip, vp]
+        L.mpg_precon.argtypes = [vp, ip, ip, ip, ip, ip]
+        L.mpg_gcrk.argtypes = [vp] + [ip] * 8 + [vp]
+        L.mpg_mpdatamper.argtypes = [vp, ip, ip]
+        L.mpg_courant.argtypes = [vp, ip, vp]
+        L.mpg_stats.argtypes = [vp, vp]
+        L.mpg_setup.argtypes = [vp, vp]
+        L.mpg_step.argtypes = [vp, vp]
+        for nm in ("mpg_half_forcing", "mpg_extrapolate", "mpg_synchronize"):
+            getattr(L, nm).argtypes = [vp]
+        for nm in ("mpg_explicit_forcing", "mpg_post_solve"):
+            getattr(L, nm).argtypes = [vp, ip]
+        L.mpg_get_gcr_stats.argtypes = [vp, vp]
+        L.mpg_analyze_mesh.argtypes = [vp, vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise MpgError(rc, lib().mpg_last_error().decode())
+
+
+def analyze_mesh(refmesh) -> dict:
+    """Prism-column analysis of a mesh on the host (no GPU needed)."""
+    mm = MeshMarshal(refmesh)
+    i = MpgInfo()
+    _check(lib().mpg_analyze_mesh(C.byref(mm.c), C.byref(i)))
+    d = {k: getattr(i, k) for k, _ in MpgInfo._fields_}
+    d["bitwise_order"] = bool(d.pop("precision"))
+    d.pop("device_bytes")
+    return d
+
+
+class Solver:
+    """A run on one GPU: mesh uploaded once, fields resident, reference subroutines as methods."""
+
+    def __init__(self, params: RunParams, refmesh, device: int = 0):
+        self.params = params
+        self.n = refmesh.npoin
+        self._mm = MeshMarshal(refmesh)
+        self._cp = params.to_c()
+        self.L = lib()
+        h = C.c_void_p()
+        _check(self.L.mpg_create(C.byref(self._cp), C.byref(self._mm.c), device, C.byref(h)))
+        self.h = h
+        self._mm = None          # the library keeps its own copy
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mpg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---------------------------------------------------------------- fields
+    def set(self, fid: int, values) -> None:
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), (self.n,)))
+        _check(self.L.mpg_set_field(self.h, fid, a.ctypes.data))
+
+    def get(self, fid: int) -> np.ndarray:
+        out = np.empty(self.n)
+        _check(self.L.mpg_get_field(self.h, fid, out.ctypes.data))
+        return out
+
+    def info(self) -> dict:
+        i = MpgInfo()
+        _check(self.L.mpg_get_info(self.h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in MpgInfo._fields_}
+
+    # ---------------------------------------------------------------- subroutines (field ids)
+    def derivative(self, unk: int, out: int, idx: int) -> None:
+        _check(self.L.mpg_derivative(self.h, unk, out, idx))
+
+    def bcv(self, u: int, v: int, w: int, flag: float) -> None:
+        _check(self.L.mpg_bcv(self.h, u, v, w, flag))
+
+    def laplc(self, press: int, alap: int, impfl: int) -> None:
+        _check(self.L.mpg_laplc(self.h, press, alap, impfl))
+
+    def prfr(self, press, ustr, vstr, wstr, uout, vout, wout, impfl) -> None:
+        _check(self.L.mpg_prfr(self.h, press, ustr, vstr, wstr, uout, vout, wout, impfl))
+
+    def div(self, ua, va, wa, rhs, iflg) -> MpgDiag:
+        d = MpgDiag()
+        _check(self.L.mpg_div(self.h, ua, va, wa, rhs, iflg, C.byref(d)))
+        return d
+
+    def precon(self, rhs, p, r, iprc, impfl) -> None:
+        _check(self.L.mpg_precon(self.h, rhs, p, r, iprc, impfl))
+
+    def gcrk(self, p, u1, v1, w1, u2, v2, w2, impfl) -> MpgGcrStats:
+        st = MpgGcrStats()
+        _check(self.L.mpg_gcrk(self.h, p, u1, v1, w1, u2, v2, w2, impfl, C.byref(st)))
+        return st
+
+    def mpdatamper(self, unk: int, iflag: int) -> None:
+        _check(self.L.mpg_mpdatamper(self.h, unk, iflag))
+
+    def courant(self, iflag: int = 1) -> MpgDiag:
+        d = MpgDiag()
+        _check(self.L.mpg_courant(self.h, iflag, C.byref(d)))
+        return d
+
+    def stats(self) -> MpgDiag:
+        d = MpgDiag()
+        _check(self.L.mpg_stats(self.h, C.byref(d)))
+        return d
+
+    def gcr_stats(self) -> MpgGcrStats:
+        st = MpgGcrStats()
+        _check(self.L.mpg_get_gcr_stats(self.h, C.byref(st)))
+        return st
+
+    # ---------------------------------------------------------------- driver
+    def setup(self) -> MpgDiag:
+        d = MpgDiag()
+        _check(self.L.mpg_setup(self.h, C.byref(d)))
+        return d
+
+    def step(self, diag: bool = True) -> MpgDiag:
+        d = MpgDiag()
+        _check(self.L.mpg_step(self.h, C.byref(d) if diag else None))
+        return d
+
+    def synchronize(self) -> None:
+        _check(self.L.mpg_synchronize(self.h))
+
+
+# convenience re-exports of the field ids
+F_UNK, F_UNK1, F_UUU, F_UUU0, F_FRC, F_UNKDASH = (cabi.F_UNK, cabi.F_UNK1, cabi.F_UUU, cabi.F_UUU0,
+                                                 cabi.F_FRC, cabi.F_UNKDASH)
+F_PRPOT, F_RHS, F_COUR, F_ALPHA, F_COEFW, F_RH0 = (cabi.F_PRPOT, cabi.F_RHS, cabi.F_COUR, cabi.F_ALPHA,
+                                                   cabi.F_COEFW, cabi.F_RH0)
+F_WORK = cabi.F_WORK

@@ -1,0 +1,892 @@
+// C ABI of the B200 MPDATA + GCR library (include/mpgcr.h): handle, field storage, the
+// reference subroutines on device-resident fields, and the mpsolver driver.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "mpdata.cuh"
+#include "mpgcr_internal.h"
+
+using namespace mpgk;
+
+// ------------------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+void mpg_set_error(const std::string &msg) { g_err = msg; }
+int mpg_fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+extern "C" const char *mpg_last_error(void) { return g_err.c_str(); }
+
+// ------------------------------------------------------------------------------ handle
+struct mpg_solver {
+    mpg_params P{};
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    int32_t NC = 0, L = 0, N = 0, NE2 = 0;
+    bool bitwise = true;
+    ColMesh M{};
+    std::vector<void *> allocs;
+    size_t dev_bytes = 0;
+    int32_t *d_perm = nullptr, *d_iperm = nullptr;
+    int32_t *d_e2a = nullptr, *d_e2b = nullptr;
+    double *f[MPG_F_COUNT] = {};
+    double *vol = nullptr, *ue = nullptr, *ve = nullptr, *stage = nullptr;
+    // GCR workspace
+    double *r = nullptr, *qr = nullptr, *ar = nullptr, *x[MPG_MAX_LORD] = {}, *ax[MPG_MAX_LORD] = {};
+    double *F[3] = {}, *tres = nullptr;
+    double *scal = nullptr, *part = nullptr, *result = nullptr, *h_res = nullptr;
+    unsigned int *counter = nullptr;
+    // line preconditioner
+    double *la[2] = {}, *lm[2] = {}, *lcp[2] = {};
+    // MPDATA scratch
+    MpScratch S{};
+    double *psi1 = nullptr, *g3[3] = {}, *mx = nullptr, *mn = nullptr;
+    // /itero/
+    int32_t niter = 0, nitsm = 0, icount = 0, gstatus = 0;
+    double eer = 0., eem = 0., dvmx_last = 0., rl2_last = 0.;
+    double betaunstr1 = 0.;
+    HostStatic hs;
+    std::vector<int32_t> iperm;
+};
+
+namespace {
+
+template <class T>
+int dalloc(mpg_handle h, T **p, size_t n, bool zero = true) {
+    size_t bytes = sizeof(T) * (n ? n : 1);
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) return mpg_fail(MPG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    h->allocs.push_back(*p);
+    h->dev_bytes += bytes;
+    if (zero) MPG_CUDA(cudaMemsetAsync(*p, 0, bytes, h->st));
+    return MPG_OK;
+}
+
+template <class T>
+int upload(mpg_handle h, T **p, const std::vector<T> &v) {
+    int rc = dalloc(h, p, v.size(), false);
+    if (rc) return rc;
+    MPG_CUDA(cudaMemcpyAsync(*p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, h->st));
+    return MPG_OK;
+}
+
+inline int grid(int n) { return (n + kThreads - 1) / kThreads; }
+
+// field pointer, allocated (zeroed) on first use
+double *fld(mpg_handle h, int fid) {
+    if (fid < 0 || fid >= MPG_F_COUNT) return nullptr;
+    if (fid >= MPG_F_UNK + 4 + h->P.nscal && fid < MPG_F_UNK1) return nullptr;
+    if (!h->f[fid]) {
+        if (dalloc(h, &h->f[fid], (size_t)h->N)) return nullptr;
+    }
+    return h->f[fid];
+}
+
+#define FLD(var, fid)                                                                      \
+    double *var = fld(h, (fid));                                                           \
+    if (!var) return mpg_fail(MPG_ERR_ARG, "invalid or unallocatable field id " + std::to_string(fid));
+
+int check_launch(const char *what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return mpg_fail(MPG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return MPG_OK;
+}
+
+// generic deterministic reduction launcher
+template <int NQ, class Prod, class Fin>
+int reduce(mpg_handle h, unsigned kinds, Prod prod, Fin fin) {
+    k_reduce<NQ><<<kRedBlocks, kRedThreads, 0, h->st>>>(h->N, kinds, prod, fin, h->part, h->counter, h->result);
+    return check_launch("k_reduce");
+}
+
+int fetch_result(mpg_handle h, int nq) {
+    MPG_CUDA(cudaMemcpyAsync(h->h_res, h->result, sizeof(double) * nq, cudaMemcpyDeviceToHost, h->st));
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    return MPG_OK;
+}
+
+// ------------------------------------------------------------------------------ operators
+int op_laplc(mpg_handle h, const double *p, double *alap, int impfl) {
+    k_lap_grad<<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW], h->ue,
+                                                   h->P.delt, impfl, h->F[0], h->F[1], h->F[2]);
+    k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, h->F[0], h->F[1], h->F[2], h->vol, h->f[MPG_F_RH0], alap);
+    return check_launch("laplc");
+}
+
+int op_prfr(mpg_handle h, const double *p, const double *us, const double *vs, const double *ws, double *uo,
+            double *vo, double *wo, int impfl) {
+    k_prfr<<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, us, vs, ws, h->vol, h->f[MPG_F_COEFW], h->ue, h->P.delt,
+                                               impfl, uo, vo, wo);
+    return check_launch("prfr");
+}
+
+int op_div(mpg_handle h, const double *ua, const double *va, const double *wa, double *rhs, int iflg) {
+    k_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, ua, va, wa, h->vol, h->f[MPG_F_RH0], iflg, rhs);
+    return check_launch("div");
+}
+
+int op_line(mpg_handle h, const double *rhs, double *p, int impfl, int acc) {
+    const int q = impfl ? 1 : 0;
+    const int nblk = (h->NC + 32 * kLineWarps - 1) / (32 * kLineWarps);
+    const size_t smem = sizeof(double) * 32 * kLineWarps * h->L;
+    k_line_solve<<<nblk, 32 * kLineWarps, smem, h->st>>>(h->NC, h->L, rhs, h->la[q], h->lm[q], h->lcp[q],
+                                                          h->P.omega, acc, p);
+    return check_launch("line_solve");
+}
+
+// precon(rhs, p, r, iprc, elas, impfl), mg_flag = 0 (ref.f:482-753); `zero_r` restores the
+// reference's clearing of r when a caller may look at it.
+int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, int impfl, bool zero_r) {
+    const int N = h->N;
+    if (iprc == 0) {
+        k_copy<<<grid(N), kThreads, 0, h->st>>>(N, rhs, p);
+        return check_launch("precon copy");
+    }
+    if (zero_r) k_fill<<<grid(N), kThreads, 0, h->st>>>(N, r, 0.0);
+    if (iprc == 2) {
+        for (int it = 1; it <= h->P.itrp1; ++it) {
+            if (it == 1) {
+                int rc = op_line(h, rhs, p, impfl, 0);
+                if (rc) return rc;
+            } else {
+                int rc = op_laplc(h, p, r, impfl);
+                if (rc) return rc;
+                k_sub<<<grid(N), kThreads, 0, h->st>>>(N, rhs, r, h->tres);
+                rc = op_line(h, h->tres, p, impfl, 1);
+                if (rc) return rc;
+            }
+        }
+        if (h->P.itrp1 < 1) k_fill<<<grid(N), kThreads, 0, h->st>>>(N, p, 0.0);
+        return check_launch("precon line");
+    }
+    if (iprc != 1) return mpg_fail(MPG_ERR_UNSUPPORTED, "iprc must be 0, 1 or 2");
+    // reference smoother: the first sweep starts from p = 0, where laplc(0) = 0 exactly
+    k_fill<<<grid(N), kThreads, 0, h->st>>>(N, p, 0.0);
+    if (!zero_r) k_fill<<<grid(N), kThreads, 0, h->st>>>(N, r, 0.0);
+    for (int it = 1; it <= h->P.itrp1; ++it) {
+        if (it > 1) {
+            int rc = op_laplc(h, p, r, impfl);
+            if (rc) return rc;
+        }
+        k_smooth<<<grid(N), kThreads, 0, h->st>>>(N, h->P.sm_flag1, h->P.omega, h->betaunstr1,
+                                                  h->f[MPG_F_D1], r, rhs, p);
+    }
+    return check_launch("precon smoother");
+}
+
+// ------------------------------------------------------------------------------ GCR
+struct FinEps {   // eer0, eem0, rl20 clamped by epa
+    double *scal;
+    __device__ void operator()(const double *v) const {
+        const double epa = 1.e-38;
+        scal[S_EER0] = amax(v[0], epa);
+        scal[S_EEM0] = amax(v[1], epa);
+        scal[S_RL20] = amax(v[2], epa);
+    }
+};
+struct FinBeta {
+    double *scal;
+    int i;
+    __device__ void operator()(const double *v) const {
+        const double ax2 = amax(1.e-38, v[1]);
+        scal[S_AX2 + i] = ax2;
+        scal[S_BETA] = -v[0] / ax2;
+    }
+};
+struct FinDel {
+    double *scal;
+    int i;
+    __device__ void operator()(const double *v) const {
+        for (int ii = 0; ii < i; ++ii) scal[S_DEL + ii] = -v[ii] / scal[S_AX2 + ii];
+    }
+};
+struct ProdNorm0 {
+    const double *qr, *r;
+    __device__ void operator()(int n, double *v) const {
+        const double q = qr[n], s = r[n];
+        v[0] = q * q;
+        v[1] = fabs(q);
+        v[2] = s * s;
+    }
+};
+struct ProdDot2 {
+    const double *r, *a;
+    __device__ void operator()(int n, double *v) const {
+        const double x = a[n];
+        v[0] = r[n] * x;
+        v[1] = x * x;
+    }
+};
+struct ProdAxpy {   // p += beta x, r += beta ax; returns |r|, r^2
+    const double *scal, *x, *a;
+    double *p, *r;
+    __device__ void operator()(int n, double *v) const {
+        const double beta = scal[S_BETA];
+        p[n] = p[n] + beta * x[n];
+        const double rn = r[n] + beta * a[n];
+        r[n] = rn;
+        v[0] = fabs(rn);
+        v[1] = rn * rn;
+    }
+};
+template <int NQ>
+struct ProdDots {
+    const double *ar;
+    VecList ax;
+    int i;
+    __device__ void operator()(int n, double *v) const {
+        const double a = ar[n];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) v[q] = q < i ? ax.v[q][n] * a : 0.0;
+    }
+};
+struct ProdQ {
+    const double *qr;
+    __device__ void operator()(int n, double *v) const {
+        v[0] = qr[n] * qr[n];
+        v[1] = fabs(qr[n]);
+    }
+};
+
+int gcr_dots(mpg_handle h, int i) {
+    VecList ax{};
+    for (int q = 0; q < h->P.lord; ++q) ax.v[q] = h->ax[q];
+    FinDel fin{h->scal, i};
+    if (i <= 4) return reduce<4>(h, 0u, ProdDots<4>{h->ar, ax, i}, fin);
+    if (i <= 8) return reduce<8>(h, 0u, ProdDots<8>{h->ar, ax, i}, fin);
+    return reduce<16>(h, 0u, ProdDots<16>{h->ar, ax, i}, fin);
+}
+
+// gcrk(p, u1, v1, w1, u2, v2, w2, impfl) — ref.f:1776-1972
+int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const double *w1, double *u2,
+            double *v2, double *w2, int impfl) {
+    const mpg_params &P = h->P;
+    const int N = h->N, lord = P.lord, itmn = P.itmn > 0 ? P.itmn : 3;
+    const double eps = P.eps0 / P.delt, epa = 1.e-38;
+    int nlc = 0, rc;
+    if ((rc = op_prfr(h, p, u1, v1, w1, u2, v2, w2, impfl))) return rc;
+    if ((rc = op_div(h, u2, v2, w2, h->r, -1))) return rc;
+    if ((rc = op_precon(h, h->r, h->qr, h->ar, P.iprc, impfl, false))) return rc;
+    if ((rc = reduce<3>(h, 0x2u, ProdNorm0{h->qr, h->r}, FinEps{h->scal}))) return rc;
+    if ((rc = fetch_result(h, 3))) return rc;
+    double rl20 = h->h_res[2] > epa ? h->h_res[2] : epa;
+    k_copy<<<grid(N), kThreads, 0, h->st>>>(N, h->qr, h->x[0]);
+    if ((rc = op_laplc(h, h->x[0], h->ax[0], impfl))) return rc;
+    int status = MPG_GCR_MAXIT;
+    double dvmx = 0., rl2 = 0.;
+    VecList xl{}, axl{};
+    for (int q = 0; q < lord; ++q) { xl.v[q] = h->x[q]; axl.v[q] = h->ax[q]; }
+    for (int it = 1; it <= P.itr && status == MPG_GCR_MAXIT; ++it) {
+        for (int i = 1; i <= lord; ++i) {
+            if ((rc = reduce<2>(h, 0u, ProdDot2{h->r, h->ax[i - 1]}, FinBeta{h->scal, i - 1}))) return rc;
+            if ((rc = reduce<2>(h, 0x1u, ProdAxpy{h->scal, h->x[i - 1], h->ax[i - 1], p, h->r}, NoFin{})))
+                return rc;
+            if ((rc = fetch_result(h, 2))) return rc;
+            dvmx = h->h_res[0] > -1.e15 ? h->h_res[0] : -1.e15;
+            rl2 = h->h_res[1];
+            if (!std::isfinite(dvmx) || !std::isfinite(rl2)) { status = MPG_GCR_NAN; break; }
+            if (dvmx <= eps && it >= itmn) { status = MPG_GCR_CONVERGED; break; }
+            if (rl2 >= rl20) { status = MPG_GCR_STALLED; break; }
+            rl20 = rl2 > epa ? rl2 : epa;
+            if ((rc = op_precon(h, h->r, h->qr, h->ar, P.iprc, impfl, false))) return rc;
+            if ((rc = op_laplc(h, h->qr, h->ar, impfl))) return rc;
+            nlc = nlc + 1;
+            if ((rc = gcr_dots(h, i))) return rc;
+            if (i < lord) {
+                k_gcr_next<<<grid(N), kThreads, 0, h->st>>>(N, i, h->scal, h->qr, h->ar, xl, axl, h->x[i], h->ax[i]);
+            } else {
+                k_gcr_restart<<<grid(N), kThreads, 0, h->st>>>(N, i, h->scal, h->qr, h->ar, xl, axl);
+            }
+            if ((rc = check_launch("gcr update"))) return rc;
+        }
+    }
+    if ((rc = reduce<2>(h, 0x2u, ProdQ{h->qr}, NoFin{}))) return rc;
+    if ((rc = fetch_result(h, 2))) return rc;
+    double eer = h->h_res[0], eem = h->h_res[1] > -1.e15 ? h->h_res[1] : -1.e15;
+    double s0[3];
+    MPG_CUDA(cudaMemcpyAsync(s0, h->scal + S_EER0, sizeof s0, cudaMemcpyDeviceToHost, h->st));
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    h->eer = eer / s0[0];
+    h->eem = eem / s0[1];
+    h->niter = nlc;
+    h->nitsm = h->nitsm + nlc;
+    h->icount = h->icount + 1;
+    h->gstatus = status;
+    h->dvmx_last = dvmx;
+    h->rl2_last = rl2;
+    return MPG_OK;
+}
+
+// ------------------------------------------------------------------------------ MPDATA
+int op_aun(mpg_handle h) {
+    U3 U{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}};
+    const int nt = h->NE2 * h->L + h->N;
+    k_aun<<<grid(nt), kThreads, 0, h->st>>>(h->M, h->S, U);
+    return check_launch("aun");
+}
+
+int op_mpdata_field(mpg_handle h, double *psi) {
+    const double dt = h->P.delt;
+    const double *vol = h->vol, *rh0 = h->f[MPG_F_RH0];
+    const int N = h->N;
+    k_mp_donor<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, psi, vol, rh0, dt, h->psi1);
+    k_mp_grad_bounds<<<grid(N), kThreads, 0, h->st>>>(h->M, h->psi1, h->g3[0], h->g3[1], h->g3[2], h->mx, h->mn);
+    AntiArgs A{h->psi1, h->g3[0], h->g3[1], h->g3[2], vol, rh0,
+               U3{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}}, dt};
+    const int nt = h->NE2 * h->L + h->N;
+    k_mp_anti<<<grid(nt), kThreads, 0, h->st>>>(h->M, h->S, A);
+    // cp, cn reuse the gradient buffers (dead after the antidiffusive fluxes)
+    k_mp_cpcn<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, h->psi1, h->mx, h->mn, vol, rh0, dt, h->g3[0], h->g3[1]);
+    k_mp_pass2<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, h->psi1, h->g3[0], h->g3[1], vol, rh0, dt, psi);
+    return check_launch("mpdata");
+}
+
+Fields make_fields(mpg_handle h) {
+    Fields F{};
+    for (int q = 0; q < 4; ++q) { F.unk[q] = fld(h, MPG_F_UNK + q); F.frc[q] = fld(h, MPG_F_FRC + q); }
+    for (int q = 0; q < 3; ++q) {
+        F.uuu[q] = fld(h, MPG_F_UUU + q);
+        F.uuu0[q] = fld(h, MPG_F_UUU0 + q);
+        F.ud[q] = fld(h, MPG_F_UNKDASH + q);
+        F.unk1[q] = fld(h, MPG_F_UNK1 + q);
+    }
+    F.rh0 = h->f[MPG_F_RH0]; F.th0 = h->f[MPG_F_TH0]; F.the = h->f[MPG_F_THE];
+    F.dthedz = h->f[MPG_F_DTHEDZ]; F.coefw = h->f[MPG_F_COEFW]; F.alpha = h->f[MPG_F_ALPHA];
+    F.ue = h->ue; F.ve = h->ve;
+    return F;
+}
+
+// ------------------------------------------------------------------------------ diagnostics
+struct ProdDivStats {
+    const double *rhs;
+    double dt;
+    __device__ void operator()(int n, double *v) const {
+        const double x = rhs[n] * dt;
+        v[0] = x; v[1] = -x; v[2] = x;
+    }
+};
+struct ProdSqDev {
+    const double *a;
+    double scale, mean;
+    __device__ void operator()(int n, double *v) const {
+        const double t = a[n] * scale - mean;
+        v[0] = t * t;
+    }
+};
+struct ProdCour {
+    const double *c;
+    __device__ void operator()(int n, double *v) const {
+        v[0] = c[n]; v[1] = c[n]; v[2] = -c[n];
+    }
+};
+struct ProdArg {
+    const double *c;
+    const int32_t *iperm;
+    double mx;
+    __device__ void operator()(int n, double *v) const { v[0] = c[n] == mx ? (double)iperm[n] : -1.0; }
+};
+struct ProdStats1 {
+    const double *rh0, *vol;
+    const double *u[8];
+    int nf;
+    __device__ void operator()(int n, double *v) const {
+        const double r = rh0[n], vr = vol[n] * r;
+        v[0] = r;
+        for (int q = 0; q < 4; ++q) {
+            const double x = u[q][n];
+            v[1 + q] = r * x;
+            v[5 + q] = x;
+            v[9 + q] = -x;
+        }
+        for (int q = 0; q < 8; ++q) v[13 + q] = q < nf ? vr * u[q][n] : 0.0;
+    }
+};
+struct ProdStats2 {
+    const double *rh0;
+    const double *u[4];
+    double av[4];
+    __device__ void operator()(int n, double *v) const {
+        const double r = rh0[n];
+        for (int q = 0; q < 4; ++q) {
+            const double t = u[q][n] - av[q];
+            v[q] = r * (t * t);
+        }
+    }
+};
+struct ProdScal {
+    const double *u[4];
+    int ns;
+    __device__ void operator()(int n, double *v) const {
+        for (int q = 0; q < 4; ++q) {
+            const double x = q < ns ? u[q][n] : 0.0;
+            v[q] = -x;
+            v[4 + q] = x;
+        }
+    }
+};
+
+int diag_div(mpg_handle h, const double *rhs, mpg_diag *d) {
+    int rc;
+    const double dt = h->P.delt;
+    if ((rc = reduce<3>(h, 0x3u, ProdDivStats{rhs, dt}, NoFin{}))) return rc;
+    if ((rc = fetch_result(h, 3))) return rc;
+    double divmx = h->h_res[0] > -1.e15 ? h->h_res[0] : -1.e15;
+    double divmn = -h->h_res[1] < 1.e15 ? -h->h_res[1] : 1.e15;
+    double divav = h->h_res[2] / (double)h->N;
+    if ((rc = reduce<1>(h, 0u, ProdSqDev{rhs, dt, divav}, NoFin{}))) return rc;
+    if ((rc = fetch_result(h, 1))) return rc;
+    d->divmx = divmx; d->divmn = divmn; d->divav = divav;
+    d->divsd = std::sqrt(h->h_res[0] / h->N);
+    d->eer = h->eer; d->eem = h->eem; d->niter = h->niter;
+    d->nitav = h->nitsm / (h->icount > 1 ? h->icount : 1);
+    return MPG_OK;
+}
+
+int diag_courant(mpg_handle h, int iflag, mpg_diag *d) {
+    int rc;
+    U3 U{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}};
+    double *cour = fld(h, MPG_F_COUR);
+    k_courant<<<grid(h->N), kThreads, 0, h->st>>>(h->M, U, h->f[MPG_F_RH0], h->vol, h->P.delt, iflag, cour);
+    if ((rc = check_launch("courant"))) return rc;
+    if (!d) return MPG_OK;
+    if ((rc = reduce<3>(h, 0x6u, ProdCour{cour}, NoFin{}))) return rc;
+    if ((rc = fetch_result(h, 3))) return rc;
+    double crnav = h->h_res[0] / h->N;
+    double crnmx = h->h_res[1] > -1.e9 ? h->h_res[1] : -1.e9;
+    double crnmn = -h->h_res[2] < 1.e9 ? -h->h_res[2] : 1.e9;
+    if ((rc = reduce<1>(h, 0x1u, ProdArg{cour, h->d_iperm, crnmx}, NoFin{}))) return rc;
+    if ((rc = fetch_result(h, 1))) return rc;
+    const int ic = (int)h->h_res[0] + 1;
+    if ((rc = reduce<1>(h, 0u, ProdSqDev{cour, 1.0, crnav}, NoFin{}))) return rc;
+    if ((rc = fetch_result(h, 1))) return rc;
+    d->crnmx = crnmx; d->crnmn = crnmn; d->crnav = crnav;
+    d->crnsd = std::sqrt(h->h_res[0] / h->N);
+    d->icrnmx = ic;
+    return MPG_OK;
+}
+
+// stats(unk) (ref.f:2847-2912) plus the FP64 mass sums and scalar extrema
+int diag_stats(mpg_handle h, mpg_diag *d) {
+    int rc;
+    ProdStats1 p1{};
+    p1.rh0 = h->f[MPG_F_RH0];
+    p1.vol = h->vol;
+    const int nf = 4 + h->P.nscal < 8 ? 4 + h->P.nscal : 8;
+    for (int q = 0; q < 8; ++q) p1.u[q] = q < nf ? fld(h, MPG_F_UNK + q) : nullptr;
+    p1.nf = nf;
+    if ((rc = reduce<21>(h, 0x1FE0u, p1, NoFin{}))) return rc;
+    if ((rc = fetch_result(h, 21))) return rc;
+    double res[21];
+    std::memcpy(res, h->h_res, sizeof res);
+    const double rav = res[0];
+    ProdStats2 p2{};
+    p2.rh0 = h->f[MPG_F_RH0];
+    for (int q = 0; q < 4; ++q) { p2.u[q] = p1.u[q]; p2.av[q] = res[1 + q] / rav; }
+    if ((rc = reduce<4>(h, 0u, p2, NoFin{}))) return rc;
+    if ((rc = fetch_result(h, 4))) return rc;
+    for (int q = 0; q < 4; ++q) {
+        const double mx = res[5 + q] > -1.e10 ? res[5 + q] : -1.e10;
+        const double mn = -res[9 + q] < 1.e10 ? -res[9 + q] : 1.e10;
+        const double sd = q < 3 ? std::sqrt(h->h_res[q] / rav) : std::sqrt(h->h_res[q] / h->N);
+        d->stats[4 * q + 0] = mx; d->stats[4 * q + 1] = mn;
+        d->stats[4 * q + 2] = p2.av[q]; d->stats[4 * q + 3] = sd;
+    }
+    for (int q = 0; q < 8; ++q) d->mass[q] = q < nf ? res[13 + q] : 0.0;
+    const int ns = h->P.nscal < 4 ? h->P.nscal : 4;
+    if (ns > 0) {
+        ProdScal ps{};
+        for (int q = 0; q < 4; ++q) ps.u[q] = q < ns ? fld(h, MPG_F_UNK + 4 + q) : p1.u[0];
+        ps.ns = ns;
+        if ((rc = reduce<8>(h, 0xFFu, ps, NoFin{}))) return rc;
+        if ((rc = fetch_result(h, 8))) return rc;
+        for (int q = 0; q < ns; ++q) { d->smin[q] = -h->h_res[q]; d->smax[q] = h->h_res[4 + q]; }
+    }
+    return MPG_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------ lifecycle
+extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int device, mpg_handle *out) {
+    if (!prm || !mesh || !out) return mpg_fail(MPG_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (prm->isfera != 0) return mpg_fail(MPG_ERR_UNSUPPORTED, "isfera=1 (spherical variant) is not provided");
+    if (prm->iper != 2 && prm->iper != 0) return mpg_fail(MPG_ERR_ARG, "iper must be 0 or 2");
+    if (prm->mg_flag != 0) return mpg_fail(MPG_ERR_UNSUPPORTED, "mg_flag=1 (multigrid V-cycle) is not provided");
+    if (prm->ielast != 0) return mpg_fail(MPG_ERR_UNSUPPORTED, "ielast=1 is not provided");
+    if (prm->lord < 1 || prm->lord > MPG_MAX_LORD) return mpg_fail(MPG_ERR_ARG, "lord out of range 1..16");
+    if (prm->nscal < 0 || 4 + prm->nscal > MPG_MAX_UNK) return mpg_fail(MPG_ERR_ARG, "nscal out of range 0..12");
+    if (prm->delt <= 0) return mpg_fail(MPG_ERR_ARG, "delt must be positive");
+    if (prm->iprc < 0 || prm->iprc > 2) return mpg_fail(MPG_ERR_ARG, "iprc must be 0, 1 or 2");
+    if (prm->precision != MPG_PREC_FP64 && prm->precision != MPG_PREC_MIXED)
+        return mpg_fail(MPG_ERR_ARG, "precision must be MPG_PREC_FP64 or MPG_PREC_MIXED");
+    HostColumnMesh hm;
+    int rc = mpg_build_column_mesh(mesh, &hm);
+    if (rc) return rc;
+    mpg_solver *h = new mpg_solver();
+    h->P = *prm;
+    h->dev = device;
+    rc = mpg_host_static(prm, mesh, hm, &h->hs);
+    if (rc) { delete h; return rc; }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { delete h; return mpg_fail(MPG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e)); }
+    e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete h; return mpg_fail(MPG_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e)); }
+    h->NC = hm.NC; h->L = hm.L; h->N = hm.N; h->NE2 = hm.NE2;
+    h->bitwise = hm.bitwise_order;
+    h->betaunstr1 = h->hs.betaunstr1;
+    h->iperm = hm.iperm;
+    auto fail = [&](int code) { mpg_destroy(h); return code; };
+    // mesh
+    ColMesh &M = h->M;
+    M.NC = hm.NC; M.L = hm.L; M.N = hm.N; M.NE2 = hm.NE2; M.iper = prm->iper;
+    int32_t *cptr, *bptr;
+    int2 *cadj;
+    BEntry *bent;
+    if ((rc = upload(h, &cptr, hm.cptr)) || (rc = upload(h, &cadj, hm.cadj)) || (rc = upload(h, &bptr, hm.bptr)))
+        return fail(rc);
+    std::vector<BEntry> be = hm.bent;
+    if (be.empty()) be.push_back(BEntry{});
+    if ((rc = upload(h, &bent, be))) return fail(rc);
+    M.cptr = cptr; M.cadj = cadj; M.bptr = bptr; M.bent = bent;
+    for (int d = 0; d < 3; ++d) {
+        double *a, *b;
+        if ((rc = upload(h, &a, hm.Sh[d])) || (rc = upload(h, &b, hm.Sv[d]))) return fail(rc);
+        M.Sh[d] = a; M.Sv[d] = b;
+    }
+    if ((rc = upload(h, &h->d_perm, hm.perm)) || (rc = upload(h, &h->d_e2a, hm.e2a)) ||
+        (rc = upload(h, &h->d_e2b, hm.e2b)))
+        return fail(rc);
+    if ((rc = upload(h, &h->vol, hm.vol)) || (rc = upload(h, &h->ue, h->hs.ue)) || (rc = upload(h, &h->ve, h->hs.ve)))
+        return fail(rc);
+    // static fields
+    struct { int fid; std::vector<double> *v; } stat[] = {
+        {MPG_F_RH0, &h->hs.rh0}, {MPG_F_TH0, &h->hs.th0}, {MPG_F_THE, &h->hs.the},
+        {MPG_F_DTHEDZ, &h->hs.dthedz}, {MPG_F_ALPHA, &h->hs.alpha}, {MPG_F_COEFW, &h->hs.coefw},
+        {MPG_F_D1, &h->hs.d1}};
+    for (auto &s : stat)
+        if ((rc = upload(h, &h->f[s.fid], *s.v))) return fail(rc);
+    for (int q = 0; q < 2; ++q)
+        if ((rc = upload(h, &h->la[q], h->hs.la[q])) || (rc = upload(h, &h->lm[q], h->hs.lm[q])) ||
+            (rc = upload(h, &h->lcp[q], h->hs.lcp[q])))
+            return fail(rc);
+    // workspace
+    const size_t N = h->N;
+    if ((rc = dalloc(h, &h->stage, N)) || (rc = dalloc(h, &h->r, N)) || (rc = dalloc(h, &h->qr, N)) ||
+        (rc = dalloc(h, &h->ar, N)) || (rc = dalloc(h, &h->tres, N)))
+        return fail(rc);
+    for (int q = 0; q < 3; ++q)
+        if ((rc = dalloc(h, &h->F[q], N))) return fail(rc);
+    for (int q = 0; q < prm->lord; ++q)
+        if ((rc = dalloc(h, &h->x[q], N)) || (rc = dalloc(h, &h->ax[q], N))) return fail(rc);
+    if ((rc = dalloc(h, &h->scal, S_COUNT)) || (rc = dalloc(h, &h->part, (size_t)kRedBlocks * kMaxQ)) ||
+        (rc = dalloc(h, &h->result, kMaxQ)) || (rc = dalloc(h, &h->counter, 1)))
+        return fail(rc);
+    e = cudaMallocHost((void **)&h->h_res, sizeof(double) * kMaxQ);
+    if (e != cudaSuccess) return fail(mpg_fail(MPG_ERR_NOMEM, "cudaMallocHost"));
+    // MPDATA scratch
+    const size_t nh = (size_t)h->NE2 * h->L;
+    double *aunh, *aunv, *Ah, *Av;
+    if ((rc = dalloc(h, &aunh, nh)) || (rc = dalloc(h, &aunv, N)) || (rc = dalloc(h, &Ah, nh)) ||
+        (rc = dalloc(h, &Av, N)) || (rc = dalloc(h, &h->psi1, N)) || (rc = dalloc(h, &h->mx, N)) ||
+        (rc = dalloc(h, &h->mn, N)))
+        return fail(rc);
+    for (int q = 0; q < 3; ++q)
+        if ((rc = dalloc(h, &h->g3[q], N))) return fail(rc);
+    h->S = MpScratch{aunh, aunv, Ah, Av, h->d_e2a, h->d_e2b};
+    if ((rc = upload(h, &h->d_iperm, hm.iperm))) return fail(rc);
+    // the column solve stages 32*kLineWarps columns of L levels; the attribute only ever grows,
+    // so handles with fewer levels keep working
+    const size_t smem = sizeof(double) * 32 * kLineWarps * h->L;
+    cudaFuncAttributes fa{};
+    e = cudaFuncGetAttributes(&fa, k_line_solve);
+    if (e == cudaSuccess && (size_t)fa.maxDynamicSharedSizeBytes < smem)
+        e = cudaFuncSetAttribute(k_line_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(mpg_fail(MPG_ERR_MESH, "too many levels for the column solve's shared memory"));
+    e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) return fail(mpg_fail(MPG_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e)));
+    *out = h;
+    return MPG_OK;
+}
+
+extern "C" int mpg_destroy(mpg_handle h) {
+    if (!h) return MPG_OK;
+    if (h->st) cudaStreamSynchronize(h->st);
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->h_res) cudaFreeHost(h->h_res);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+    return MPG_OK;
+}
+
+extern "C" int mpg_get_info(mpg_handle h, mpg_info *info) {
+    if (!h || !info) return mpg_fail(MPG_ERR_ARG, "null argument");
+    info->npoin = h->N;
+    info->nedge = (int64_t)h->NE2 * h->L + (int64_t)h->NC * (h->L - 1);
+    info->ncol = h->NC;
+    info->nedge2d = h->NE2;
+    info->nlev = h->L;
+    info->precision = h->P.precision;
+    info->device_bytes = (int64_t)h->dev_bytes;
+    return MPG_OK;
+}
+
+extern "C" int mpg_set_field(mpg_handle h, int fid, const double *src) {
+    if (!h || !src) return mpg_fail(MPG_ERR_ARG, "null argument");
+    FLD(dst, fid);
+    MPG_CUDA(cudaMemcpyAsync(h->stage, src, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->st));
+    k_scatter_perm<<<grid(h->N), kThreads, 0, h->st>>>(h->N, h->d_perm, h->stage, dst);
+    int rc = check_launch("set_field");
+    if (rc) return rc;
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    return MPG_OK;
+}
+
+extern "C" int mpg_get_field(mpg_handle h, int fid, double *dst) {
+    if (!h || !dst) return mpg_fail(MPG_ERR_ARG, "null argument");
+    FLD(src, fid);
+    k_gather_perm<<<grid(h->N), kThreads, 0, h->st>>>(h->N, h->d_perm, src, h->stage);
+    int rc = check_launch("get_field");
+    if (rc) return rc;
+    MPG_CUDA(cudaMemcpyAsync(dst, h->stage, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->st));
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    return MPG_OK;
+}
+
+extern "C" int mpg_derivative(mpg_handle h, int unk, int out, int idx) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (idx < 1 || idx > 3) return mpg_fail(MPG_ERR_ARG, "idx must be 1, 2 or 3");
+    FLD(a, unk);
+    FLD(b, out);
+    if (a == b) return mpg_fail(MPG_ERR_ARG, "derivative: input and output must differ");
+    k_derivative<<<grid(h->N), kThreads, 0, h->st>>>(h->M, a, b, idx);
+    return check_launch("derivative");
+}
+
+extern "C" int mpg_bcv(mpg_handle h, int u, int v, int w, double flag) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    FLD(a, u);
+    FLD(b, v);
+    FLD(c, w);
+    k_bcv<<<grid(h->N), kThreads, 0, h->st>>>(h->M, a, b, c, h->ue, flag);
+    return check_launch("bcv");
+}
+
+extern "C" int mpg_laplc(mpg_handle h, int press, int alap, int impfl) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    FLD(a, press);
+    FLD(b, alap);
+    if (a == b) return mpg_fail(MPG_ERR_ARG, "laplc: input and output must differ");
+    return op_laplc(h, a, b, impfl);
+}
+
+extern "C" int mpg_prfr(mpg_handle h, int press, int ustr, int vstr, int wstr, int uout, int vout, int wout,
+                        int impfl) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    FLD(p, press);
+    FLD(us, ustr);
+    FLD(vs, vstr);
+    FLD(ws, wstr);
+    FLD(uo, uout);
+    FLD(vo, vout);
+    FLD(wo, wout);
+    if (p == uo || p == vo || p == wo) return mpg_fail(MPG_ERR_ARG, "prfr: press must not alias an output");
+    return op_prfr(h, p, us, vs, ws, uo, vo, wo, impfl);
+}
+
+extern "C" int mpg_div(mpg_handle h, int ua, int va, int wa, int rhs, int iflg, mpg_diag *diag) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (iflg != 1 && iflg != -1) return mpg_fail(MPG_ERR_ARG, "iflg must be 1 or -1");
+    FLD(a, ua);
+    FLD(b, va);
+    FLD(c, wa);
+    FLD(r, rhs);
+    if (r == a || r == b || r == c) return mpg_fail(MPG_ERR_ARG, "div: rhs must not alias an input");
+    int rc = op_div(h, a, b, c, r, iflg);
+    if (rc) return rc;
+    if (iflg == 1 && diag) return diag_div(h, r, diag);
+    return MPG_OK;
+}
+
+extern "C" int mpg_precon(mpg_handle h, int rhs, int p, int r, int iprc, int impfl) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    FLD(a, rhs);
+    FLD(b, p);
+    FLD(c, r);
+    if (a == b || a == c || b == c) return mpg_fail(MPG_ERR_ARG, "precon: arguments must be distinct fields");
+    return op_precon(h, a, b, c, iprc, impfl, true);
+}
+
+static void fill_stats(mpg_handle h, mpg_gcr_stats *st) {
+    std::memset(st, 0, sizeof(*st));
+    st->niter = h->niter; st->nitsm = h->nitsm; st->icount = h->icount; st->status = h->gstatus;
+    st->eer = h->eer; st->eem = h->eem; st->dvmx = h->dvmx_last; st->rl2 = h->rl2_last;
+}
+
+extern "C" int mpg_gcrk(mpg_handle h, int p, int u1, int v1, int w1, int u2, int v2, int w2, int impfl,
+                        mpg_gcr_stats *stats) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    FLD(pp, p);
+    FLD(a1, u1);
+    FLD(b1, v1);
+    FLD(c1, w1);
+    FLD(a2, u2);
+    FLD(b2, v2);
+    FLD(c2, w2);
+    int rc = op_gcrk(h, pp, a1, b1, c1, a2, b2, c2, impfl);
+    if (rc) return rc;
+    if (stats) fill_stats(h, stats);
+    if (h->gstatus == MPG_GCR_NAN) return mpg_fail(MPG_ERR_NUMERIC, "gcrk: NaN/Inf in the residual");
+    return MPG_OK;
+}
+
+extern "C" int mpg_get_gcr_stats(mpg_handle h, mpg_gcr_stats *stats) {
+    if (!h || !stats) return mpg_fail(MPG_ERR_ARG, "null argument");
+    fill_stats(h, stats);
+    return MPG_OK;
+}
+
+extern "C" int mpg_mpdatamper(mpg_handle h, int unk, int iflag) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    (void)iflag;
+    if (h->P.iper != 2) return mpg_fail(MPG_ERR_UNSUPPORTED, "mpdatam (iper=0 inflow closure) is not provided");
+    FLD(psi, unk);
+    for (int q = 0; q < 3; ++q)
+        if (!fld(h, MPG_F_UUU + q)) return mpg_fail(MPG_ERR_NOMEM, "uuu");
+    int rc = op_aun(h);
+    if (rc) return rc;
+    return op_mpdata_field(h, psi);
+}
+
+extern "C" int mpg_courant(mpg_handle h, int iflag, mpg_diag *diag) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (iflag < 1 || iflag > 3) return mpg_fail(MPG_ERR_ARG, "iflag must be 1, 2 or 3");
+    for (int q = 0; q < 3; ++q)
+        if (!fld(h, MPG_F_UUU + q)) return mpg_fail(MPG_ERR_NOMEM, "uuu");
+    return diag_courant(h, iflag, diag);
+}
+
+extern "C" int mpg_stats(mpg_handle h, mpg_diag *diag) {
+    if (!h || !diag) return mpg_fail(MPG_ERR_ARG, "null argument");
+    return diag_stats(h, diag);
+}
+
+static int step_diag(mpg_handle h, mpg_diag *diag) {
+    mpg_diag d;
+    std::memset(&d, 0, sizeof d);
+    int rc;
+    double *rhs = fld(h, MPG_F_RHS);
+    if ((rc = op_div(h, h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2], rhs, 1))) return rc;
+    if (diag) {
+        if ((rc = diag_div(h, rhs, &d))) return rc;
+        if ((rc = diag_courant(h, 1, &d))) return rc;
+        if ((rc = diag_stats(h, &d))) return rc;
+        *diag = d;
+    } else {
+        if ((rc = diag_courant(h, 1, nullptr))) return rc;
+    }
+    return MPG_OK;
+}
+
+extern "C" int mpg_setup(mpg_handle h, mpg_diag *diag) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    Fields F = make_fields(h);
+    double *prpot = fld(h, MPG_F_PRPOT), *u4 = fld(h, MPG_F_UNK1 + 3);
+    if (!prpot || !u4) return mpg_fail(MPG_ERR_NOMEM, "fields");
+    const int N = h->N;
+    int rc;
+    k_setup_ambient<<<grid(N), kThreads, 0, h->st>>>(N, F, prpot, u4);
+    if ((rc = check_launch("setup ambient"))) return rc;
+    if ((rc = op_gcrk(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.unk[0], F.unk[1], F.unk[2], 0))) return rc;
+    if ((rc = op_prfr(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.unk[0], F.unk[1], F.unk[2], 0))) return rc;
+    k_setup_post<<<grid(N), kThreads, 0, h->st>>>(N, F, prpot);
+    if ((rc = check_launch("setup post"))) return rc;
+    if ((rc = step_diag(h, diag))) return rc;
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    if (h->gstatus == MPG_GCR_NAN) return mpg_fail(MPG_ERR_NUMERIC, "setup: NaN in the potential-flow solve");
+    return MPG_OK;
+}
+
+static const double kF0 = 1.4584e-03, kXlat = 20.;   // mpsolver constants, ref.f:108-109
+static double fcr3_of() { return kF0 * std::sin(kXlat) * 0.0; }   // icorio = 0
+static double fcr2_of() { return kF0 * std::cos(kXlat) * 0.0; }
+
+extern "C" int mpg_half_forcing(mpg_handle h) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    Fields F = make_fields(h);
+    k_half_forcing<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.implgw);
+    return check_launch("half forcing");
+}
+
+extern "C" int mpg_explicit_forcing(mpg_handle h, int mtri) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    Fields F = make_fields(h);
+    k_explicit_forcing<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.g, fcr2_of(), fcr3_of(), 1.0,
+                                                           h->P.implgw, mtri);
+    return check_launch("explicit forcing");
+}
+
+extern "C" int mpg_post_solve(mpg_handle h, int mtri) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    Fields F = make_fields(h);
+    k_post_solve<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.g, mtri == 2 ? 1 : 0);
+    return check_launch("post solve");
+}
+
+extern "C" int mpg_extrapolate(mpg_handle h) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    Fields F = make_fields(h);
+    k_extrapolate<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, fcr2_of(), fcr3_of(), 1.0);
+    return check_launch("extrapolate");
+}
+
+// One pass of DO ITIME (ref.f:285-463), driving the entry points above in mpsolver's order.
+extern "C" int mpg_step(mpg_handle h, mpg_diag *diag) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (h->P.iper != 2) return mpg_fail(MPG_ERR_UNSUPPORTED, "mpdatam (iper=0 inflow closure) is not provided");
+    int rc;
+    Fields F = make_fields(h);
+    if ((rc = mpg_half_forcing(h))) return rc;
+    if ((rc = op_aun(h))) return rc;                          // uuu is fixed over the advection calls
+    for (int q = 0; q < 4 + h->P.nscal; ++q) {
+        double *psi = fld(h, MPG_F_UNK + q);
+        if (!psi) return mpg_fail(MPG_ERR_NOMEM, "unk");
+        if ((rc = op_mpdata_field(h, psi))) return rc;
+    }
+    double *prpot = fld(h, MPG_F_PRPOT);
+    for (int mtri = 1; mtri <= 2; ++mtri) {
+        if ((rc = mpg_explicit_forcing(h, mtri))) return rc;
+        const int imp = h->P.implgw;
+        if ((rc = op_gcrk(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.uuu[0], F.uuu[1], F.uuu[2], imp))) return rc;
+        if (h->gstatus == MPG_GCR_NAN) return mpg_fail(MPG_ERR_NUMERIC, "step: NaN in the pressure solve");
+        if ((rc = op_prfr(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.uuu[0], F.uuu[1], F.uuu[2], imp))) return rc;
+        if ((rc = mpg_post_solve(h, mtri))) return rc;
+    }
+    if ((rc = mpg_extrapolate(h))) return rc;
+    return step_diag(h, diag);
+}
+
+extern "C" int mpg_synchronize(mpg_handle h) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    return MPG_OK;
+}
+
+extern "C" int mpg_analyze_mesh(const mpg_mesh_ref *mesh, mpg_info *info) {
+    if (!mesh || !info) return mpg_fail(MPG_ERR_ARG, "null argument");
+    HostColumnMesh hm;
+    int rc = mpg_build_column_mesh(mesh, &hm);
+    if (rc) return rc;
+    info->npoin = hm.N;
+    info->nedge = (int64_t)hm.NE2 * hm.L + (int64_t)hm.NC * (hm.L - 1);
+    info->ncol = hm.NC;
+    info->nedge2d = hm.NE2;
+    info->nlev = hm.L;
+    info->precision = hm.bitwise_order ? 1 : 0;
+    info->device_bytes = 0;
+    return MPG_OK;
+}

