@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Time steps of the anelastic MPDATA + GCR solver on B200 (one JSON line on rank 0).
+
+Workload (default): the 21.2M-node plain FP64 case — 512x512 jittered columns on a doubly
+periodic 120 km square, Delaunay-triangulated with median-dual cells, 81 terrain-following
+levels over 20 km above a 400 m Witch-of-Agnesi hill (half-width 10 km), N = 0.01 1/s,
+U = 10 m/s, anelastic reference state; dt = 6 s, MPDATA iord=2 with the nonoscillatory option,
+GCR(3) to max|r|*dt <= 1e-8 with the vertical-line preconditioner, plus one passive positive
+scalar (3D Gaussian, peak 1, sigma 5 km).  Synthetic, seeded inputs.
+
+A step is one pass of mpsolver's DO ITIME loop: 5 MPDATA fields, two (gcrk + prfr) pressure
+solves, the node loops and the per-step diagnostics.  `value` is steps/s over all GPUs with the
+state resident in HBM; `e2e` is the same through the C ABI from pinned host state (upload,
+K steps with the per-step diagnostics read back, download).  `--impl reference` times the CPU
+restatement of the reference (the oracle; no Fortran compiler exists on these machines).
+
+Multi-GPU: the path does not shard (a single mesh per GPU), so N GPUs run N independent
+replicas; the timed region is bracketed by barriers and the max over ranks is taken.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "steps/s & ms/pressure-solve: learned+mixed vs plain FP64 GCR, 1 B200, resid≤1e-8"
+WORKLOADS = {
+    # name: (nx, levels, dt, h0, lord, nscal)
+    "fp64_512x512x81": (512, 81, 6.0, 400.0, 3, 1),
+    "fp64_48x48x41": (48, 41, 10.0, 400.0, 3, 0),
+    "fp64_256x256x81": (256, 81, 6.0, 400.0, 3, 1),
+}
+DEFAULT = "fp64_512x512x81"
+CPU_SAMPLE = "fp64_48x48x41"
+L2_BYTES = 126 * 2 ** 20
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def build_params(name, precision=0):
+    from src_b200.cabi import RunParams
+    nx, L, dt, h0, lord, nscal = WORKLOADS[name]
+    return RunParams(delt=dt, lord=lord, nscal=nscal, eps0=1e-8, itr=200, iprc=2, itrp1=1,
+                     lipps=1, strat=0.01 ** 2 / 9.80616, precision=precision)
+
+
+def build_mesh(name):
+    from src_b200 import mesh
+    nx, L, dt, h0, lord, nscal = WORKLOADS[name]
+    cm = mesh.generate(nx, L=L, seed=0, h0=h0)
+    return cm, cm.to_reference()
+
+
+def gaussian_scalar(rm):
+    x, y, z = rm.coord[:, 0], rm.coord[:, 1], rm.coord[:, 2]
+    return np.exp(-((x - 30e3) ** 2 + (y - 60e3) ** 2 + (z - 5e3) ** 2) / (2 * 5e3 ** 2))
+
+
+def algorithmic_bytes(cls, N, Eh, Ev):
+    """FP64 bytes each launch must move: every distinct array element read once, written once.
+
+    N nodes, Eh horizontal faces (2D edges x levels), Ev vertical faces; a face vector is 3
+    doubles.  The per-column adjacency lists (a few ints per column) are not counted."""
+    E = Eh + Ev
+    table = {
+        "lap_grad": 56 * N + 24 * E,      # p, vol, rh0, coefw in; S; Fx, Fy, Fz out
+        "lap_div": 48 * N + 24 * E,       # Fx, Fy, Fz, vol, rh0 in; S; alap out
+        "prfr": 72 * N + 24 * E,          # p, u*, v*, w*, vol, coefw in; S; u, v, w out
+        "div": 48 * N + 24 * E,           # u, v, w, vol, rh0 in; S; rhs out
+        "line_solve": 40 * N,             # rhs, a, m, c' in; p out
+        "aun": 24 * N + 32 * E,           # uuu in; S in; aun out
+        "mp_donor": 32 * N + 8 * E,       # psi, vol, rh0 in; aun; psi1 out
+        "mp_grad_bounds": 48 * N + 24 * E,  # psi1 in; S; 3 gradients, max, min out
+        "mp_anti": 72 * N + 16 * E,       # psi1, grad x3, vol, rh0, uuu x3; aun in, A out
+        "mp_cpcn": 56 * N + 8 * E,        # A; psi1, mx, mn, vol, rh0 in; cp, cn out
+        "mp_pass2": 48 * N + 8 * E,       # A; psi1, cp, cn, vol, rh0 in; psi out
+        "courant": 40 * N + 24 * E,       # uuu, rh0, vol in; S; cour out
+    }
+    return table.get(cls)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f".clocks_{os.getpid()}.csv") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else f"/tmp/.clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_sample(steps, warmup):
+    """Oracle (CPU restatement, 1 thread) full steps of the 48x48x41 workload."""
+    from oracle.oracle import Oracle
+    cm, rm = build_mesh(CPU_SAMPLE)
+    o = Oracle(build_params(CPU_SAMPLE), rm)
+    o.setup()
+    for _ in range(warmup):
+        o.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step()
+    dt = (time.perf_counter() - t0) / steps
+    return dt, rm.npoin
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    nx, L = WORKLOADS[DEFAULT][0], WORKLOADS[DEFAULT][1]
+    n_work = nx * nx * L
+    sec, n_sample = cpu_sample(args.steps, args.warmup)
+    value = (1.0 / sec) * n_sample / n_work
+    sample = (f"{args.steps} oracle steps (after {args.warmup} warm-up) of the 48x48x41 mesh "
+              f"({n_sample} nodes, dt=10 s), {sec:.3f} s/step, per-node cost scaled to {n_work} nodes")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(DEFAULT),
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(name):
+    nx, L, dt, h0, lord, nscal = WORKLOADS[name]
+    return {"workload": f"plain FP64 MPDATA+GCR step, {nx}x{nx} jittered periodic columns x {L} levels "
+                        f"({nx * nx * L} nodes), Agnesi hill h0={h0:g} m, dt={dt:g} s",
+            "nodes": nx * nx * L, "edges": 3 * nx * nx * L + nx * nx * (L - 1), "levels": L, "dt_s": dt,
+            "gcr": f"GCR({lord}) to max|r|*dt<=1e-8, vertical-line preconditioner",
+            "mpdata": "iord=2 + nonoscillatory (FCT)", "passive_scalars": nscal,
+            "l2": "inputs larger than L2 (each FP64 node field is 8*nodes bytes > 126 MB)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    rank, local, world = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    from src_b200.api import Solver
+    from src_b200.cabi import F_UNK, F_UUU, F_UUU0, F_FRC, F_UNKDASH, F_PRPOT, MpgDiag
+
+    name = args.workload
+    cm, rm = build_mesh(name)
+    P = build_params(name)
+    s = Solver(P, rm, device=local)
+    info = s.info()
+    d0 = s.setup()
+    if P.nscal:
+        s.set(F_UNK + 4, gaussian_scalar(rm))
+    stream = torch.cuda.ExternalStream(s.stream())
+    for _ in range(args.warmup):
+        s.step()
+    s.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # ---------------- timed region: K steps, state resident in HBM
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    s.kernel_timing(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.start()
+    e0.record(stream)
+    iters, diags = [], []
+    for _ in range(args.steps):
+        d = s.step()
+        iters.append((d.niter1, d.niter))
+        diags.append(d)
+    e1.record(stream)
+    e1.synchronize()
+    clocks = sampler.stop()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    kt = s.kernel_times()
+    s.kernel_timing(False)
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1000.0)
+
+    # ---------------- per-kernel roofline
+    N, L, NC, NE2 = info["npoin"], info["nlev"], info["ncol"], info["nedge2d"]
+    Eh, Ev = NE2 * L, NC * (L - 1)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    kernels = {}
+    for cls, (nl, tot) in kt.items():
+        ent = {"launches": nl, "total_ms": round(tot, 3), "avg_us": round(1000 * tot / nl, 2)}
+        ab = algorithmic_bytes(cls, N, Eh, Ev)
+        if ab:
+            gbs = ab / (tot / nl / 1000.0) / 1e9
+            ent.update({"bytes_per_launch": ab, "gbs": round(gbs, 1), "frac": round(gbs / hbm, 3)})
+        kernels[cls] = ent
+    real = {k: v for k, v in kernels.items() if k != "pressure_solve"}
+    dom = max((k for k in real if "gbs" in real[k]), key=lambda k: real[k]["total_ms"])
+    launches = int(sum(v["launches"] for v in real.values()))
+    solve = kernels.get("pressure_solve", {"launches": 0, "total_ms": 0.0})
+    ms_solve = solve["total_ms"] / max(solve["launches"], 1)
+    roof = {"kernel": dom, "bound": "hbm", "achieved": real[dom]["gbs"], "peak": hbm, "unit": "GB/s",
+            "frac": round(real[dom]["gbs"] / hbm, 3), "peak_source": peak_src,
+            "traffic": None, "bytes_per_launch": real[dom]["bytes_per_launch"]}
+    tr_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr_path):
+        try:
+            tr = json.load(open(tr_path)).get(name, {}).get(dom)
+            roof["traffic"] = tr
+        except Exception:
+            pass
+
+    # ---------------- end to end through the C ABI from pinned host state
+    e2e = None
+    if not args.no_e2e:
+        fids = [F_UNK + k for k in range(4 + P.nscal)] + [F_UUU + k for k in range(3)] + \
+               [F_UUU0 + k for k in range(3)] + [F_FRC + k for k in range(4)] + \
+               [F_UNKDASH + k for k in range(3)] + [F_PRPOT]
+        host = {f: torch.empty(rm.npoin, dtype=torch.float64, pin_memory=True).numpy() for f in fids}
+        for f in fids:
+            host[f][:] = s.get(f)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for f in fids:
+            s.set(f, host[f])
+        for _ in range(args.steps):
+            s.step()
+        for f in fids:
+            host[f][:] = s.get(f)
+        t1 = time.perf_counter()
+        sec = t1 - t0
+        if world > 1:
+            t = torch.tensor([sec], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            sec = float(t.item())
+        state = len(fids) * 8 * rm.npoin
+        import ctypes
+        e2e = {"value": world * args.steps / sec, "unit": "steps/s",
+               "h2d_bytes_per_step": state // args.steps,
+               "d2h_bytes_per_step": (state + args.steps * ctypes.sizeof(MpgDiag)) // args.steps,
+               "path": "mpg_set_field x%d from pinned host arrays, %d x mpg_step (per-step diagnostics "
+                       "read back), mpg_get_field x%d" % (len(fids), args.steps, len(fids))}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sec, n_sample = cpu_sample(3, 1)
+        v = (1.0 / sec) * n_sample / N
+        cpu = {"value": v, "unit": "steps/s", "cores": 1, "kind": "port",
+               "sample": f"3 oracle steps of the 48x48x41 mesh ({n_sample} nodes, dt=10 s), {sec:.3f} s/step, "
+                         f"per-node cost scaled to {N} nodes"}
+
+    if rank == 0:
+        last = diags[-1]
+        line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": workload_config(name),
+                "ms_per_pressure_solve": round(ms_solve, 3),
+                "gcr_iters_per_solve": round(float(np.mean([a for p in iters for a in p])), 2),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks, "kernels": kernels,
+                "diag_last_step": {"divmx": last.divmx, "crnmx": last.crnmx,
+                                   "scalar_min": last.smin[0] if P.nscal else None,
+                                   "mass_scalar": last.mass[4] if P.nscal else None},
+                "setup_gcr_iters": d0.niter}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -115,7 +115,8 @@ typedef struct mpg_gcr_stats {         /* /itero/ (ref.f:1953-1963) plus the exi
 typedef struct mpg_diag {              /* per-step diagnostics printed by mpsolver (ref.f:456-459) */
     double divmx, divmn, divav, divsd; /* div(...,1)        ref.f:2148-2168 */
     double crnmx, crnmn, crnav, crnsd; /* courant(...,1)    ref.f:2076-2092 */
-    int32_t icrnmx, niter, nitav, pad; /* node of max Courant (1-based), solver stats */
+    int32_t icrnmx, niter, nitav;      /* node of max Courant (1-based), solver stats (ref.f:2164) */
+    int32_t niter1;                    /* GCR iterations of the step's first pressure solve      */
     double eer, eem;
     double stats[16];                  /* umx,umn,uav,usd, vmx.., wmx.., tmx,tmn,tav,tsd (ref.f:2904) */
     double mass[8];                    /* sum(vol*rh0*unk(:,k)) for the prognostic fields (FP64)  */
@@ -208,6 +209,21 @@ int mpg_extrapolate(mpg_handle h);                  /* ref.f:387-439 */
 int mpg_get_gcr_stats(mpg_handle h, mpg_gcr_stats *stats);
 /* Wait for all work of the handle. */
 int mpg_synchronize(mpg_handle h);
+
+/* ---------------------------------------------------------------- instrumentation */
+/* The CUDA stream every kernel of the handle runs on (a cudaStream_t), so callers can time
+ * or order their own work against it. */
+int mpg_get_stream(mpg_handle h, void **stream);
+/* Per-kernel-class timing with CUDA events recorded around each launch on the handle's stream
+ * (off by default; enabling it clears the totals).  Pressure solves (gcrk + prfr inside
+ * mpg_step) are always timed, as class "pressure_solve". */
+typedef struct mpg_ktime {
+    char    name[24];
+    int64_t launches;
+    double  total_ms;
+} mpg_ktime;
+int mpg_kernel_timing(mpg_handle h, int enable);
+int mpg_kernel_times(mpg_handle h, mpg_ktime *out, int max, int *count);
 
 #ifdef __cplusplus
 }

@@ -952,7 +952,7 @@ void orc_step(orc *o, mpg_diag *diag) {
     }
     for (int k = 0; k < 4 + P->nscal; ++k)                     /* ref.f:314-319 */
         orc_mpdatamper(o, f[MPG_F_UNK + k], k + 1);
-    int mtrimx = 2;
+    int mtrimx = 2, niter1 = 0;
     for (int mtri = 1; mtri <= mtrimx; ++mtri) {
         for (int ip = 0; ip < n; ++ip) {                       /* ref.f:323-359 */
             double frm1 = 0., frm2 = 0., frm3 = 0.;
@@ -975,6 +975,7 @@ void orc_step(orc *o, mpg_diag *diag) {
         int imp = implgw;                                      /* ref.f:361-365 */
         orc_gcrk(o, f[MPG_F_PRPOT], unk1[0], unk1[1], unk1[2], uuu[0], uuu[1], uuu[2], imp, NULL);
         orc_prfr(o, f[MPG_F_PRPOT], unk1[0], unk1[1], unk1[2], uuu[0], uuu[1], uuu[2], imp);
+        if (mtri == 1) niter1 = o->niter;
         for (int ip = 0; ip < n; ++ip) {                       /* ref.f:367-383 */
             ud[0][ip] = uuu[0][ip] * o->gmm[ip] * o->cosa[ip];
             ud[1][ip] = uuu[1][ip] * o->gmm[ip];
@@ -1017,6 +1018,7 @@ void orc_step(orc *o, mpg_diag *diag) {
     orc_div(o, uuu[0], uuu[1], uuu[2], f[MPG_F_RHS], 1, &dd);
     orc_courant(o, 1, &dd);
     orc_stats(o, &dd);
+    dd.niter1 = niter1;
     if (diag) *diag = dd;
 }
 

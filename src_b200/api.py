@@ -28,7 +28,7 @@ EXPORTS = [
     "mpg_derivative", "mpg_bcv", "mpg_laplc", "mpg_prfr", "mpg_div", "mpg_precon", "mpg_gcrk",
     "mpg_mpdatamper", "mpg_courant", "mpg_stats", "mpg_setup", "mpg_step", "mpg_half_forcing",
     "mpg_explicit_forcing", "mpg_post_solve", "mpg_extrapolate", "mpg_get_gcr_stats",
-    "mpg_synchronize", "mpg_analyze_mesh",
+    "mpg_synchronize", "mpg_analyze_mesh", "mpg_get_stream", "mpg_kernel_timing", "mpg_kernel_times",
 ]
 
 
@@ -70,6 +70,9 @@ def lib():
             getattr(L, nm).argtypes = [vp, ip]
         L.mpg_get_gcr_stats.argtypes = [vp, vp]
         L.mpg_analyze_mesh.argtypes = [vp, vp]
+        L.mpg_get_stream.argtypes = [vp, C.POINTER(vp)]
+        L.mpg_kernel_timing.argtypes = [vp, ip]
+        L.mpg_kernel_times.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -190,6 +193,24 @@ class Solver:
 
     def synchronize(self) -> None:
         _check(self.L.mpg_synchronize(self.h))
+
+    # ---------------------------------------------------------------- instrumentation
+    def stream(self) -> int:
+        """cudaStream_t of the handle, as an integer (for torch.cuda.ExternalStream)."""
+        p = C.c_void_p()
+        _check(self.L.mpg_get_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def kernel_timing(self, enable: bool) -> None:
+        _check(self.L.mpg_kernel_timing(self.h, 1 if enable else 0))
+
+    def kernel_times(self) -> dict:
+        """{class: (launches, total_ms)} from CUDA events around each launch."""
+        from .cabi import MpgKtime
+        arr = (MpgKtime * 32)()
+        n = C.c_int()
+        _check(self.L.mpg_kernel_times(self.h, arr, 32, C.byref(n)))
+        return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms) for i in range(min(n.value, 32))}
 
 
 # convenience re-exports of the field ids

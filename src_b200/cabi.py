@@ -64,7 +64,7 @@ class MpgDiag(C.Structure):
     _fields_ = [
         ("divmx", C.c_double), ("divmn", C.c_double), ("divav", C.c_double), ("divsd", C.c_double),
         ("crnmx", C.c_double), ("crnmn", C.c_double), ("crnav", C.c_double), ("crnsd", C.c_double),
-        ("icrnmx", C.c_int32), ("niter", C.c_int32), ("nitav", C.c_int32), ("pad", C.c_int32),
+        ("icrnmx", C.c_int32), ("niter", C.c_int32), ("nitav", C.c_int32), ("niter1", C.c_int32),
         ("eer", C.c_double), ("eem", C.c_double),
         ("stats", C.c_double * 16), ("mass", C.c_double * 8),
         ("smin", C.c_double * 4), ("smax", C.c_double * 4),
@@ -78,6 +78,10 @@ class MpgDiag(C.Structure):
             v = getattr(self, k)
             d[k] = list(v) if not isinstance(v, (int, float)) else v
         return d
+
+
+class MpgKtime(C.Structure):
+    _fields_ = [("name", C.c_char * 24), ("launches", C.c_int64), ("total_ms", C.c_double)]
 
 
 class MpgInfo(C.Structure):

@@ -21,6 +21,26 @@ int mpg_fail(int code, const std::string &msg) {
 }
 extern "C" const char *mpg_last_error(void) { return g_err.c_str(); }
 
+// ------------------------------------------------------------------------------ kernel timing
+enum KClass {
+    KT_LAP_GRAD, KT_LAP_DIV, KT_PRFR, KT_DIV, KT_LINE, KT_REDUCE, KT_GCR_UPD, KT_AUN, KT_MP_DONOR,
+    KT_MP_GRADB, KT_MP_ANTI, KT_MP_CPCN, KT_MP_PASS2, KT_NODE, KT_COURANT, KT_MISC, KT_SOLVE, KT_COUNT
+};
+static const char *kKNames[KT_COUNT] = {
+    "lap_grad", "lap_div", "prfr", "div", "line_solve", "reduce", "gcr_update", "aun", "mp_donor",
+    "mp_grad_bounds", "mp_anti", "mp_cpcn", "mp_pass2", "node_loops", "courant", "misc", "pressure_solve"};
+
+struct KTimer {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    struct Rec { int cls; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    std::vector<int> open;          // stack of pending (class, start) for nested scopes
+    std::vector<cudaEvent_t> open_ev;
+    double total_ms[KT_COUNT] = {};
+    int64_t launches[KT_COUNT] = {};
+};
+
 // ------------------------------------------------------------------------------ handle
 struct mpg_solver {
     mpg_params P{};
@@ -51,7 +71,56 @@ struct mpg_solver {
     double betaunstr1 = 0.;
     HostStatic hs;
     std::vector<int32_t> iperm;
+    KTimer kt;
 };
+
+static cudaEvent_t kt_event(mpg_handle h) {
+    if (h->kt.pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaEvent_t e = h->kt.pool.back();
+    h->kt.pool.pop_back();
+    return e;
+}
+
+// fold recorded event pairs into the totals (synchronises the stream)
+static void kt_collect(mpg_handle h) {
+    if (h->kt.recs.empty()) return;
+    cudaStreamSynchronize(h->st);
+    for (auto &r : h->kt.recs) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            h->kt.total_ms[r.cls] += ms;
+            h->kt.launches[r.cls] += 1;
+        }
+        h->kt.pool.push_back(r.a);
+        h->kt.pool.push_back(r.b);
+    }
+    h->kt.recs.clear();
+}
+
+// times the launches issued in its scope when timing is on (always for the solve class)
+struct KScope {
+    mpg_handle h;
+    int cls;
+    cudaEvent_t a = nullptr;
+    KScope(mpg_handle h_, int c) : h(h_), cls(c) {
+        if (h->kt.on || cls == KT_SOLVE) {
+            a = kt_event(h);
+            cudaEventRecord(a, h->st);
+        }
+    }
+    ~KScope() {
+        if (!a) return;
+        cudaEvent_t b = kt_event(h);
+        cudaEventRecord(b, h->st);
+        h->kt.recs.push_back({cls, a, b});
+        if (h->kt.recs.size() > 16384) kt_collect(h);
+    }
+};
+#define KTIME(cls) KScope _kscope_(h, cls)
 
 namespace {
 
@@ -99,7 +168,10 @@ int check_launch(const char *what) {
 // generic deterministic reduction launcher
 template <int NQ, class Prod, class Fin>
 int reduce(mpg_handle h, unsigned kinds, Prod prod, Fin fin) {
-    k_reduce<NQ><<<kRedBlocks, kRedThreads, 0, h->st>>>(h->N, kinds, prod, fin, h->part, h->counter, h->result);
+    {
+        KTIME(KT_REDUCE);
+        k_reduce<NQ><<<kRedBlocks, kRedThreads, 0, h->st>>>(h->N, kinds, prod, fin, h->part, h->counter, h->result);
+    }
     return check_launch("k_reduce");
 }
 
@@ -111,21 +183,33 @@ int fetch_result(mpg_handle h, int nq) {
 
 // ------------------------------------------------------------------------------ operators
 int op_laplc(mpg_handle h, const double *p, double *alap, int impfl) {
-    k_lap_grad<<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW], h->ue,
-                                                   h->P.delt, impfl, h->F[0], h->F[1], h->F[2]);
-    k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, h->F[0], h->F[1], h->F[2], h->vol, h->f[MPG_F_RH0], alap);
+    {
+        KTIME(KT_LAP_GRAD);
+        k_lap_grad<<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW], h->ue,
+                                                       h->P.delt, impfl, h->F[0], h->F[1], h->F[2]);
+    }
+    {
+        KTIME(KT_LAP_DIV);
+        k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, h->F[0], h->F[1], h->F[2], h->vol, h->f[MPG_F_RH0], alap);
+    }
     return check_launch("laplc");
 }
 
 int op_prfr(mpg_handle h, const double *p, const double *us, const double *vs, const double *ws, double *uo,
             double *vo, double *wo, int impfl) {
-    k_prfr<<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, us, vs, ws, h->vol, h->f[MPG_F_COEFW], h->ue, h->P.delt,
-                                               impfl, uo, vo, wo);
+    {
+        KTIME(KT_PRFR);
+        k_prfr<<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, us, vs, ws, h->vol, h->f[MPG_F_COEFW], h->ue, h->P.delt,
+                                                   impfl, uo, vo, wo);
+    }
     return check_launch("prfr");
 }
 
 int op_div(mpg_handle h, const double *ua, const double *va, const double *wa, double *rhs, int iflg) {
-    k_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, ua, va, wa, h->vol, h->f[MPG_F_RH0], iflg, rhs);
+    {
+        KTIME(KT_DIV);
+        k_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, ua, va, wa, h->vol, h->f[MPG_F_RH0], iflg, rhs);
+    }
     return check_launch("div");
 }
 
@@ -133,8 +217,11 @@ int op_line(mpg_handle h, const double *rhs, double *p, int impfl, int acc) {
     const int q = impfl ? 1 : 0;
     const int nblk = (h->NC + 32 * kLineWarps - 1) / (32 * kLineWarps);
     const size_t smem = sizeof(double) * 32 * kLineWarps * h->L;
-    k_line_solve<<<nblk, 32 * kLineWarps, smem, h->st>>>(h->NC, h->L, rhs, h->la[q], h->lm[q], h->lcp[q],
-                                                          h->P.omega, acc, p);
+    {
+        KTIME(KT_LINE);
+        k_line_solve<<<nblk, 32 * kLineWarps, smem, h->st>>>(h->NC, h->L, rhs, h->la[q], h->lm[q], h->lcp[q],
+                                                              h->P.omega, acc, p);
+    }
     return check_launch("line_solve");
 }
 
@@ -143,10 +230,16 @@ int op_line(mpg_handle h, const double *rhs, double *p, int impfl, int acc) {
 int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, int impfl, bool zero_r) {
     const int N = h->N;
     if (iprc == 0) {
-        k_copy<<<grid(N), kThreads, 0, h->st>>>(N, rhs, p);
+        {
+            KTIME(KT_MISC);
+            k_copy<<<grid(N), kThreads, 0, h->st>>>(N, rhs, p);
+        }
         return check_launch("precon copy");
     }
-    if (zero_r) k_fill<<<grid(N), kThreads, 0, h->st>>>(N, r, 0.0);
+    if (zero_r) {
+        KTIME(KT_MISC);
+        k_fill<<<grid(N), kThreads, 0, h->st>>>(N, r, 0.0);
+    }
     if (iprc == 2) {
         for (int it = 1; it <= h->P.itrp1; ++it) {
             if (it == 1) {
@@ -155,25 +248,40 @@ int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, i
             } else {
                 int rc = op_laplc(h, p, r, impfl);
                 if (rc) return rc;
-                k_sub<<<grid(N), kThreads, 0, h->st>>>(N, rhs, r, h->tres);
+                {
+                    KTIME(KT_MISC);
+                    k_sub<<<grid(N), kThreads, 0, h->st>>>(N, rhs, r, h->tres);
+                }
                 rc = op_line(h, h->tres, p, impfl, 1);
                 if (rc) return rc;
             }
         }
-        if (h->P.itrp1 < 1) k_fill<<<grid(N), kThreads, 0, h->st>>>(N, p, 0.0);
+        if (h->P.itrp1 < 1) {
+            KTIME(KT_MISC);
+            k_fill<<<grid(N), kThreads, 0, h->st>>>(N, p, 0.0);
+        }
         return check_launch("precon line");
     }
     if (iprc != 1) return mpg_fail(MPG_ERR_UNSUPPORTED, "iprc must be 0, 1 or 2");
     // reference smoother: the first sweep starts from p = 0, where laplc(0) = 0 exactly
-    k_fill<<<grid(N), kThreads, 0, h->st>>>(N, p, 0.0);
-    if (!zero_r) k_fill<<<grid(N), kThreads, 0, h->st>>>(N, r, 0.0);
+    {
+        KTIME(KT_MISC);
+        k_fill<<<grid(N), kThreads, 0, h->st>>>(N, p, 0.0);
+    }
+    if (!zero_r) {
+        KTIME(KT_MISC);
+        k_fill<<<grid(N), kThreads, 0, h->st>>>(N, r, 0.0);
+    }
     for (int it = 1; it <= h->P.itrp1; ++it) {
         if (it > 1) {
             int rc = op_laplc(h, p, r, impfl);
             if (rc) return rc;
         }
-        k_smooth<<<grid(N), kThreads, 0, h->st>>>(N, h->P.sm_flag1, h->P.omega, h->betaunstr1,
-                                                  h->f[MPG_F_D1], r, rhs, p);
+        {
+            KTIME(KT_MISC);
+            k_smooth<<<grid(N), kThreads, 0, h->st>>>(N, h->P.sm_flag1, h->P.omega, h->betaunstr1,
+                                                      h->f[MPG_F_D1], r, rhs, p);
+        }
     }
     return check_launch("precon smoother");
 }
@@ -274,7 +382,10 @@ int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const d
     if ((rc = reduce<3>(h, 0x2u, ProdNorm0{h->qr, h->r}, FinEps{h->scal}))) return rc;
     if ((rc = fetch_result(h, 3))) return rc;
     double rl20 = h->h_res[2] > epa ? h->h_res[2] : epa;
-    k_copy<<<grid(N), kThreads, 0, h->st>>>(N, h->qr, h->x[0]);
+    {
+        KTIME(KT_MISC);
+        k_copy<<<grid(N), kThreads, 0, h->st>>>(N, h->qr, h->x[0]);
+    }
     if ((rc = op_laplc(h, h->x[0], h->ax[0], impfl))) return rc;
     int status = MPG_GCR_MAXIT;
     double dvmx = 0., rl2 = 0.;
@@ -297,9 +408,15 @@ int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const d
             nlc = nlc + 1;
             if ((rc = gcr_dots(h, i))) return rc;
             if (i < lord) {
-                k_gcr_next<<<grid(N), kThreads, 0, h->st>>>(N, i, h->scal, h->qr, h->ar, xl, axl, h->x[i], h->ax[i]);
+                {
+                    KTIME(KT_GCR_UPD);
+                    k_gcr_next<<<grid(N), kThreads, 0, h->st>>>(N, i, h->scal, h->qr, h->ar, xl, axl, h->x[i], h->ax[i]);
+                }
             } else {
-                k_gcr_restart<<<grid(N), kThreads, 0, h->st>>>(N, i, h->scal, h->qr, h->ar, xl, axl);
+                {
+                    KTIME(KT_GCR_UPD);
+                    k_gcr_restart<<<grid(N), kThreads, 0, h->st>>>(N, i, h->scal, h->qr, h->ar, xl, axl);
+                }
             }
             if ((rc = check_launch("gcr update"))) return rc;
         }
@@ -325,7 +442,10 @@ int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const d
 int op_aun(mpg_handle h) {
     U3 U{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}};
     const int nt = h->NE2 * h->L + h->N;
-    k_aun<<<grid(nt), kThreads, 0, h->st>>>(h->M, h->S, U);
+    {
+        KTIME(KT_AUN);
+        k_aun<<<grid(nt), kThreads, 0, h->st>>>(h->M, h->S, U);
+    }
     return check_launch("aun");
 }
 
@@ -333,15 +453,30 @@ int op_mpdata_field(mpg_handle h, double *psi) {
     const double dt = h->P.delt;
     const double *vol = h->vol, *rh0 = h->f[MPG_F_RH0];
     const int N = h->N;
-    k_mp_donor<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, psi, vol, rh0, dt, h->psi1);
-    k_mp_grad_bounds<<<grid(N), kThreads, 0, h->st>>>(h->M, h->psi1, h->g3[0], h->g3[1], h->g3[2], h->mx, h->mn);
+    {
+        KTIME(KT_MP_DONOR);
+        k_mp_donor<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, psi, vol, rh0, dt, h->psi1);
+    }
+    {
+        KTIME(KT_MP_GRADB);
+        k_mp_grad_bounds<<<grid(N), kThreads, 0, h->st>>>(h->M, h->psi1, h->g3[0], h->g3[1], h->g3[2], h->mx, h->mn);
+    }
     AntiArgs A{h->psi1, h->g3[0], h->g3[1], h->g3[2], vol, rh0,
                U3{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}}, dt};
     const int nt = h->NE2 * h->L + h->N;
-    k_mp_anti<<<grid(nt), kThreads, 0, h->st>>>(h->M, h->S, A);
+    {
+        KTIME(KT_MP_ANTI);
+        k_mp_anti<<<grid(nt), kThreads, 0, h->st>>>(h->M, h->S, A);
+    }
     // cp, cn reuse the gradient buffers (dead after the antidiffusive fluxes)
-    k_mp_cpcn<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, h->psi1, h->mx, h->mn, vol, rh0, dt, h->g3[0], h->g3[1]);
-    k_mp_pass2<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, h->psi1, h->g3[0], h->g3[1], vol, rh0, dt, psi);
+    {
+        KTIME(KT_MP_CPCN);
+        k_mp_cpcn<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, h->psi1, h->mx, h->mn, vol, rh0, dt, h->g3[0], h->g3[1]);
+    }
+    {
+        KTIME(KT_MP_PASS2);
+        k_mp_pass2<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, h->psi1, h->g3[0], h->g3[1], vol, rh0, dt, psi);
+    }
     return check_launch("mpdata");
 }
 
@@ -450,7 +585,10 @@ int diag_courant(mpg_handle h, int iflag, mpg_diag *d) {
     int rc;
     U3 U{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}};
     double *cour = fld(h, MPG_F_COUR);
-    k_courant<<<grid(h->N), kThreads, 0, h->st>>>(h->M, U, h->f[MPG_F_RH0], h->vol, h->P.delt, iflag, cour);
+    {
+        KTIME(KT_COURANT);
+        k_courant<<<grid(h->N), kThreads, 0, h->st>>>(h->M, U, h->f[MPG_F_RH0], h->vol, h->P.delt, iflag, cour);
+    }
     if ((rc = check_launch("courant"))) return rc;
     if (!d) return MPG_OK;
     if ((rc = reduce<3>(h, 0x6u, ProdCour{cour}, NoFin{}))) return rc;
@@ -616,6 +754,8 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
 extern "C" int mpg_destroy(mpg_handle h) {
     if (!h) return MPG_OK;
     if (h->st) cudaStreamSynchronize(h->st);
+    kt_collect(h);
+    for (cudaEvent_t e : h->kt.pool) cudaEventDestroy(e);
     for (void *p : h->allocs) cudaFree(p);
     if (h->h_res) cudaFreeHost(h->h_res);
     if (h->st) cudaStreamDestroy(h->st);
@@ -799,11 +939,17 @@ extern "C" int mpg_setup(mpg_handle h, mpg_diag *diag) {
     if (!prpot || !u4) return mpg_fail(MPG_ERR_NOMEM, "fields");
     const int N = h->N;
     int rc;
-    k_setup_ambient<<<grid(N), kThreads, 0, h->st>>>(N, F, prpot, u4);
+    {
+        KTIME(KT_NODE);
+        k_setup_ambient<<<grid(N), kThreads, 0, h->st>>>(N, F, prpot, u4);
+    }
     if ((rc = check_launch("setup ambient"))) return rc;
     if ((rc = op_gcrk(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.unk[0], F.unk[1], F.unk[2], 0))) return rc;
     if ((rc = op_prfr(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.unk[0], F.unk[1], F.unk[2], 0))) return rc;
-    k_setup_post<<<grid(N), kThreads, 0, h->st>>>(N, F, prpot);
+    {
+        KTIME(KT_NODE);
+        k_setup_post<<<grid(N), kThreads, 0, h->st>>>(N, F, prpot);
+    }
     if ((rc = check_launch("setup post"))) return rc;
     if ((rc = step_diag(h, diag))) return rc;
     MPG_CUDA(cudaStreamSynchronize(h->st));
@@ -818,29 +964,41 @@ static double fcr2_of() { return kF0 * std::cos(kXlat) * 0.0; }
 extern "C" int mpg_half_forcing(mpg_handle h) {
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
     Fields F = make_fields(h);
-    k_half_forcing<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.implgw);
+    {
+        KTIME(KT_NODE);
+        k_half_forcing<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.implgw);
+    }
     return check_launch("half forcing");
 }
 
 extern "C" int mpg_explicit_forcing(mpg_handle h, int mtri) {
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
     Fields F = make_fields(h);
-    k_explicit_forcing<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.g, fcr2_of(), fcr3_of(), 1.0,
-                                                           h->P.implgw, mtri);
+    {
+        KTIME(KT_NODE);
+        k_explicit_forcing<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.g, fcr2_of(), fcr3_of(), 1.0,
+                                                               h->P.implgw, mtri);
+    }
     return check_launch("explicit forcing");
 }
 
 extern "C" int mpg_post_solve(mpg_handle h, int mtri) {
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
     Fields F = make_fields(h);
-    k_post_solve<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.g, mtri == 2 ? 1 : 0);
+    {
+        KTIME(KT_NODE);
+        k_post_solve<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, h->P.delt, h->P.g, mtri == 2 ? 1 : 0);
+    }
     return check_launch("post solve");
 }
 
 extern "C" int mpg_extrapolate(mpg_handle h) {
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
     Fields F = make_fields(h);
-    k_extrapolate<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, fcr2_of(), fcr3_of(), 1.0);
+    {
+        KTIME(KT_NODE);
+        k_extrapolate<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, fcr2_of(), fcr3_of(), 1.0);
+    }
     return check_launch("extrapolate");
 }
 
@@ -858,16 +1016,25 @@ extern "C" int mpg_step(mpg_handle h, mpg_diag *diag) {
         if ((rc = op_mpdata_field(h, psi))) return rc;
     }
     double *prpot = fld(h, MPG_F_PRPOT);
+    int niter1 = 0;
     for (int mtri = 1; mtri <= 2; ++mtri) {
         if ((rc = mpg_explicit_forcing(h, mtri))) return rc;
         const int imp = h->P.implgw;
-        if ((rc = op_gcrk(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.uuu[0], F.uuu[1], F.uuu[2], imp))) return rc;
-        if (h->gstatus == MPG_GCR_NAN) return mpg_fail(MPG_ERR_NUMERIC, "step: NaN in the pressure solve");
-        if ((rc = op_prfr(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.uuu[0], F.uuu[1], F.uuu[2], imp))) return rc;
+        {
+            KTIME(KT_SOLVE);
+            if ((rc = op_gcrk(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.uuu[0], F.uuu[1], F.uuu[2], imp)))
+                return rc;
+            if (h->gstatus == MPG_GCR_NAN) return mpg_fail(MPG_ERR_NUMERIC, "step: NaN in the pressure solve");
+            if ((rc = op_prfr(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.uuu[0], F.uuu[1], F.uuu[2], imp)))
+                return rc;
+        }
+        if (mtri == 1) niter1 = h->niter;
         if ((rc = mpg_post_solve(h, mtri))) return rc;
     }
     if ((rc = mpg_extrapolate(h))) return rc;
-    return step_diag(h, diag);
+    if ((rc = step_diag(h, diag))) return rc;
+    if (diag) diag->niter1 = niter1;
+    return MPG_OK;
 }
 
 extern "C" int mpg_synchronize(mpg_handle h) {
@@ -888,5 +1055,37 @@ extern "C" int mpg_analyze_mesh(const mpg_mesh_ref *mesh, mpg_info *info) {
     info->nlev = hm.L;
     info->precision = hm.bitwise_order ? 1 : 0;
     info->device_bytes = 0;
+    return MPG_OK;
+}
+
+extern "C" int mpg_get_stream(mpg_handle h, void **stream) {
+    if (!h || !stream) return mpg_fail(MPG_ERR_ARG, "null argument");
+    *stream = (void *)h->st;
+    return MPG_OK;
+}
+
+extern "C" int mpg_kernel_timing(mpg_handle h, int enable) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    kt_collect(h);
+    for (int c = 0; c < KT_COUNT; ++c) { h->kt.total_ms[c] = 0.; h->kt.launches[c] = 0; }
+    h->kt.on = enable != 0;
+    return MPG_OK;
+}
+
+extern "C" int mpg_kernel_times(mpg_handle h, mpg_ktime *out, int max, int *count) {
+    if (!h || !count) return mpg_fail(MPG_ERR_ARG, "null argument");
+    kt_collect(h);
+    int n = 0;
+    for (int c = 0; c < KT_COUNT; ++c) {
+        if (!h->kt.launches[c]) continue;
+        if (out && n < max) {
+            std::memset(out[n].name, 0, sizeof out[n].name);
+            std::strncpy(out[n].name, kKNames[c], sizeof out[n].name - 1);
+            out[n].launches = h->kt.launches[c];
+            out[n].total_ms = h->kt.total_ms[c];
+        }
+        ++n;
+    }
+    *count = n;
     return MPG_OK;
 }

@@ -117,7 +117,7 @@ __device__ __forceinline__ void div3(const ColMesh &M, FX f, int c, int k, int n
 }
 
 // bcv (ref.f:1583-1643) applied to one node
-__device__ __forceinline__ void bcv_node(const ColMesh &M, int c, int k, double ue, double flag,
+__device__ __forceinline__ void bcv_node(const ColMesh &M, int c, int k, int n, const double *ue, double flag,
                                          double &u, double &v, double &w) {
     const bool per = (M.iper == 2);
     for_boundary(M, c, k, [&](const BEntry &be) {
@@ -128,7 +128,7 @@ __device__ __forceinline__ void bcv_node(const ColMesh &M, int c, int k, double 
             v = v - be.anp[1] * vn;
             w = w - be.anp[2] * vn;
         }
-        if (!per && (t == 7 || t == 8)) u = ue * flag;
+        if (!per && (t == 7 || t == 8)) u = ue[n] * flag;
     });
 }
 
@@ -152,7 +152,7 @@ __global__ void k_bcv(ColMesh M, double *u, double *v, double *w, const double *
     col_lev(M, n, c, k);
     if (__ldg(&M.bptr[c]) == __ldg(&M.bptr[c + 1])) return;
     double a = u[n], b = v[n], d = w[n];
-    bcv_node(M, c, k, ue[n], flag, a, b, d);
+    bcv_node(M, c, k, n, ue, flag, a, b, d);
     u[n] = a; v[n] = b; w[n] = d;
 }
 
@@ -172,7 +172,7 @@ __global__ void k_lap_grad(ColMesh M, const double *__restrict__ p, const double
     dx = 0.5 * dx / 1.0;                       // (gmm*cosa)**2 == 1 for isfera = 0
     dy = 0.5 * dy / 1.0;
     dz = 0.5 * dz * (coefw[n] * (double)impfl + (double)(1 - impfl));
-    bcv_node(M, c, k, ue[n], 0.0, dx, dy, dz);
+    bcv_node(M, c, k, n, ue, 0.0, dx, dy, dz);
     const double r = rh0[n];
     Fx[n] = dx * r; Fy[n] = dy * r; Fz[n] = dz * r;
 }
@@ -207,7 +207,7 @@ __global__ void k_prfr(ColMesh M, const double *__restrict__ p, const double *__
     double a = us[n] - 0.5 * dt * dpx;
     double b = vs[n] - 0.5 * dt * dpy;
     double d = ws[n] - 0.5 * dt * dpz * (coefw[n] * (double)impfl + (double)(1 - impfl));
-    bcv_node(M, c, k, ue[n], 1.0, a, b, d);
+    bcv_node(M, c, k, n, ue, 1.0, a, b, d);
     uo[n] = a; vo[n] = b; wo[n] = d;
 }
 

@@ -68,10 +68,18 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out) {
     cmap.reserve((size_t)npoin / 8 + 16);
     std::vector<int32_t> col(npoin);
     std::vector<int32_t> csize;
+    // nodes usually arrive column by column: remember the last column looked up
+    std::pair<uint64_t, uint64_t> last_key(~0ull, ~0ull);
+    int32_t last_col = -1;
     for (int i = 0; i < npoin; ++i) {
         auto key = std::make_pair(bits(X[i]), bits(Y[i]));
-        auto it = cmap.find(key);
         int32_t c;
+        if (key == last_key) {
+            col[i] = last_col;
+            csize[last_col]++;
+            continue;
+        }
+        auto it = cmap.find(key);
         if (it == cmap.end()) {
             c = (int32_t)csize.size();
             cmap.emplace(key, c);
@@ -81,6 +89,8 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out) {
         }
         col[i] = c;
         csize[c]++;
+        last_key = key;
+        last_col = c;
     }
     const int NC = (int)csize.size();
     const int L = csize[0];
@@ -111,17 +121,14 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out) {
         }
     }
 
-    // ---- 3. classify edges
+    // ---- 3. classify edges: vertical faces, and the 2D edges (unique column pairs found at
+    //         level 0, numbered in (a, b) order for locality), then every horizontal edge
     EdgeView ev{m};
     const int64_t nall = ev.n();
     std::vector<int32_t> vorig((size_t)npoin, -1);
-    std::vector<double> Sv[3];
-    for (int d = 0; d < 3; ++d) Sv[d].assign(npoin, 0.0);
-    std::unordered_map<uint64_t, int32_t> emap;
-    emap.reserve((size_t)NC * 4);
-    std::vector<int32_t> ea, eb;
-    std::vector<double> Sh[3];
-    std::vector<int32_t> horig;
+    for (int d = 0; d < 3; ++d) out->Sv[d].assign(npoin, 0.0);
+    std::vector<uint64_t> keys0;
+    int64_t nhor = 0;
     for (int64_t j = 0; j < nall; ++j) {
         int i1 = ev.i1(j), i2 = ev.i2(j);
         if (i1 < 0 || i1 >= npoin || i2 < 0 || i2 >= npoin || i1 == i2)
@@ -134,61 +141,65 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out) {
             int64_t f = (int64_t)c1 * L + klo;
             if (vorig[f] != -1) return mpg_fail(MPG_ERR_MESH, "two vertical edges between the same nodes");
             vorig[f] = (int32_t)j;
-            double sg = k1 < k2 ? 1.0 : -1.0;
-            for (int d = 0; d < 3; ++d) Sv[d][f] = sg == 1.0 ? ev.s(j, d) : -ev.s(j, d);
+            const bool up = k1 < k2;
+            for (int d = 0; d < 3; ++d) out->Sv[d][f] = up ? ev.s(j, d) : -ev.s(j, d);
         } else {
             if (k1 != k2) return mpg_fail(MPG_ERR_MESH, "edge joins different levels of two columns");
-            int a = std::min(c1, c2), b = std::max(c1, c2);
-            uint64_t key = (uint64_t)a * (uint64_t)NC + (uint64_t)b;
-            auto it = emap.find(key);
-            int32_t e;
-            if (it == emap.end()) {
-                e = (int32_t)ea.size();
-                emap.emplace(key, e);
-                ea.push_back(a);
-                eb.push_back(b);
-                for (int d = 0; d < 3; ++d) Sh[d].resize((size_t)(e + 1) * L, 0.0);
-                horig.resize((size_t)(e + 1) * L, -1);
-            } else {
-                e = it->second;
+            ++nhor;
+            if (k1 == 0) {
+                int a = std::min(c1, c2), b = std::max(c1, c2);
+                keys0.push_back((uint64_t)a * (uint64_t)NC + (uint64_t)b);
             }
-            size_t idx = (size_t)e * L + k1;
-            if (horig[idx] != -1) return mpg_fail(MPG_ERR_MESH, "two edges between the same pair of nodes");
-            horig[idx] = (int32_t)j;
-            bool flip = (c1 != a);
-            for (int d = 0; d < 3; ++d) Sh[d][idx] = flip ? -ev.s(j, d) : ev.s(j, d);
         }
     }
-    const int NE2 = (int)ea.size();
-    for (size_t q = 0; q < horig.size(); ++q)
-        if (horig[q] == -1)
-            return mpg_fail(MPG_ERR_MESH, "a horizontal edge is missing at some level");
+    std::sort(keys0.begin(), keys0.end());
+    if (std::adjacent_find(keys0.begin(), keys0.end()) != keys0.end())
+        return mpg_fail(MPG_ERR_MESH, "two edges between the same pair of nodes");
+    const int NE2 = (int)keys0.size();
+    if (nhor != (int64_t)NE2 * L)
+        return mpg_fail(MPG_ERR_MESH, "a horizontal edge is missing at some level");
+    if ((int64_t)NC * L > INT32_MAX / 2 || (int64_t)NE2 * L > INT32_MAX / 2)
+        return mpg_fail(MPG_ERR_MESH, "mesh too large for 32-bit indexing");
+    std::unordered_map<uint64_t, int32_t> emap;
+    emap.reserve((size_t)NE2 * 2 + 16);
+    out->e2a.resize(NE2);
+    out->e2b.resize(NE2);
+    for (int e = 0; e < NE2; ++e) {
+        emap.emplace(keys0[e], e);
+        out->e2a[e] = (int32_t)(keys0[e] / (uint64_t)NC);
+        out->e2b[e] = (int32_t)(keys0[e] % (uint64_t)NC);
+    }
+    std::vector<uint64_t>().swap(keys0);
+    for (int d = 0; d < 3; ++d) out->Sh[d].assign((size_t)NE2 * L, 0.0);
+    std::vector<int32_t> horig2((size_t)NE2 * L, -1);
+    uint64_t last_ekey = ~0ull;
+    int32_t last_e = -1;
+    for (int64_t j = 0; j < nall; ++j) {
+        int i1 = ev.i1(j), i2 = ev.i2(j);
+        int c1 = col[i1], c2 = col[i2];
+        if (c1 == c2) continue;
+        int a = std::min(c1, c2), b = std::max(c1, c2), k = lev[i1];
+        uint64_t key = (uint64_t)a * (uint64_t)NC + (uint64_t)b;
+        int32_t e;
+        if (key == last_ekey) {          // edges usually arrive level by level for one 2D edge
+            e = last_e;
+        } else {
+            auto it = emap.find(key);
+            if (it == emap.end()) return mpg_fail(MPG_ERR_MESH, "a horizontal edge is missing at level 0");
+            e = it->second;
+            last_ekey = key;
+            last_e = e;
+        }
+        size_t idx = (size_t)e * L + k;
+        if (horig2[idx] != -1) return mpg_fail(MPG_ERR_MESH, "two edges between the same pair of nodes");
+        horig2[idx] = (int32_t)j;
+        const bool flip = (c1 != a);
+        for (int d = 0; d < 3; ++d) out->Sh[d][idx] = flip ? -ev.s(j, d) : ev.s(j, d);
+    }
     for (int c = 0; c < NC; ++c)
         for (int k = 0; k + 1 < L; ++k)
             if (vorig[(size_t)c * L + k] == -1)
                 return mpg_fail(MPG_ERR_MESH, "a column lacks a vertical edge between consecutive levels");
-    if ((int64_t)NC * L > INT32_MAX / 2 || (int64_t)NE2 * L > INT32_MAX / 2)
-        return mpg_fail(MPG_ERR_MESH, "mesh too large for 32-bit indexing");
-
-    // ---- 4. order 2D edges by (a, b) for locality
-    std::vector<int32_t> order(NE2);
-    std::iota(order.begin(), order.end(), 0);
-    std::sort(order.begin(), order.end(), [&](int32_t p, int32_t q) {
-        return ea[p] != ea[q] ? ea[p] < ea[q] : eb[p] < eb[q];
-    });
-    out->e2a.resize(NE2);
-    out->e2b.resize(NE2);
-    for (int d = 0; d < 3; ++d) out->Sh[d].resize((size_t)NE2 * L);
-    std::vector<int32_t> horig2((size_t)NE2 * L);
-    for (int ne = 0; ne < NE2; ++ne) {
-        int e = order[ne];
-        out->e2a[ne] = ea[e];
-        out->e2b[ne] = eb[e];
-        for (int d = 0; d < 3; ++d)
-            std::memcpy(&out->Sh[d][(size_t)ne * L], &Sh[d][(size_t)e * L], sizeof(double) * L);
-        std::memcpy(&horig2[(size_t)ne * L], &horig[(size_t)e * L], sizeof(int32_t) * L);
-    }
-    for (int d = 0; d < 3; ++d) { std::vector<double>().swap(Sh[d]); out->Sv[d] = std::move(Sv[d]); }
 
     // ---- 5. per-column adjacency in reference edge order
     std::vector<int32_t> deg(NC + 1, 0);
