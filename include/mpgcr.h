@@ -210,6 +210,25 @@ int mpg_get_gcr_stats(mpg_handle h, mpg_gcr_stats *stats);
 /* Wait for all work of the handle. */
 int mpg_synchronize(mpg_handle h);
 
+/* ---------------------------------------------------------------- allocation-free laplc */
+/* laplc(press, alap, impfl) for callers that must not allocate device memory at call time: a
+ * host application whose own pool owns all device memory (a Fortran or PyTorch code with a
+ * caching allocator, where an outside cudaMalloc can fail on a full pool or break its
+ * accounting), or a time-critical loop where cudaMalloc/cudaFree would synchronise the device.
+ * It has no counterpart in the reference.
+ *
+ * `press` and `alap` are caller-owned DEVICE arrays of npoin doubles in reference node order on
+ * the handle's device.  The work is queued on the handle's stream (mpg_get_stream) and the
+ * call returns without waiting; order your own stream against it before reading alap.
+ * Scratch is a static device array sized for MPG_NOALLOC_MAX_NODES nodes (5 MiB), held by every
+ * GPU that loads the library until the process exits; larger meshes get MPG_ERR_ARG.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress): make that first
+ * call before any stream capture.  All calls share the one array, so calls that overlap on the
+ * GPU (two handles, or two streams, on the same device) race; serialise them.  The call
+ * allocates nothing: no cudaMalloc, cudaFree or allocating library routine. */
+#define MPG_NOALLOC_MAX_NODES 131072
+int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap, int impfl);
+
 /* ---------------------------------------------------------------- instrumentation */
 /* The CUDA stream every kernel of the handle runs on (a cudaStream_t), so callers can time
  * or order their own work against it. */

@@ -29,6 +29,7 @@ EXPORTS = [
     "mpg_mpdatamper", "mpg_courant", "mpg_stats", "mpg_setup", "mpg_step", "mpg_half_forcing",
     "mpg_explicit_forcing", "mpg_post_solve", "mpg_extrapolate", "mpg_get_gcr_stats",
     "mpg_synchronize", "mpg_analyze_mesh", "mpg_get_stream", "mpg_kernel_timing", "mpg_kernel_times",
+    "mpg_laplc_noalloc",
 ]
 
 
@@ -73,6 +74,7 @@ def lib():
         L.mpg_get_stream.argtypes = [vp, C.POINTER(vp)]
         L.mpg_kernel_timing.argtypes = [vp, ip]
         L.mpg_kernel_times.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
+        L.mpg_laplc_noalloc.argtypes = [vp, vp, vp, ip]
         _lib = L
     return _lib
 

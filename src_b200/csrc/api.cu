@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1088,4 +1089,54 @@ extern "C" int mpg_kernel_times(mpg_handle h, mpg_ktime *out, int max, int *coun
     }
     *count = n;
     return MPG_OK;
+}
+
+// ------------------------------------------------------------------------------ allocation-free laplc
+// Scratch of mpg_laplc_noalloc: the permuted input, the three scaled gradient components and the
+// permuted output, MPG_NOALLOC_MAX_NODES doubles each (5 x 131072 x 8 B = 5 MiB).  It is a
+// static device array, so every GPU that loads this library holds it until the process exits,
+// whether or not the entry point is ever called.
+static __device__ __align__(256) double g_noalloc_scratch[5 * (size_t)MPG_NOALLOC_MAX_NODES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+double *g_noalloc_addr[kNoallocMaxDevices] = {};
+std::mutex g_noalloc_mutex;
+}  // namespace
+
+extern "C" int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap, int impfl) {
+    if (!h || !press || !alap) return mpg_fail(MPG_ERR_ARG, "laplc_noalloc: null argument");
+    if (h->N > MPG_NOALLOC_MAX_NODES)
+        return mpg_fail(MPG_ERR_ARG, "laplc_noalloc: mesh has " + std::to_string(h->N) +
+                                         " nodes, more than the static scratch holds (" +
+                                         std::to_string(MPG_NOALLOC_MAX_NODES) + "); use mpg_laplc");
+    if (h->dev < 0 || h->dev >= kNoallocMaxDevices)
+        return mpg_fail(MPG_ERR_ARG, "laplc_noalloc: device index out of range");
+    if (press == alap) return mpg_fail(MPG_ERR_ARG, "laplc_noalloc: input and output must differ");
+    MPG_CUDA(cudaSetDevice(h->dev));
+    double *base;
+    {
+        // first call on this device: the host-side name of the array is not a device address, so
+        // ask the runtime for the device address once, with this device current
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_addr[h->dev]) {
+            void *ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr)
+                return mpg_fail(MPG_ERR_CUDA, std::string("laplc_noalloc: cudaGetSymbolAddress: ") +
+                                                  cudaGetErrorString(e));
+            g_noalloc_addr[h->dev] = (double *)ptr;
+        }
+        base = g_noalloc_addr[h->dev];
+    }
+    const size_t cap = MPG_NOALLOC_MAX_NODES;
+    double *pin = base, *F0 = base + cap, *F1 = base + 2 * cap, *F2 = base + 3 * cap, *aout = base + 4 * cap;
+    // every scratch element read below is written earlier in this call, so nothing needs clearing
+    const int N = h->N;
+    k_scatter_perm<<<grid(N), kThreads, 0, h->st>>>(N, h->d_perm, press, pin);
+    k_lap_grad<<<grid(N), kThreads, 0, h->st>>>(h->M, pin, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW], h->ue,
+                                                h->P.delt, impfl, F0, F1, F2);
+    k_lap_div<<<grid(N), kThreads, 0, h->st>>>(h->M, F0, F1, F2, h->vol, h->f[MPG_F_RH0], aout);
+    k_gather_perm<<<grid(N), kThreads, 0, h->st>>>(N, h->d_perm, aout, alap);
+    return check_launch("laplc_noalloc");
 }
