@@ -47,6 +47,7 @@ struct orc {
     int *colnodes;
     int nvert_e;
     int *vedge;         /* vertical edges: index into the combined edge list */
+    int blocked;        /* 1: global sums in the GPU's reduction order (see rsum) */
 };
 
 /* ------------------------------------------------------------------ helpers */
@@ -56,6 +57,65 @@ static int *iz(int n) { return (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int
 int orc_npoin(const orc *o) { return o->npoin; }
 double *orc_field(orc *o, int fid) { return (fid >= 0 && fid < MPG_F_COUNT) ? o->f[fid] : NULL; }
 double orc_beta(orc *o) { return o->betaunstr1; }
+
+/* ------------------------------------------------------------------ global sums
+ * The reference sums sequentially (k = 1..n).  With `blocked` set, sums follow the product's
+ * deterministic reduction order instead: 592 blocks x 256 threads, thread g adds v[g],
+ * v[g+151552], ... from 0.0; each warp folds its 32 partials by the shuffle tree
+ * (lane l += lane l+off for off = 16, 8, 4, 2, 1); thread 0 adds the 8 warp results in order;
+ * the block results are folded the same way by one final block (thread t adds results t, t+256,
+ * t+512).  Both orders are FP64 evaluations of the same sum; the blocked one lets the test
+ * suite check whole time steps bit for bit.  This is the only place the oracle departs from the
+ * reference's rounding, and only when asked to. */
+#define RB 592
+#define RT 256
+
+static double warp_tree(const double *lanes32) {
+    double a[32], b[32];
+    memcpy(a, lanes32, sizeof a);
+    for (int off = 16; off > 0; off >>= 1) {
+        for (int l = 0; l < 32; ++l) b[l] = a[l] + (l + off < 32 ? a[l + off] : a[l]);
+        memcpy(a, b, sizeof a);
+    }
+    return a[0];
+}
+
+static double block_fold(const double *thread_acc /* RT values */) {
+    double w[RT / 32];
+    for (int q = 0; q < RT / 32; ++q) w[q] = warp_tree(thread_acc + 32 * q);
+    double s = w[0];
+    for (int q = 1; q < RT / 32; ++q) s = s + w[q];
+    return s;
+}
+
+static double red_sum_blocked(const double *v, int n) {
+    static double part[RB];
+    double acc[RT];
+    const int stride = RB * RT;
+    for (int b = 0; b < RB; ++b) {
+        for (int t = 0; t < RT; ++t) {
+            double a = 0.;
+            for (int i = b * RT + t; i < n; i += stride) a = a + v[i];
+            acc[t] = a;
+        }
+        part[b] = block_fold(acc);
+    }
+    for (int t = 0; t < RT; ++t) {
+        double a = 0.;
+        for (int b = t; b < RB; b += RT) a = a + part[b];
+        acc[t] = a;
+    }
+    return block_fold(acc);
+}
+
+static double rsum(const orc *o, const double *v, int n) {
+    if (o->blocked) return red_sum_blocked(v, n);
+    double s = 0.;
+    for (int i = 0; i < n; ++i) s = s + v[i];
+    return s;
+}
+
+void orc_set_reduction(orc *o, int blocked) { o->blocked = blocked ? 1 : 0; }
 
 /* cyclicr, cyclicr2, cyclicr4 — ref.f:4377-4446 */
 static void cyclicr(orc *o, double *u) {
@@ -218,17 +278,21 @@ void orc_div(orc *o, const double *ua, const double *va, const double *wa, doubl
                                   + dwdz[ip] / o->vol[ip]) / rh0[ip];
     if (iflg == 1 && diag) {
         double divmx = -1.e15, divmn = 1.e15, divav = 0.;
+        double *tv = dz(n);
         for (int ip = 0; ip < n; ++ip) {
             divmx = AMAX(divmx, rhs[ip] * o->timestp[ip]);
             divmn = AMIN(divmn, rhs[ip] * o->timestp[ip]);
-            divav = divav + rhs[ip] * o->timestp[ip];
+            tv[ip] = rhs[ip] * o->timestp[ip];
         }
+        divav = rsum(o, tv, n);
         divav = divav / (double)n;
         double divsd = 0.;
         for (int ip = 0; ip < n; ++ip) {
             double t = rhs[ip] * o->timestp[ip] - divav;
-            divsd = divsd + t * t;
+            tv[ip] = t * t;
         }
+        divsd = rsum(o, tv, n);
+        free(tv);
         divsd = sqrt(divsd / n);
         diag->divmx = divmx; diag->divmn = divmn; diag->divav = divav; diag->divsd = divsd;
         diag->eer = o->eer; diag->eem = o->eem; diag->niter = o->niter;
@@ -405,11 +469,14 @@ void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const doubl
     orc_div(o, u2, v2, w2, r, -1, NULL);
     orc_precon(o, r, qr, ar, iprc, impfl);
     double eer0 = 0., eem0 = -1.e15, rl20 = 0.;
+    double *t1 = dz(nml), *t2 = dz(nml);
     for (int k = 0; k < nml; ++k) {
-        eer0 = eer0 + qr[k] * qr[k];
+        t1[k] = qr[k] * qr[k];
         eem0 = AMAX(eem0, fabs(qr[k]));
-        rl20 = rl20 + r[k] * r[k];
+        t2[k] = r[k] * r[k];
     }
+    eer0 = rsum(o, t1, nml);
+    rl20 = rsum(o, t2, nml);
     eer0 = AMAX(eer0, epa);
     eem0 = AMAX(eem0, epa);
     rl20 = AMAX(rl20, epa);
@@ -420,12 +487,12 @@ void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const doubl
     for (int it = 1; it <= o->P.itr; ++it) {
         for (int i = 1; i <= lord; ++i) {
             double *xi = x[i - 1], *axi = ax[i - 1];
-            double rax = 0.;
-            ax2[i - 1] = 0.;
             for (int k = 0; k < nml; ++k) {
-                rax = rax + r[k] * axi[k];
-                ax2[i - 1] = ax2[i - 1] + axi[k] * axi[k];
+                t1[k] = r[k] * axi[k];
+                t2[k] = axi[k] * axi[k];
             }
+            double rax = rsum(o, t1, nml);
+            ax2[i - 1] = rsum(o, t2, nml);
             ax2[i - 1] = AMAX(epa, ax2[i - 1]);
             double beta = -rax / ax2[i - 1];
             dvmx = -1.e15;
@@ -434,8 +501,9 @@ void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const doubl
                 p[k] = p[k] + beta * xi[k];
                 r[k] = r[k] + beta * axi[k];
                 dvmx = AMAX(dvmx, fabs(r[k]));
-                rl2 = rl2 + r[k] * r[k];
+                t1[k] = r[k] * r[k];
             }
+            rl2 = rsum(o, t1, nml);
             if (!(dvmx == dvmx) || !(rl2 == rl2)) { status = MPG_GCR_NAN; goto done; }
             if (dvmx <= eps && it >= itmn) { status = MPG_GCR_CONVERGED; goto done; }
             if (rl2 >= rl20) { status = MPG_GCR_STALLED; goto done; }
@@ -444,8 +512,8 @@ void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const doubl
             orc_laplc(o, qr, ar, impfl);
             nlc = nlc + 1;
             for (int ii = 1; ii <= i; ++ii) {
-                axar[ii - 1] = 0.;
-                for (int k = 0; k < nml; ++k) axar[ii - 1] = axar[ii - 1] + ax[ii - 1][k] * ar[k];
+                for (int k = 0; k < nml; ++k) t1[k] = ax[ii - 1][k] * ar[k];
+                axar[ii - 1] = rsum(o, t1, nml);
                 del[ii - 1] = -axar[ii - 1] / ax2[ii - 1];
             }
             if (i < lord) {
@@ -473,9 +541,11 @@ void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const doubl
 done:;
     double eer = 0., eem = -1.e15;                             /* ref.f:1953-1963 */
     for (int k = 0; k < nml; ++k) {
-        eer = eer + qr[k] * qr[k];
+        t1[k] = qr[k] * qr[k];
         eem = AMAX(eem, fabs(qr[k]));
     }
+    eer = rsum(o, t1, nml);
+    free(t1); free(t2);
     o->eer = eer / eer0;
     o->eem = eem / eem0;
     o->niter = nlc;
@@ -687,13 +757,16 @@ void orc_courant(orc *o, int iflag, mpg_diag *diag) {
     double crnmx = -1.e9, crnmn = 1.e9, crnav = 0., crnsd = 0.;
     int ic = 0;
     for (int ip = 0; ip < n; ++ip) {
-        crnav = crnav + cour[ip];
         crnmx = AMAX(crnmx, cour[ip]);
         crnmn = AMIN(crnmn, cour[ip]);
         if (crnmx == cour[ip]) ic = ip + 1;
     }
+    crnav = rsum(o, cour, n);
     crnav = crnav / n;
-    for (int ip = 0; ip < n; ++ip) crnsd = crnsd + (cour[ip] - crnav) * (cour[ip] - crnav);
+    double *tv = dz(n);
+    for (int ip = 0; ip < n; ++ip) tv[ip] = (cour[ip] - crnav) * (cour[ip] - crnav);
+    crnsd = rsum(o, tv, n);
+    free(tv);
     crnsd = sqrt(crnsd / n);
     if (diag) {
         diag->crnmx = crnmx; diag->crnmn = crnmn; diag->crnav = crnav; diag->crnsd = crnsd;
@@ -705,43 +778,49 @@ void orc_courant(orc *o, int iflag, mpg_diag *diag) {
 void orc_stats(orc *o, mpg_diag *diag) {
     int n = o->npoin;
     const double *rh0 = o->f[MPG_F_RH0];
-    double av[4] = {0, 0, 0, 0}, mx[4], mn[4], sd[4] = {0, 0, 0, 0}, rav = 0.;
+    double av[4], mx[4], mn[4], sd[4], rav;
+    double *tv = dz(n);
     for (int k = 0; k < 4; ++k) { mx[k] = -1.e10; mn[k] = 1.e10; }
-    for (int ip = 0; ip < n; ++ip) {
-        rav = rav + rh0[ip];
-        for (int k = 0; k < 4; ++k) {
-            double u = o->f[MPG_F_UNK + k][ip];
-            av[k] = av[k] + rh0[ip] * u;
-            mx[k] = AMAX(mx[k], u);
-            mn[k] = AMIN(mn[k], u);
+    rav = rsum(o, rh0, n);
+    for (int k = 0; k < 4; ++k) {
+        const double *u = o->f[MPG_F_UNK + k];
+        for (int ip = 0; ip < n; ++ip) {
+            tv[ip] = rh0[ip] * u[ip];
+            mx[k] = AMAX(mx[k], u[ip]);
+            mn[k] = AMIN(mn[k], u[ip]);
         }
+        av[k] = rsum(o, tv, n);
     }
     for (int k = 0; k < 4; ++k) av[k] = av[k] / rav;
-    for (int ip = 0; ip < n; ++ip)
-        for (int k = 0; k < 4; ++k) {
-            double t = o->f[MPG_F_UNK + k][ip] - av[k];
-            sd[k] = sd[k] + rh0[ip] * (t * t);
+    for (int k = 0; k < 4; ++k) {
+        const double *u = o->f[MPG_F_UNK + k];
+        for (int ip = 0; ip < n; ++ip) {
+            double t = u[ip] - av[k];
+            tv[ip] = rh0[ip] * (t * t);
         }
+        sd[k] = rsum(o, tv, n);
+    }
     for (int k = 0; k < 3; ++k) sd[k] = sqrt(sd[k] / rav);
     sd[3] = sqrt(sd[3] / n);                                   /* ref.f:2903 divides by npoin */
-    if (!diag) return;
-    for (int k = 0; k < 4; ++k) {
-        diag->stats[4 * k + 0] = mx[k]; diag->stats[4 * k + 1] = mn[k];
-        diag->stats[4 * k + 2] = av[k]; diag->stats[4 * k + 3] = sd[k];
+    if (diag) {
+        for (int k = 0; k < 4; ++k) {
+            diag->stats[4 * k + 0] = mx[k]; diag->stats[4 * k + 1] = mn[k];
+            diag->stats[4 * k + 2] = av[k]; diag->stats[4 * k + 3] = sd[k];
+        }
+        int nf = 4 + o->P.nscal;
+        for (int k = 0; k < nf && k < 8; ++k) {               /* NEW: FP64 mass sums */
+            const double *u = o->f[MPG_F_UNK + k];
+            for (int ip = 0; ip < n; ++ip) tv[ip] = o->vol[ip] * rh0[ip] * u[ip];
+            diag->mass[k] = rsum(o, tv, n);
+        }
+        for (int s = 0; s < o->P.nscal && s < 4; ++s) {
+            const double *u = o->f[MPG_F_UNK + 4 + s];
+            double a = 1.e300, b = -1.e300;
+            for (int ip = 0; ip < n; ++ip) { a = AMIN(a, u[ip]); b = AMAX(b, u[ip]); }
+            diag->smin[s] = a; diag->smax[s] = b;
+        }
     }
-    int nf = 4 + o->P.nscal;
-    for (int k = 0; k < nf && k < 8; ++k) {                   /* NEW: FP64 mass sums */
-        double s = 0.;
-        const double *u = o->f[MPG_F_UNK + k];
-        for (int ip = 0; ip < n; ++ip) s = s + o->vol[ip] * rh0[ip] * u[ip];
-        diag->mass[k] = s;
-    }
-    for (int s = 0; s < o->P.nscal && s < 4; ++s) {
-        const double *u = o->f[MPG_F_UNK + 4 + s];
-        double a = 1.e300, b = -1.e300;
-        for (int ip = 0; ip < n; ++ip) { a = AMIN(a, u[ip]); b = AMAX(b, u[ip]); }
-        diag->smin[s] = a; diag->smax[s] = b;
-    }
+    free(tv);
 }
 
 /* ------------------------------------------------------------------ set-up helpers */

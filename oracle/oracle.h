@@ -27,6 +27,9 @@ typedef struct orc orc;
 
 orc   *orc_create(const mpg_params *prm, const mpg_mesh_ref *mesh);
 void   orc_destroy(orc *o);
+/* 0 (default): global sums in the reference's sequential order; 1: in the GPU kernels' fixed
+ * reduction order, so that CPU and GPU runs can be compared bit for bit */
+void   orc_set_reduction(orc *o, int blocked);
 /* pointer to a field (same ids as the product) — n = npoin doubles */
 double *orc_field(orc *o, int fid);
 int    orc_npoin(const orc *o);

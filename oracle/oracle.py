@@ -53,6 +53,7 @@ def lib():
         L.orc_beta.restype = C.c_double
         L.orc_beta.argtypes = [vp]
         L.orc_line_solve.argtypes = [vp, dp, dp, ip]
+        L.orc_set_reduction.argtypes = [vp, ip]
         _lib = L
     return _lib
 
@@ -65,7 +66,7 @@ def _p(a: np.ndarray):
 class Oracle:
     """The reference restated on the CPU; fields addressed by the product's field ids."""
 
-    def __init__(self, params: RunParams, refmesh):
+    def __init__(self, params: RunParams, refmesh, gpu_order: bool = False):
         self.params = params
         self.mm = MeshMarshal(refmesh)
         self._cp = params.to_c()
@@ -74,6 +75,8 @@ class Oracle:
         if not self.h:
             raise ValueError("oracle rejected the parameters (isfera/mg_flag/nscal/lord)")
         self.n = refmesh.npoin
+        if gpu_order:
+            self.L.orc_set_reduction(self.h, 1)
 
     def __del__(self):
         h = getattr(self, "h", None)

@@ -1,9 +1,16 @@
 """GPU parity against the CPU oracle, through the C ABI.
 
 Operators whose per-node sums follow the reference's edge order (derivative, laplc, prfr, div,
-bcv, the line solve, precon, mpdatamper) must agree bit for bit.  Anything that goes through a
-global FP64 reduction (GCR inner products, diagnostics) is compared with the tolerances stated
-by the workload: relative L2 <= 1e-11 after one step, <= 1e-7 after 100 steps.
+bcv, the line solve, precon, mpdatamper) must agree bit for bit with the oracle.
+
+Global FP64 sums (GCR inner products, norms, diagnostics) are the only place where the order of
+operations is free.  Against the oracle in the reference's sequential order the workload's
+tolerances apply: relative L2 <= 1e-11 after one step and <= 1e-7 for the velocity after 100
+steps.  After many steps the GCR stopping test (max|r|*dt <= eps0) can stop one iteration
+earlier or later on the two sides when the residual sits at the tolerance, so small fields
+(theta', the transverse and vertical velocity) differ at the level the solver tolerance allows.
+With the oracle summing in the GPU's reduction order (`gpu_order=True`) every solve, step and
+diagnostic must agree bit for bit, for 100 steps.
 """
 import numpy as np
 import pytest
@@ -25,7 +32,7 @@ def rel(a, b):
 def pair(request, small_mesh, c1_mesh):
     cm, rm = small_mesh if request.param == "small" else c1_mesh
     P = RunParams(delt=10.0, nscal=1)
-    o = Oracle(P, rm)
+    o = Oracle(P, rm, gpu_order=True)
     o.setup()
     s = Solver(P, rm)
     s.setup()
@@ -146,7 +153,7 @@ def test_courant_bitwise(pair):
     assert abs(d.crnav - dref.crnav) <= 1e-13 * dref.crnav
 
 
-def test_gcrk_matches(pair):
+def test_gcrk_bitwise(pair):
     cm, rm, o, s = pair
     x, y, z = rm.coord.T
     bump = np.exp(-((x - 40e3) ** 2 + (y - 70e3) ** 2) / 15e3 ** 2 - (z - 6e3) ** 2 / 3e3 ** 2)
@@ -158,80 +165,117 @@ def test_gcrk_matches(pair):
     p, (u2, v2, w2), sto = o.gcrk(np.zeros(rm.npoin), u1[0], u1[1], u1[2], 1)
     assert st.status == sto.status == 0
     assert st.niter == sto.niter
-    # p carries null-space components of laplc (constants, odd-even modes) that the solve does
-    # not control, so it is compared loosely; the velocity the caller's prfr makes from it is
-    # what the step uses and must match to 1e-11
-    assert rel(s.get(W0), p) <= 1e-9
+    assert np.array_equal(s.get(W0), p)
     for k, ref in enumerate((u2, v2, w2)):
-        assert np.array_equal(s.get(W4 + k), ref)      # gcrk's prfr runs before any reduction
-    s.prfr(W0, W1, W2, W3, W4, W5, W6, 1)
-    uf = np.concatenate(o.prfr(p, u1[0], u1[1], u1[2], 1))
-    ug = np.concatenate([s.get(W4 + k) for k in range(3)])
-    assert rel(ug, uf) <= 1e-11
-    assert abs(st.eer - sto.eer) <= 1e-6 * sto.eer    # a ratio of residual-level norms
+        assert np.array_equal(s.get(W4 + k), ref)
+    assert st.eer == sto.eer and st.eem == sto.eem and st.dvmx == sto.dvmx and st.rl2 == sto.rl2
 
 
-def test_setup_matches(small_mesh):
+def test_gcrk_reference_order(small_mesh):
+    """Against the oracle's sequential sums: the velocity the caller's prfr makes agrees to 1e-11
+    (p itself carries null-space components of laplc that the solve does not control)."""
     cm, rm = small_mesh
     P = RunParams(delt=10.0)
     o = Oracle(P, rm)
+    o.setup()
+    with Solver(P, rm) as s:
+        s.setup()
+        x, y, z = rm.coord.T
+        bump = np.exp(-((x - 40e3) ** 2 + (y - 70e3) ** 2) / 15e3 ** 2 - (z - 6e3) ** 2 / 3e3 ** 2)
+        u1 = [o.get(F_UNK1 + k) + (0.5, -0.3, 0.2)[k] * bump for k in range(3)]
+        for k in range(3):
+            s.set(W1 + k, u1[k])
+        s.set(W0, 0.0)
+        st = s.gcrk(W0, W1, W2, W3, W4, W5, W6, 1)
+        p, _, sto = o.gcrk(np.zeros(rm.npoin), u1[0], u1[1], u1[2], 1)
+        assert st.status == sto.status == 0 and st.niter == sto.niter
+        assert rel(s.get(W0), p) <= 1e-9
+        s.prfr(W0, W1, W2, W3, W4, W5, W6, 1)
+        uf = np.concatenate(o.prfr(p, u1[0], u1[1], u1[2], 1))
+        ug = np.concatenate([s.get(W4 + k) for k in range(3)])
+        assert rel(ug, uf) <= 1e-11
+
+
+def test_setup_bitwise(small_mesh):
+    cm, rm = small_mesh
+    P = RunParams(delt=10.0)
+    o = Oracle(P, rm, gpu_order=True)
     do = o.setup()
     with Solver(P, rm) as s:
         d = s.setup()
-        for k in range(4):
-            assert rel(s.get(F_UNK + k), o.get(F_UNK + k)) <= 1e-11 or np.abs(o.get(F_UNK + k)).max() < 1e-12
-        for k in range(3):
-            assert rel(s.get(F_UUU + k), o.get(F_UUU + k)) <= 1e-11 or np.abs(o.get(F_UUU + k)).max() < 1e-12
-        assert d.niter == do.niter
-        assert abs(d.crnmx - do.crnmx) <= 1e-11 * do.crnmx
+        for fid in [F_UNK + k for k in range(4)] + [F_UUU + k for k in range(3)]:
+            assert np.array_equal(s.get(fid), o.get(fid)), fid
+        assert_diag_equal(d, do)
 
 
-def _run_steps(rm, nsteps, nscal=0):
+def assert_diag_equal(d, do):
+    a, b = d.as_dict(), do.as_dict()
+    for k in a:
+        assert a[k] == b[k], (k, a[k], b[k])
+
+
+def _run_steps(rm, nsteps, nscal=0, gpu_order=False, check_each=False):
     P = RunParams(delt=10.0, nscal=nscal)
-    o = Oracle(P, rm)
+    o = Oracle(P, rm, gpu_order=gpu_order)
     o.setup()
     s = Solver(P, rm)
     s.setup()
     if nscal:
         x, y, z = rm.coord.T
-        g = np.exp(-((x - 30e3) ** 2 + (y - 60e3) ** 2 + (z - 5e3) ** 2) / 5e3 ** 2)
+        g = np.exp(-((x - 30e3) ** 2 + (y - 60e3) ** 2 + (z - 5e3) ** 2) / (2 * 5e3 ** 2))
         o.set(F_UNK + 4, g)
         s.set(F_UNK + 4, g)
     for _ in range(nsteps):
         do = o.step()
         d = s.step()
+        if check_each:
+            assert (d.niter1, d.niter) == (do.niter1, do.niter)
     return o, s, d, do
 
 
-def test_one_step_c1(c1_mesh):
+def velocity_rel(o, s):
+    num = sum(np.sum((s.get(F_UNK + k) - o.get(F_UNK + k)) ** 2) for k in range(3))
+    den = sum(np.sum(o.get(F_UNK + k) ** 2) for k in range(3))
+    return np.sqrt(num / den)
+
+
+def test_one_step_c1_reference_order(c1_mesh):
     cm, rm = c1_mesh
     o, s, d, do = _run_steps(rm, 1)
     for k in range(4):
-        ref = o.get(F_UNK + k)
-        assert rel(s.get(F_UNK + k), ref) <= 1e-11, k
-    assert d.niter == do.niter
+        assert rel(s.get(F_UNK + k), o.get(F_UNK + k)) <= 1e-11, k
+    assert (d.niter1, d.niter) == (do.niter1, do.niter)
     for q in range(16):
         assert abs(d.stats[q] - do.stats[q]) <= 1e-9 * (abs(do.stats[q]) + 1e-3)
     s.close()
 
 
-def test_100_steps_small(small_mesh):
+def test_100_steps_small_bitwise(small_mesh):
+    cm, rm = small_mesh
+    o, s, d, do = _run_steps(rm, 100, nscal=1, gpu_order=True, check_each=True)
+    for k in range(5):
+        assert np.array_equal(s.get(F_UNK + k), o.get(F_UNK + k)), k
+    assert_diag_equal(d, do)
+    assert d.smin[0] >= 0.0                    # the passive scalar stays non-negative
+    s.close()
+
+
+def test_100_steps_small_reference_order(small_mesh):
     cm, rm = small_mesh
     o, s, d, do = _run_steps(rm, 100, nscal=1)
+    assert velocity_rel(o, s) <= 1e-7
     for k in range(5):
-        ref = o.get(F_UNK + k)
-        assert rel(s.get(F_UNK + k), ref) <= 1e-7, k
-    # mass of the passive scalar conserved to round-off, sign preserved
-    assert d.smin[0] >= 0.0
+        assert rel(s.get(F_UNK + k), o.get(F_UNK + k)) <= 1e-7, k
     s.close()
 
 
 @pytest.mark.slow
-def test_100_steps_c1(c1_mesh):
+def test_100_steps_c1_bitwise(c1_mesh):
     cm, rm = c1_mesh
-    o, s, d, do = _run_steps(rm, 100)
+    o, s, d, do = _run_steps(rm, 100, gpu_order=True, check_each=True)
     for k in range(4):
-        assert rel(s.get(F_UNK + k), o.get(F_UNK + k)) <= 1e-7, k
+        assert np.array_equal(s.get(F_UNK + k), o.get(F_UNK + k)), k
+    assert_diag_equal(d, do)
     s.close()
 
 
