@@ -312,8 +312,8 @@ void orc_div(orc *o, const double *ua, const double *va, const double *wa, doubl
  * Row i:  a_i = (sum of T below)/(vol_i*rh0_i),  c_i = (sum of T above)/(vol_i*rh0_i),
  *         Dh_i = -((0.5*dt)*((dhx+dhy)+dhz)) / ((4*vol_i)*rh0_i)   (non-vertical edges),
  *         b_i = (Dh_i - a_i) - c_i.
- * Thomas from the bottom: m_0=b_0, cp_k=c_k/m_k, m_k=b_k-a_k*cp_{k-1};
- *     d_k=(r_k-a_k*d_{k-1})/m_k;  z_top=d_top;  z_k=d_k-cp_k*z_{k+1}.            */
+ * Thomas from the bottom: m_0=b_0, cp_k=c_k/m_k, m_k=b_k-a_k*cp_{k-1}, inverse pivot 1/m_k;
+ *     d_k=(r_k-a_k*d_{k-1})*(1/m_k);  z_top=d_top;  z_k=d_k-cp_k*z_{k+1}.                 */
 static int is_vertical(orc *o, int i1, int i2) {
     return o->x[i1] == o->x[i2] && o->y[i1] == o->y[i2];
 }
@@ -388,9 +388,9 @@ static void line_coeffs(orc *o, int impfl, double *a, double *m, double *cp) {
         int s = o->colstart[col], t = o->colstart[col + 1];
         for (int k = s; k < t; ++k) {
             int i = o->colnodes[k];
-            if (k == s) m[i] = b[i];
-            else m[i] = b[i] - a[i] * cp[o->colnodes[k - 1]];
-            cp[i] = c[i] / m[i];
+            double mm = (k == s) ? b[i] : b[i] - a[i] * cp[o->colnodes[k - 1]];
+            cp[i] = c[i] / mm;
+            m[i] = 1. / mm;                               /* stored as the inverse pivot */
         }
     }
     free(Ta); free(Tc); free(hx); free(hy); free(hz); free(b); free(c);
@@ -404,8 +404,8 @@ void orc_line_solve(orc *o, const double *rhs, double *zout, int impfl) {
         int s = o->colstart[col], t = o->colstart[col + 1];
         for (int k = s; k < t; ++k) {
             int i = o->colnodes[k];
-            if (k == s) d[i] = rhs[i] / m[i];
-            else d[i] = (rhs[i] - a[i] * d[o->colnodes[k - 1]]) / m[i];
+            if (k == s) d[i] = rhs[i] * m[i];
+            else d[i] = (rhs[i] - a[i] * d[o->colnodes[k - 1]]) * m[i];
         }
         for (int k = t - 1; k >= s; --k) {
             int i = o->colnodes[k];

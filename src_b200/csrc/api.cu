@@ -47,7 +47,7 @@ struct mpg_solver {
     mpg_params P{};
     int dev = 0;
     cudaStream_t st = nullptr;
-    int32_t NC = 0, L = 0, N = 0, NE2 = 0;
+    int32_t NC = 0, L = 0, N = 0, NE2 = 0, kch = 1;
     bool bitwise = true;
     ColMesh M{};
     std::vector<void *> allocs;
@@ -62,7 +62,8 @@ struct mpg_solver {
     double *scal = nullptr, *part = nullptr, *result = nullptr, *h_res = nullptr;
     unsigned int *counter = nullptr;
     // line preconditioner
-    double *la[2] = {}, *lm[2] = {}, *lcp[2] = {};
+    double *la[2] = {}, *lm[2] = {}, *lcp[2] = {};   // a, 1/m, c' (interleaved)
+    double *dbuf = nullptr;                          // forward-sweep values (interleaved)
     // MPDATA scratch
     MpScratch S{};
     double *psi1 = nullptr, *g3[3] = {}, *mx = nullptr, *mn = nullptr;
@@ -146,6 +147,18 @@ int upload(mpg_handle h, T **p, const std::vector<T> &v) {
 
 inline int grid(int n) { return (n + kThreads - 1) / kThreads; }
 
+// launch a column-gather kernel template with the level-chunk count of the mesh
+#define COLL(kern, ...)                                                                      \
+    do {                                                                                     \
+        const dim3 g_((h->NC + kColWarps - 1) / kColWarps), b_(kColThreads);                 \
+        switch (h->kch) {                                                                    \
+            case 1: kern<1><<<g_, b_, 0, h->st>>>(__VA_ARGS__); break;                        \
+            case 2: kern<2><<<g_, b_, 0, h->st>>>(__VA_ARGS__); break;                        \
+            case 3: kern<3><<<g_, b_, 0, h->st>>>(__VA_ARGS__); break;                        \
+            default: kern<4><<<g_, b_, 0, h->st>>>(__VA_ARGS__); break;                       \
+        }                                                                                    \
+    } while (0)
+
 // field pointer, allocated (zeroed) on first use
 double *fld(mpg_handle h, int fid) {
     if (fid < 0 || fid >= MPG_F_COUNT) return nullptr;
@@ -217,11 +230,10 @@ int op_div(mpg_handle h, const double *ua, const double *va, const double *wa, d
 int op_line(mpg_handle h, const double *rhs, double *p, int impfl, int acc) {
     const int q = impfl ? 1 : 0;
     const int nblk = (h->NC + 32 * kLineWarps - 1) / (32 * kLineWarps);
-    const size_t smem = sizeof(double) * 32 * kLineWarps * h->L;
     {
         KTIME(KT_LINE);
-        k_line_solve<<<nblk, 32 * kLineWarps, smem, h->st>>>(h->NC, h->L, rhs, h->la[q], h->lm[q], h->lcp[q],
-                                                              h->P.omega, acc, p);
+        k_line_solve<<<nblk, 32 * kLineWarps, 0, h->st>>>(h->NC, h->L, rhs, h->la[q], h->lm[q], h->lcp[q],
+                                                          h->P.omega, acc, h->dbuf, p);
     }
     return check_launch("line_solve");
 }
@@ -370,6 +382,75 @@ int gcr_dots(mpg_handle h, int i) {
     return reduce<16>(h, 0u, ProdDots<16>{h->ar, ax, i}, fin);
 }
 
+// x(:,i+1) = qr + sum del(ii) x(:,ii), ax likewise (ref.f:1914-1923), or the restart collapse
+// into x(:,1) (ref.f:1924-1937), with the next iteration's r.ax and ax.ax (ref.f:1881-1884)
+// reduced in the same pass.  I = number of previous directions, known at compile time.
+template <int I, bool RESTART>
+struct ProdUpdate {
+    const double *scal, *qr, *ar, *r;
+    VecList x, ax;
+    double *xo, *axo;
+    __device__ void operator()(int n, double *v) const {
+        double a, b;
+        if (RESTART) {
+            a = qr[n] + scal[S_DEL] * x.v[0][n];
+            b = ar[n] + scal[S_DEL] * ax.v[0][n];
+#pragma unroll
+            for (int ii = 1; ii < I; ++ii) {
+                const double d = scal[S_DEL + ii];
+                a = a + d * x.v[ii][n];
+                b = b + d * ax.v[ii][n];
+            }
+        } else {
+            a = qr[n];
+            b = ar[n];
+#pragma unroll
+            for (int ii = 0; ii < I; ++ii) {
+                const double d = scal[S_DEL + ii];
+                a = a + d * x.v[ii][n];
+                b = b + d * ax.v[ii][n];
+            }
+        }
+        xo[n] = a;
+        axo[n] = b;
+        v[0] = r[n] * b;
+        v[1] = b * b;
+    }
+};
+
+template <int I>
+int gcr_update_n(mpg_handle h, int lord) {
+    VecList x{}, ax{};
+    for (int q = 0; q < lord; ++q) { x.v[q] = h->x[q]; ax.v[q] = h->ax[q]; }
+    if (I < lord) {
+        ProdUpdate<I, false> pu{h->scal, h->qr, h->ar, h->r, x, ax, h->x[I], h->ax[I]};
+        return reduce<2>(h, 0u, pu, FinBeta{h->scal, I});
+    }
+    ProdUpdate<I, true> pu{h->scal, h->qr, h->ar, h->r, x, ax, h->x[0], h->ax[0]};
+    return reduce<2>(h, 0u, pu, FinBeta{h->scal, 0});
+}
+
+int gcr_update(mpg_handle h, int i, int lord) {
+    switch (i) {
+        case 1: return gcr_update_n<1>(h, lord);
+        case 2: return gcr_update_n<2>(h, lord);
+        case 3: return gcr_update_n<3>(h, lord);
+        case 4: return gcr_update_n<4>(h, lord);
+        case 5: return gcr_update_n<5>(h, lord);
+        case 6: return gcr_update_n<6>(h, lord);
+        case 7: return gcr_update_n<7>(h, lord);
+        case 8: return gcr_update_n<8>(h, lord);
+        case 9: return gcr_update_n<9>(h, lord);
+        case 10: return gcr_update_n<10>(h, lord);
+        case 11: return gcr_update_n<11>(h, lord);
+        case 12: return gcr_update_n<12>(h, lord);
+        case 13: return gcr_update_n<13>(h, lord);
+        case 14: return gcr_update_n<14>(h, lord);
+        case 15: return gcr_update_n<15>(h, lord);
+        default: return gcr_update_n<16>(h, lord);
+    }
+}
+
 // gcrk(p, u1, v1, w1, u2, v2, w2, impfl) — ref.f:1776-1972
 int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const double *w1, double *u2,
             double *v2, double *w2, int impfl) {
@@ -394,7 +475,8 @@ int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const d
     for (int q = 0; q < lord; ++q) { xl.v[q] = h->x[q]; axl.v[q] = h->ax[q]; }
     for (int it = 1; it <= P.itr && status == MPG_GCR_MAXIT; ++it) {
         for (int i = 1; i <= lord; ++i) {
-            if ((rc = reduce<2>(h, 0u, ProdDot2{h->r, h->ax[i - 1]}, FinBeta{h->scal, i - 1}))) return rc;
+            if (it == 1 && i == 1)      // later iterations get (r.ax, ax.ax) from gcr_update
+                if ((rc = reduce<2>(h, 0u, ProdDot2{h->r, h->ax[0]}, FinBeta{h->scal, 0}))) return rc;
             if ((rc = reduce<2>(h, 0x1u, ProdAxpy{h->scal, h->x[i - 1], h->ax[i - 1], p, h->r}, NoFin{})))
                 return rc;
             if ((rc = fetch_result(h, 2))) return rc;
@@ -408,17 +490,8 @@ int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const d
             if ((rc = op_laplc(h, h->qr, h->ar, impfl))) return rc;
             nlc = nlc + 1;
             if ((rc = gcr_dots(h, i))) return rc;
-            if (i < lord) {
-                {
-                    KTIME(KT_GCR_UPD);
-                    k_gcr_next<<<grid(N), kThreads, 0, h->st>>>(N, i, h->scal, h->qr, h->ar, xl, axl, h->x[i], h->ax[i]);
-                }
-            } else {
-                {
-                    KTIME(KT_GCR_UPD);
-                    k_gcr_restart<<<grid(N), kThreads, 0, h->st>>>(N, i, h->scal, h->qr, h->ar, xl, axl);
-                }
-            }
+            // direction update fused with the next iteration's (r.ax, ax.ax) reduction
+            if ((rc = gcr_update(h, i, lord))) return rc;
             if ((rc = check_launch("gcr update"))) return rc;
         }
     }
@@ -676,6 +749,8 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete h; return mpg_fail(MPG_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e)); }
     h->NC = hm.NC; h->L = hm.L; h->N = hm.N; h->NE2 = hm.NE2;
+    if (hm.L > 128) { delete h; return mpg_fail(MPG_ERR_MESH, "more than 128 levels per column"); }
+    h->kch = (hm.L + 31) / 32;
     h->bitwise = hm.bitwise_order;
     h->betaunstr1 = h->hs.betaunstr1;
     h->iperm = hm.iperm;
@@ -738,14 +813,7 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
         if ((rc = dalloc(h, &h->g3[q], N))) return fail(rc);
     h->S = MpScratch{aunh, aunv, Ah, Av, h->d_e2a, h->d_e2b};
     if ((rc = upload(h, &h->d_iperm, hm.iperm))) return fail(rc);
-    // the column solve stages 32*kLineWarps columns of L levels; the attribute only ever grows,
-    // so handles with fewer levels keep working
-    const size_t smem = sizeof(double) * 32 * kLineWarps * h->L;
-    cudaFuncAttributes fa{};
-    e = cudaFuncGetAttributes(&fa, k_line_solve);
-    if (e == cudaSuccess && (size_t)fa.maxDynamicSharedSizeBytes < smem)
-        e = cudaFuncSetAttribute(k_line_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return fail(mpg_fail(MPG_ERR_MESH, "too many levels for the column solve's shared memory"));
+    if ((rc = dalloc(h, &h->dbuf, h->hs.la[0].size()))) return fail(rc);
     e = cudaStreamSynchronize(h->st);
     if (e != cudaSuccess) return fail(mpg_fail(MPG_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e)));
     *out = h;
@@ -1134,9 +1202,9 @@ extern "C" int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap
     // every scratch element read below is written earlier in this call, so nothing needs clearing
     const int N = h->N;
     k_scatter_perm<<<grid(N), kThreads, 0, h->st>>>(N, h->d_perm, press, pin);
-    k_lap_grad<<<grid(N), kThreads, 0, h->st>>>(h->M, pin, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW], h->ue,
+    k_lap_grad<<<grid(h->N), kThreads, 0, h->st>>>(h->M, pin, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW], h->ue,
                                                 h->P.delt, impfl, F0, F1, F2);
-    k_lap_div<<<grid(N), kThreads, 0, h->st>>>(h->M, F0, F1, F2, h->vol, h->f[MPG_F_RH0], aout);
+    k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, F0, F1, F2, h->vol, h->f[MPG_F_RH0], aout);
     k_gather_perm<<<grid(N), kThreads, 0, h->st>>>(N, h->d_perm, aout, alap);
     return check_launch("laplc_noalloc");
 }

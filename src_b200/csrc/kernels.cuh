@@ -26,33 +26,56 @@ constexpr int kMaxQ = 24;                // quantities per reduction
 __device__ __forceinline__ double amax(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double amin(double a, double b) { return a < b ? a : b; }
 
-__device__ __forceinline__ void col_lev(const ColMesh &M, int n, int &c, int &k) {
-    c = n / M.L;
-    k = n - c * M.L;
+// ------------------------------------------------------------------------------ gathers
+// Thread n = c*L + k visits the faces of node (c,k) in the reference's edge order.  The loop is
+// branch-free and takes two faces per iteration: both faces' operands are loaded before either
+// is accumulated, which doubles the loads in flight of this latency-bound gather while keeping
+// the reference's order of additions.
+struct Face {
+    int j;        // neighbour node
+    int si;       // face index into Sv (vert) or Sh
+    bool sub;     // the reference stores the face with this node second: subtract
+    bool vert;
+    bool valid;   // false for the missing vertical face at the column's bottom or top
+};
+
+__device__ __forceinline__ Face decode_face(int2 en, int n, int k, int L) {
+    Face f;
+    const bool vert = en.x < 0, below = en.x == MPG_ADJ_BELOW;
+    f.vert = vert;
+    f.valid = !vert || (below ? k > 0 : k + 1 < L);
+    f.sub = vert ? below : ((en.x & 1) != 0);
+    const int jv = below ? n - 1 : n + 1, sv = below ? n - 1 : n;
+    f.j = vert ? (f.valid ? jv : n) : en.y * L + k;
+    f.si = vert ? (f.valid ? sv : n) : (en.x >> 1) * L + k;
+    return f;
 }
 
-// ------------------------------------------------------------------------------ gathers
-// Visits the faces of node n = (c,k) in reference edge order.  For each face the visitor gets
-// the neighbour node j, the face-vector index (into Sh or Sv) and whether the face is stored
-// with this node as its second end (then the reference subtracts).
-template <class V>
-__device__ __forceinline__ void for_faces(const ColMesh &M, int c, int k, int n, V &&visit) {
+template <int U = 2, class LD, class AC>
+__device__ __forceinline__ void for_faces(const ColMesh &M, int c, int k, int n, LD &&load, AC &&acc) {
     const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
     const int L = M.L;
-    for (int j = beg; j < end; ++j) {
-        const int2 en = __ldg(&M.cadj[j]);
-        if (en.x >= 0) {
-            visit(en.y * L + k, (en.x >> 1) * L + k, (en.x & 1) != 0, false);
-        } else if (en.x == MPG_ADJ_BELOW) {
-            if (k > 0) visit(n - 1, n - 1, true, true);
-        } else {
-            if (k + 1 < L) visit(n + 1, n, false, true);
-        }
+    int j = beg;
+    for (; j + U <= end; j += U) {
+        Face f[U];
+        decltype(load(f[0])) v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) f[u] = decode_face(__ldg(&M.cadj[j + u]), n, k, L);
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] = load(f[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (f[u].valid) acc(f[u], v[u]);
+    }
+    for (; j < end; ++j) {
+        const Face f = decode_face(__ldg(&M.cadj[j]), n, k, L);
+        const auto v = load(f);
+        if (f.valid) acc(f, v);
     }
 }
 
-__device__ __forceinline__ double sh(const ColMesh &M, int d, int idx, bool vert) {
-    return vert ? __ldg(&M.Sv[d][idx]) : __ldg(&M.Sh[d][idx]);
+__device__ __forceinline__ const double *spick(const ColMesh &M, int d, bool vert) {
+    return vert ? M.Sv[d] : M.Sh[d];
 }
 
 // Boundary entries of node (c,k), in reference order.
@@ -65,20 +88,26 @@ __device__ __forceinline__ void for_boundary(const ColMesh &M, int c, int k, V &
     }
 }
 
+struct V4 { double a, b, c, d; };
+struct V6 { double a, b, c, d, e, f; };
+
 // derivative (ref.f:3943-4022) of phi for the three components at once:
 // g_d = sum over faces of (+/-) S_d * ((phi_n + phi_j) * 0.5)
 __device__ __forceinline__ void grad3(const ColMesh &M, const double *__restrict__ phi, int c, int k,
                                       int n, double &gx, double &gy, double &gz) {
     const double pn = phi[n];
     double ax = 0., ay = 0., az = 0.;
-    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
-        const double u = (pn + phi[j]) * 0.5;
-        const double tx = sh(M, 0, si, vert) * u;
-        const double ty = sh(M, 1, si, vert) * u;
-        const double tz = sh(M, 2, si, vert) * u;
-        if (sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
-        else     { ax = ax + tx; ay = ay + ty; az = az + tz; }
-    });
+    for_faces(M, c, k, n,
+        [&](const Face &f) {
+            return V4{__ldg(spick(M, 0, f.vert) + f.si), __ldg(spick(M, 1, f.vert) + f.si),
+                      __ldg(spick(M, 2, f.vert) + f.si), phi[f.j]};
+        },
+        [&](const Face &f, const V4 &v) {
+            const double u = (pn + v.d) * 0.5;
+            const double tx = v.a * u, ty = v.b * u, tz = v.c * u;
+            if (f.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
+            else       { ax = ax + tx; ay = ay + ty; az = az + tz; }
+        });
     if (M.iper == 0) {                                  // closure, ref.f:4007-4014
         for_boundary(M, c, k, [&](const BEntry &be) {
             ax = ax + be.sbb[0] * pn;
@@ -89,23 +118,29 @@ __device__ __forceinline__ void grad3(const ColMesh &M, const double *__restrict
     gx = ax; gy = ay; gz = az;
 }
 
-// three derivatives of three different fields, component d of field d (the divergence):
-// returns derivative(fx,1), derivative(fy,2), derivative(fz,3)
+// derivative(fx,1), derivative(fy,2), derivative(fz,3) of three fields (the divergence)
 template <class FX>
 __device__ __forceinline__ void div3(const ColMesh &M, FX f, int c, int k, int n,
                                      double &dx, double &dy, double &dz) {
     double fnx, fny, fnz;
     f(n, fnx, fny, fnz);
     double ax = 0., ay = 0., az = 0.;
-    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
-        double fjx, fjy, fjz;
-        f(j, fjx, fjy, fjz);
-        const double tx = sh(M, 0, si, vert) * ((fnx + fjx) * 0.5);
-        const double ty = sh(M, 1, si, vert) * ((fny + fjy) * 0.5);
-        const double tz = sh(M, 2, si, vert) * ((fnz + fjz) * 0.5);
-        if (sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
-        else     { ax = ax + tx; ay = ay + ty; az = az + tz; }
-    });
+    for_faces(M, c, k, n,
+        [&](const Face &fc) {
+            V6 v;
+            v.a = __ldg(spick(M, 0, fc.vert) + fc.si);
+            v.b = __ldg(spick(M, 1, fc.vert) + fc.si);
+            v.c = __ldg(spick(M, 2, fc.vert) + fc.si);
+            f(fc.j, v.d, v.e, v.f);
+            return v;
+        },
+        [&](const Face &fc, const V6 &v) {
+            const double tx = v.a * ((fnx + v.d) * 0.5);
+            const double ty = v.b * ((fny + v.e) * 0.5);
+            const double tz = v.c * ((fnz + v.f) * 0.5);
+            if (fc.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
+            else        { ax = ax + tx; ay = ay + ty; az = az + tz; }
+        });
     if (M.iper == 0) {
         for_boundary(M, c, k, [&](const BEntry &be) {
             ax = ax + be.sbb[0] * fnx;
@@ -133,12 +168,17 @@ __device__ __forceinline__ void bcv_node(const ColMesh &M, int c, int k, int n, 
 }
 
 // ------------------------------------------------------------------------------ operators
+// latency-bound gathers that fit 40 registers without spilling: keep 6 blocks (48 warps) per SM
+#define GATHER_BOUNDS __launch_bounds__(kThreads, 6)
+
+#define NODE_BEGIN                                                            \
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;                      \
+    if (n >= M.N) return;                                                     \
+    const int c = n / M.L, k = n - c * M.L;
+
 // derivative(unk, out, idx)
-__global__ void k_derivative(ColMesh M, const double *__restrict__ phi, double *__restrict__ out, int idx) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+__global__ void GATHER_BOUNDS k_derivative(ColMesh M, const double *__restrict__ phi, double *__restrict__ out, int idx) {
+    NODE_BEGIN
     double gx, gy, gz;
     grad3(M, phi, c, k, n, gx, gy, gz);
     out[n] = idx == 1 ? gx : idx == 2 ? gy : gz;
@@ -146,10 +186,7 @@ __global__ void k_derivative(ColMesh M, const double *__restrict__ phi, double *
 
 // bcv(u, v, w, flag) on whole fields
 __global__ void k_bcv(ColMesh M, double *u, double *v, double *w, const double *__restrict__ ue, double flag) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     if (__ldg(&M.bptr[c]) == __ldg(&M.bptr[c + 1])) return;
     double a = u[n], b = v[n], d = w[n];
     bcv_node(M, c, k, n, ue, flag, a, b, d);
@@ -157,14 +194,11 @@ __global__ void k_bcv(ColMesh M, double *u, double *v, double *w, const double *
 }
 
 // laplc first half (ref.f:1303-1338): gradient, scaling, bcv(.,0.), times rh0
-__global__ void k_lap_grad(ColMesh M, const double *__restrict__ p, const double *__restrict__ vol,
+__global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const double *__restrict__ p, const double *__restrict__ vol,
                            const double *__restrict__ rh0, const double *__restrict__ coefw,
                            const double *__restrict__ ue, double dt, int impfl,
                            double *__restrict__ Fx, double *__restrict__ Fy, double *__restrict__ Fz) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     double gx, gy, gz;
     grad3(M, p, c, k, n, gx, gy, gz);
     const double v = vol[n];
@@ -181,25 +215,19 @@ __global__ void k_lap_grad(ColMesh M, const double *__restrict__ p, const double
 __global__ void k_lap_div(ColMesh M, const double *__restrict__ Fx, const double *__restrict__ Fy,
                           const double *__restrict__ Fz, const double *__restrict__ vol,
                           const double *__restrict__ rh0, double *__restrict__ alap) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     double dx, dy, dz;
     div3(M, [&](int j, double &a, double &b, double &d) { a = Fx[j]; b = Fy[j]; d = Fz[j]; }, c, k, n, dx, dy, dz);
     alap[n] = (dx + dy + dz) / (vol[n] * rh0[n]);
 }
 
 // prfr (ref.f:1536-1580)
-__global__ void k_prfr(ColMesh M, const double *__restrict__ p, const double *__restrict__ us,
+__global__ void GATHER_BOUNDS k_prfr(ColMesh M, const double *__restrict__ p, const double *__restrict__ us,
                        const double *__restrict__ vs, const double *__restrict__ ws,
                        const double *__restrict__ vol, const double *__restrict__ coefw,
                        const double *__restrict__ ue, double dt, int impfl,
                        double *__restrict__ uo, double *__restrict__ vo, double *__restrict__ wo) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     double gx, gy, gz;
     grad3(M, p, c, k, n, gx, gy, gz);
     const double v = vol[n];
@@ -215,10 +243,7 @@ __global__ void k_prfr(ColMesh M, const double *__restrict__ p, const double *__
 __global__ void k_div(ColMesh M, const double *__restrict__ ua, const double *__restrict__ va,
                       const double *__restrict__ wa, const double *__restrict__ vol,
                       const double *__restrict__ rh0, int iflg, double *__restrict__ rhs) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     double dx, dy, dz;
     if (iflg == -1)
         div3(M, [&](int j, double &a, double &b, double &d) {
@@ -231,46 +256,65 @@ __global__ void k_div(ColMesh M, const double *__restrict__ ua, const double *__
 
 // ------------------------------------------------------------------------------ line solve
 // z = M^{-1} rhs per column (Thomas, FP64, bottom to top), p = (acc ? p : 0) + omega * z.
-// Each warp solves 32 consecutive columns; their right-hand sides (contiguous in the column
-// layout) are staged through shared memory with coalesced loads and stores, and the
-// coefficients are stored interleaved so that the 32 lanes read level k of their columns
-// from one 256-byte segment.
-constexpr int kLineWarps = 4;
+// A warp owns 32 consecutive columns.  Their right-hand sides (contiguous in the column layout)
+// pass through a 32 x kLineChunk shared-memory tile, loaded and stored with coalesced accesses;
+// the factorisation (a, 1/m, c') and the forward-sweep values d are stored interleaved
+// (line_index), so lane l reads and writes level k of column col0+l inside one 256-byte segment.
+// With 4 KiB of shared memory per warp the kernel keeps enough warps resident to stream.
+constexpr int kLineWarps = 8;
+constexpr int kLineChunk = 16;
 __global__ void __launch_bounds__(32 * kLineWarps)
 k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__restrict__ la,
-             const double *__restrict__ lm, const double *__restrict__ lcp, double omega, int acc,
-             double *__restrict__ p) {
-    extern __shared__ double sm[];
+             const double *__restrict__ linv, const double *__restrict__ lcp, double omega, int acc,
+             double *__restrict__ dbuf, double *__restrict__ p) {
+    __shared__ double tile[kLineWarps][32][kLineChunk + 1];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col0 = (blockIdx.x * kLineWarps + w) * 32;
     if (col0 >= NC) return;
     const int ncols = min(32, NC - col0);
-    double *s = sm + (size_t)w * 32 * L;
-    const int64_t base = (int64_t)col0 * L;
-    const int cnt = ncols * L;
-    for (int i = lane; i < cnt; i += 32) s[i] = rhs[base + i];
-    __syncwarp();
-    if (lane < ncols) {
-        const int c = col0 + lane;
-        double *sc = s + lane * L;
-        double d = 0.;
-        for (int k = 0; k < L; ++k) {
-            const int64_t li = line_index(c, k, L);
-            const double m = lm[li];
-            d = (k == 0) ? sc[0] / m : (sc[k] - la[li] * d) / m;
-            sc[k] = d;
+    double(*t)[kLineChunk + 1] = tile[w];
+    const int c = col0 + lane;
+    const bool own = lane < ncols;
+    // forward sweep: d_k = (r_k - a_k d_{k-1}) / m_k
+    double d = 0.;
+    for (int k0 = 0; k0 < L; k0 += kLineChunk) {
+        const int nk = min(kLineChunk, L - k0);
+        for (int i = lane; i < ncols * nk; i += 32) {
+            const int cc = i / nk, kk = i - cc * nk;
+            t[cc][kk] = rhs[(int64_t)(col0 + cc) * L + k0 + kk];
         }
-        double z = 0.;
-        for (int k = L - 1; k >= 0; --k) {
-            const int64_t li = line_index(c, k, L);
-            z = (k == L - 1) ? sc[k] : sc[k] - lcp[li] * z;
-            sc[k] = z;
+        __syncwarp();
+        if (own) {
+            for (int kk = 0; kk < nk; ++kk) {
+                const int k = k0 + kk;
+                const int64_t li = line_index(c, k, L);
+                d = (k == 0) ? t[lane][kk] * linv[li] : (t[lane][kk] - la[li] * d) * linv[li];
+                dbuf[li] = d;
+            }
         }
+        __syncwarp();
     }
-    __syncwarp();
-    for (int i = lane; i < cnt; i += 32) {
-        const double prev = acc ? p[base + i] : 0.0;
-        p[base + i] = prev + omega * s[i];
+    // backward sweep: z_k = d_k - c'_k z_{k+1}, top chunk first
+    double z = 0.;
+    const int last0 = ((L - 1) / kLineChunk) * kLineChunk;
+    for (int k0 = last0; k0 >= 0; k0 -= kLineChunk) {
+        const int nk = min(kLineChunk, L - k0);
+        if (own) {
+            for (int kk = nk - 1; kk >= 0; --kk) {
+                const int k = k0 + kk;
+                const int64_t li = line_index(c, k, L);
+                z = (k == L - 1) ? dbuf[li] : dbuf[li] - lcp[li] * z;
+                t[lane][kk] = z;
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < ncols * nk; i += 32) {
+            const int cc = i / nk, kk = i - cc * nk;
+            const int64_t g = (int64_t)(col0 + cc) * L + k0 + kk;
+            const double prev = acc ? p[g] : 0.0;
+            p[g] = prev + omega * t[cc][kk];
+        }
+        __syncwarp();
     }
 }
 
@@ -385,36 +429,6 @@ __global__ void k_axpy_pr(int N, const double *__restrict__ scal, const double *
 struct VecList {
     double *v[MPG_MAX_LORD];
 };
-__global__ void k_gcr_next(int N, int i, const double *__restrict__ scal, const double *__restrict__ qr,
-                           const double *__restrict__ ar, VecList x, VecList ax, double *__restrict__ xo,
-                           double *__restrict__ axo) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    double a = qr[n], b = ar[n];
-    for (int ii = 0; ii < i; ++ii) {
-        const double d = scal[S_DEL + ii];
-        a = a + d * x.v[ii][n];
-        b = b + d * ax.v[ii][n];
-    }
-    xo[n] = a;
-    axo[n] = b;
-}
-
-// restart collapse (ref.f:1924-1937): x(:,1) = qr + del(1) x(:,1) + sum_{ii>=2} del(ii) x(:,ii)
-__global__ void k_gcr_restart(int N, int i, const double *__restrict__ scal, const double *__restrict__ qr,
-                              const double *__restrict__ ar, VecList x, VecList ax) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    double a = qr[n] + scal[S_DEL] * x.v[0][n];
-    double b = ar[n] + scal[S_DEL] * ax.v[0][n];
-    for (int ii = 1; ii < i; ++ii) {
-        const double d = scal[S_DEL + ii];
-        a = a + d * x.v[ii][n];
-        b = b + d * ax.v[ii][n];
-    }
-    x.v[0][n] = a;
-    ax.v[0][n] = b;
-}
 
 // ------------------------------------------------------------------------------ element-wise
 __global__ void k_fill(int N, double *__restrict__ a, double v) {

@@ -62,18 +62,17 @@ __device__ __forceinline__ bool has_boundary(const ColMesh &M, int c, int k) {
 __global__ void k_mp_donor(ColMesh M, MpScratch S, const double *__restrict__ psi,
                            const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
                            double *__restrict__ psi1) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     const double pn = psi[n];
     double arh2 = 0.;
-    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
-        const double aun = face_val(S.aunh, S.aunv, si, vert);
-        const double pa = sub ? psi[j] : pn, pb = sub ? pn : psi[j];
-        const double fl = pa * amax(0., aun) + pb * amin(0., aun);
-        arh2 = sub ? arh2 - fl : arh2 + fl;
-    });
+    for_faces(M, c, k, n,
+        [&](const Face &f) { return V4{(f.vert ? S.aunv : S.aunh)[f.si], psi[f.j], 0., 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double aun = v.a;
+            const double pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
+            const double fl = pa * amax(0., aun) + pb * amin(0., aun);
+            arh2 = f.sub ? arh2 - fl : arh2 + fl;
+        });
     if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;          // zero boundary flux, ref.f:3732-3738
     psi1[n] = pn - arh2 * dt / vol[n] / rh0[n];
 }
@@ -82,23 +81,23 @@ __global__ void k_mp_donor(ColMesh M, MpScratch S, const double *__restrict__ ps
 __global__ void k_mp_grad_bounds(ColMesh M, const double *__restrict__ psi1, double *__restrict__ gx,
                                  double *__restrict__ gy, double *__restrict__ gz,
                                  double *__restrict__ mx, double *__restrict__ mn) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     const double pn = psi1[n];
     double ax = 0., ay = 0., az = 0., hi = -1.e15, lo = 1.e15;
-    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
-        const double pj = psi1[j];
-        const double u = (pn + pj) * 0.5;
-        const double tx = sh(M, 0, si, vert) * u;
-        const double ty = sh(M, 1, si, vert) * u;
-        const double tz = sh(M, 2, si, vert) * u;
-        if (sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
-        else     { ax = ax + tx; ay = ay + ty; az = az + tz; }
-        hi = amax(amax(hi, pn), pj);
-        lo = amin(amin(lo, pn), pj);
-    });
+    for_faces(M, c, k, n,
+        [&](const Face &f) {
+            return V4{__ldg(spick(M, 0, f.vert) + f.si), __ldg(spick(M, 1, f.vert) + f.si),
+                      __ldg(spick(M, 2, f.vert) + f.si), psi1[f.j]};
+        },
+        [&](const Face &f, const V4 &v) {
+            const double pj = v.d;
+            const double u = (pn + pj) * 0.5;
+            const double tx = v.a * u, ty = v.b * u, tz = v.c * u;
+            if (f.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
+            else       { ax = ax + tx; ay = ay + ty; az = az + tz; }
+            hi = amax(amax(hi, pn), pj);
+            lo = amin(amin(lo, pn), pj);
+        });
     gx[n] = ax; gy[n] = ay; gz[n] = az;
     mx[n] = hi; mn[n] = lo;
 }
@@ -142,17 +141,16 @@ __global__ void k_mp_cpcn(ColMesh M, MpScratch S, const double *__restrict__ psi
                           const double *__restrict__ mx, const double *__restrict__ mn,
                           const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
                           double *__restrict__ cp, double *__restrict__ cn) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     double rin = 0., rout = 0.;
-    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
-        const double a = face_val(S.Ah, S.Av, si, vert);
-        const double pp = amax(0., a), pn = -amin(0., a);
-        if (!sub) { rin = rin + pn; rout = rout + pp; }
-        else      { rin = rin + pp; rout = rout + pn; }
-    });
+    for_faces(M, c, k, n,
+        [&](const Face &f) { return V4{(f.vert ? S.Av : S.Ah)[f.si], 0., 0., 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double a = v.a;
+            const double pp = amax(0., a), pn = -amin(0., a);
+            if (!f.sub) { rin = rin + pn; rout = rout + pp; }
+            else        { rin = rin + pp; rout = rout + pn; }
+        });
     const double tol = 1.e-10;
     const double p = psi1[n], v = vol[n], r = rh0[n];
     cp[n] = (mx[n] - p) * v * r / (rin * dt + tol);
@@ -164,20 +162,19 @@ __global__ void k_mp_pass2(ColMesh M, MpScratch S, const double *__restrict__ ps
                            const double *__restrict__ cp, const double *__restrict__ cn,
                            const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
                            double *__restrict__ psi2) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
     const double cpn = cp[n], cnn = cn[n];
     double arh2 = 0.;
-    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
-        const double a = face_val(S.Ah, S.Av, si, vert);
-        // canonical ends: first = this node unless sub
-        const double cpa = sub ? cp[j] : cpn, cna = sub ? cn[j] : cnn;
-        const double cpb = sub ? cpn : cp[j], cnb = sub ? cnn : cn[j];
-        const double lim = a > 0. ? a * amin(amin(1., cpb), cna) : a * amin(amin(1., cnb), cpa);
-        arh2 = sub ? arh2 - lim : arh2 + lim;
-    });
+    for_faces(M, c, k, n,
+        [&](const Face &f) { return V4{(f.vert ? S.Av : S.Ah)[f.si], cp[f.j], cn[f.j], 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double a = v.a;
+            // canonical ends: first = this node unless sub
+            const double cpa = f.sub ? v.b : cpn, cna = f.sub ? v.c : cnn;
+            const double cpb = f.sub ? cpn : v.b, cnb = f.sub ? cnn : v.c;
+            const double lim = a > 0. ? a * amin(amin(1., cpb), cna) : a * amin(amin(1., cnb), cpa);
+            arh2 = f.sub ? arh2 - lim : arh2 + lim;
+        });
     if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;
     psi2[n] = psi1[n] - arh2 * dt / vol[n] / rh0[n];
 }
@@ -300,30 +297,37 @@ __global__ void k_setup_post(int N, Fields F, double *prpot) {
 // courant(uuu, cour, iflag) node part (ref.f:1994-2069): sum of |aun|/rhav over the faces
 __global__ void k_courant(ColMesh M, U3 U, const double *__restrict__ rh0, const double *__restrict__ vol,
                           double dt, int iflag, double *__restrict__ cour) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= M.N) return;
-    int c, k;
-    col_lev(M, n, c, k);
+    NODE_BEGIN
+    const double un0 = U.u[0][n], un1 = U.u[1][n], un2 = U.u[2][n], rn = rh0[n];
     double s = 0.;
-    for_faces(M, c, k, n, [&](int j, int si, bool sub, bool vert) {
-        const int a = sub ? j : n, b = sub ? n : j;
-        const double rhav = 0.5 * (rh0[a] + rh0[b]);
-        double aun = face_aun(U.u, a, b, sh(M, 0, si, vert), sh(M, 1, si, vert), sh(M, 2, si, vert));
-        aun = aun / rhav;
-        if (iflag == 1) s = s + fabs(aun);
-        else if (iflag == 2) s = sub ? s - aun : s + aun;
-        else s = sub ? s - amin(0., aun) : s + amax(0., aun);
-    });
+    for_faces(M, c, k, n,
+        [&](const Face &f) {
+            V6 v;
+            v.a = __ldg(spick(M, 0, f.vert) + f.si);
+            v.b = __ldg(spick(M, 1, f.vert) + f.si);
+            v.c = __ldg(spick(M, 2, f.vert) + f.si);
+            v.d = U.u[0][f.j]; v.e = U.u[1][f.j]; v.f = U.u[2][f.j];
+            return v;
+        },
+        [&](const Face &f, const V6 &v) {
+            const double rhav = 0.5 * (rn + rh0[f.j]);
+            // (U_a + U_b): the sum is symmetric, so the order of the ends does not matter
+            double aun = (un0 + v.d) * 0.5 * v.a + (un1 + v.e) * 0.5 * v.b + (un2 + v.f) * 0.5 * v.c;
+            aun = aun / rhav;
+            if (iflag == 1) s = s + fabs(aun);
+            else if (iflag == 2) s = f.sub ? s - aun : s + aun;
+            else s = f.sub ? s - amin(0., aun) : s + amax(0., aun);
+        });
     if (M.iper != 2) {
         for_boundary(M, c, k, [&](const BEntry &be) {
-            double aun = U.u[0][n] * be.sbb[0] + U.u[1][n] * be.sbb[1] + U.u[2][n] * be.sbb[2];
-            aun = aun / rh0[n];
+            double aun = un0 * be.sbb[0] + un1 * be.sbb[1] + un2 * be.sbb[2];
+            aun = aun / rn;
             if (iflag == 1) s = s + fabs(aun);
             else if (iflag == 2) s = s + aun;
             else s = s + amax(0., aun);
         });
     }
-    cour[n] = s * dt / vol[n] / rh0[n];
+    cour[n] = s * dt / vol[n] / rn;
 }
 
 }  // namespace mpgk

@@ -84,7 +84,8 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out);
 struct HostStatic {
     std::vector<double> rh0, th0, the, dthedz, alpha, coefw, d1, ue, ve;
     double betaunstr1 = 0.;
-    // line preconditioner, per impfl, in the column-interleaved layout used by the solve kernel
+    // line preconditioner, per impfl, in the column-interleaved layout used by the solve kernel:
+    // sub-diagonal a, inverse pivot 1/m and c' of the Thomas factorisation
     std::vector<double> la[2], lm[2], lcp[2];
 };
 

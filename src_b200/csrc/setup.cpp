@@ -471,7 +471,7 @@ int mpg_host_static(const mpg_params *P, const mpg_mesh_ref *m, const HostColumn
                 double cp = c[n] / mm;
                 int64_t li = line_index(col, k, L);
                 hs->la[q][li] = a[n];
-                hs->lm[q][li] = mm;
+                hs->lm[q][li] = 1. / mm;         // the solve multiplies by the inverse pivot
                 hs->lcp[q][li] = cp;
                 cpprev = cp;
             }
