@@ -191,6 +191,7 @@ def main():
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-variants", action="store_true", help="skip the mixed-precision variant")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -233,6 +234,7 @@ def main():
     s.kernel_timing(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sampler.start()
+    torch.cuda.nvtx.range_push("timed_steps")       # lets a profiler capture just this region
     e0.record(stream)
     iters, diags = [], []
     for _ in range(args.steps):
@@ -240,6 +242,7 @@ def main():
         iters.append((d.niter1, d.niter))
         diags.append(d)
     e1.record(stream)
+    torch.cuda.nvtx.range_pop()
     e1.synchronize()
     clocks = sampler.stop()
     torch.cuda.synchronize()
@@ -320,6 +323,50 @@ def main():
                "path": "mpg_set_field x%d from pinned host arrays, %d x mpg_step (per-step diagnostics "
                        "read back), mpg_get_field x%d" % (len(fids), args.steps, len(fids))}
 
+    s.close()
+
+    # ---------------- variants on the same workload (reported beside the headline FP64 path)
+    variants = {}
+    if not args.no_variants:
+        for vname, prec in (("mixed", 1),):
+            Pv = build_params(name, precision=prec)
+            sv = Solver(Pv, rm, device=local)
+            sv.setup()
+            if Pv.nscal:
+                sv.set(F_UNK + 4, gaussian_scalar(rm))
+            for _ in range(args.warmup):
+                sv.step()
+            sv.synchronize()
+            stream_v = torch.cuda.ExternalStream(sv.stream())
+            barrier()
+            torch.cuda.synchronize()
+            sv.kernel_timing(True)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream_v)
+            vit = []
+            for _ in range(args.steps):
+                dv = sv.step()
+                vit.append((dv.niter1, dv.niter))
+            a1.record(stream_v)
+            a1.synchronize()
+            barrier()
+            vms = a0.elapsed_time(a1)
+            if world > 1:
+                t = torch.tensor([vms], device="cuda")
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                vms = float(t.item())
+            vkt = sv.kernel_times()
+            vsolve = vkt.get("pressure_solve", (1, 0.0))
+            variants[vname] = {
+                "value": world * args.steps / (vms / 1000.0), "unit": "steps/s",
+                "ms_per_step": vms / args.steps,
+                "ms_per_pressure_solve": round(vsolve[1] / max(vsolve[0], 1), 3),
+                "gcr_iters_per_solve": round(float(np.mean([a for p in vit for a in p])), 2),
+                "speedup_vs_fp64": round((world * args.steps / (vms / 1000.0)) / value, 3),
+                "precision": "FP32 face vectors, MPDATA fluxes, GCR directions and operator; "
+                             "FP64 p, r, inner products, coefficients, stopping test, Thomas solves, mass sums"}
+            sv.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, n_sample = cpu_sample(3, 1)
@@ -337,13 +384,12 @@ def main():
                 "ms_per_pressure_solve": round(ms_solve, 3),
                 "gcr_iters_per_solve": round(float(np.mean([a for p in iters for a in p])), 2),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks, "kernels": kernels,
+                "clocks": clocks, "kernels": kernels, "variants": variants,
                 "diag_last_step": {"divmx": last.divmx, "crnmx": last.crnmx,
                                    "scalar_min": last.smin[0] if P.nscal else None,
                                    "mass_scalar": last.mass[4] if P.nscal else None},
                 "setup_gcr_iters": d0.niter}
         print(json.dumps(line), flush=True)
-    s.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

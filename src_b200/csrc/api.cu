@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -59,6 +60,9 @@ struct mpg_solver {
     // GCR workspace
     double *r = nullptr, *qr = nullptr, *ar = nullptr, *x[MPG_MAX_LORD] = {}, *ax[MPG_MAX_LORD] = {};
     double *F[3] = {}, *tres = nullptr;
+    // mixed precision: FP32 directions, operator intermediates and node metrics
+    float *xf[MPG_MAX_LORD] = {}, *axf[MPG_MAX_LORD] = {}, *qrf = nullptr, *arf = nullptr, *Ff[3] = {};
+    float *volf = nullptr, *rh0f = nullptr, *coefwf = nullptr;
     double *scal = nullptr, *part = nullptr, *result = nullptr, *h_res = nullptr;
     unsigned int *counter = nullptr;
     // line preconditioner
@@ -67,6 +71,8 @@ struct mpg_solver {
     // MPDATA scratch
     MpScratch S{};
     double *psi1 = nullptr, *g3[3] = {}, *mx = nullptr, *mn = nullptr;
+    MpScratchT<float> Sf{};
+    float *psi1f = nullptr, *g3f[3] = {}, *mxf = nullptr, *mnf = nullptr;
     // /itero/
     int32_t niter = 0, nitsm = 0, icount = 0, gstatus = 0;
     double eer = 0., eem = 0., dvmx_last = 0., rl2_last = 0.;
@@ -196,18 +202,45 @@ int fetch_result(mpg_handle h, int nq) {
 }
 
 // ------------------------------------------------------------------------------ operators
-int op_laplc(mpg_handle h, const double *p, double *alap, int impfl) {
+// buffers of the GCR directions and of laplc in the storage type T
+template <class T> struct Buf;
+template <> struct Buf<double> {
+    static double *x(mpg_handle h, int q) { return h->x[q]; }
+    static double *ax(mpg_handle h, int q) { return h->ax[q]; }
+    static double *qr(mpg_handle h) { return h->qr; }
+    static double *ar(mpg_handle h) { return h->ar; }
+    static double *F(mpg_handle h, int d) { return h->F[d]; }
+    static const double *vol(mpg_handle h) { return h->vol; }
+    static const double *rh0(mpg_handle h) { return h->f[MPG_F_RH0]; }
+    static const double *coefw(mpg_handle h) { return h->f[MPG_F_COEFW]; }
+};
+template <> struct Buf<float> {
+    static float *x(mpg_handle h, int q) { return h->xf[q]; }
+    static float *ax(mpg_handle h, int q) { return h->axf[q]; }
+    static float *qr(mpg_handle h) { return h->qrf; }
+    static float *ar(mpg_handle h) { return h->arf; }
+    static float *F(mpg_handle h, int d) { return h->Ff[d]; }
+    static const float *vol(mpg_handle h) { return h->volf; }
+    static const float *rh0(mpg_handle h) { return h->rh0f; }
+    static const float *coefw(mpg_handle h) { return h->coefwf; }
+};
+
+template <class T>
+int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
+    using B = Buf<T>;
     {
         KTIME(KT_LAP_GRAD);
-        k_lap_grad<<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW], h->ue,
-                                                       h->P.delt, impfl, h->F[0], h->F[1], h->F[2]);
+        k_lap_grad<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
+                                                          (T)h->P.delt, impfl, B::F(h, 0), B::F(h, 1), B::F(h, 2));
     }
     {
         KTIME(KT_LAP_DIV);
-        k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, h->F[0], h->F[1], h->F[2], h->vol, h->f[MPG_F_RH0], alap);
+        k_lap_div<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, B::F(h, 0), B::F(h, 1), B::F(h, 2), B::vol(h),
+                                                         B::rh0(h), alap);
     }
     return check_launch("laplc");
 }
+int op_laplc(mpg_handle h, const double *p, double *alap, int impfl) { return op_laplc_t<double>(h, p, alap, impfl); }
 
 int op_prfr(mpg_handle h, const double *p, const double *us, const double *vs, const double *ws, double *uo,
             double *vo, double *wo, int impfl) {
@@ -227,13 +260,14 @@ int op_div(mpg_handle h, const double *ua, const double *va, const double *wa, d
     return check_launch("div");
 }
 
-int op_line(mpg_handle h, const double *rhs, double *p, int impfl, int acc) {
+template <class TO>
+int op_line(mpg_handle h, const double *rhs, TO *p, int impfl, int acc) {
     const int q = impfl ? 1 : 0;
     const int nblk = (h->NC + 32 * kLineWarps - 1) / (32 * kLineWarps);
     {
         KTIME(KT_LINE);
-        k_line_solve<<<nblk, 32 * kLineWarps, 0, h->st>>>(h->NC, h->L, rhs, h->la[q], h->lm[q], h->lcp[q],
-                                                          h->P.omega, acc, h->dbuf, p);
+        k_line_solve<TO><<<nblk, 32 * kLineWarps, 0, h->st>>>(h->NC, h->L, rhs, h->la[q], h->lm[q], h->lcp[q],
+                                                              h->P.omega, acc, h->dbuf, p);
     }
     return check_launch("line_solve");
 }
@@ -245,7 +279,7 @@ int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, i
     if (iprc == 0) {
         {
             KTIME(KT_MISC);
-            k_copy<<<grid(N), kThreads, 0, h->st>>>(N, rhs, p);
+            k_copy<double, double><<<grid(N), kThreads, 0, h->st>>>(N, rhs, p);
         }
         return check_launch("precon copy");
     }
@@ -256,7 +290,7 @@ int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, i
     if (iprc == 2) {
         for (int it = 1; it <= h->P.itrp1; ++it) {
             if (it == 1) {
-                int rc = op_line(h, rhs, p, impfl, 0);
+                int rc = op_line<double>(h, rhs, p, impfl, 0);
                 if (rc) return rc;
             } else {
                 int rc = op_laplc(h, p, r, impfl);
@@ -265,7 +299,7 @@ int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, i
                     KTIME(KT_MISC);
                     k_sub<<<grid(N), kThreads, 0, h->st>>>(N, rhs, r, h->tres);
                 }
-                rc = op_line(h, h->tres, p, impfl, 1);
+                rc = op_line<double>(h, h->tres, p, impfl, 1);
                 if (rc) return rc;
             }
         }
@@ -299,6 +333,41 @@ int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, i
     return check_launch("precon smoother");
 }
 
+// the preconditioner inside gcrk, writing its result in the direction type T
+template <class T>
+int op_precon_gcr(mpg_handle h, const double *r, int impfl) {
+    const int N = h->N;
+    T *qr = Buf<T>::qr(h);
+    if constexpr (std::is_same<T, double>::value) return op_precon(h, r, qr, h->ar, h->P.iprc, impfl, false);
+    else {
+    if (h->P.iprc == 2) {
+        for (int it = 1; it <= h->P.itrp1; ++it) {
+            int rc;
+            if (it == 1) {
+                if ((rc = op_line<T>(h, r, qr, impfl, 0))) return rc;
+            } else {
+                T *tmp = Buf<T>::ar(h);                   // free until laplc(qr) overwrites it
+                if ((rc = op_laplc_t<T>(h, qr, tmp, impfl))) return rc;
+                {
+                    KTIME(KT_MISC);
+                    k_sub_mixed<T><<<grid(N), kThreads, 0, h->st>>>(N, r, tmp, h->tres);
+                }
+                if ((rc = op_line<T>(h, h->tres, qr, impfl, 1))) return rc;
+            }
+        }
+        return check_launch("precon line (mixed)");
+    }
+    // iprc 0 or 1: the FP64 operator, then rounded to T
+    int rc = op_precon(h, r, h->tres, h->ar, h->P.iprc, impfl, false);
+    if (rc) return rc;
+    {
+        KTIME(KT_MISC);
+        k_copy<double, T><<<grid(N), kThreads, 0, h->st>>>(N, h->tres, qr);
+    }
+    return check_launch("precon convert");
+    }
+}
+
 // ------------------------------------------------------------------------------ GCR
 struct FinEps {   // eer0, eem0, rl20 clamped by epa
     double *scal;
@@ -325,159 +394,188 @@ struct FinDel {
         for (int ii = 0; ii < i; ++ii) scal[S_DEL + ii] = -v[ii] / scal[S_AX2 + ii];
     }
 };
+template <class T>
 struct ProdNorm0 {
-    const double *qr, *r;
+    const T *qr;
+    const double *r;
     __device__ void operator()(int n, double *v) const {
-        const double q = qr[n], s = r[n];
+        const double q = (double)qr[n], s = r[n];
         v[0] = q * q;
         v[1] = fabs(q);
         v[2] = s * s;
     }
 };
+template <class T>
 struct ProdDot2 {
-    const double *r, *a;
+    const double *r;
+    const T *a;
     __device__ void operator()(int n, double *v) const {
-        const double x = a[n];
+        const double x = (double)a[n];
         v[0] = r[n] * x;
         v[1] = x * x;
     }
 };
+template <class T>
 struct ProdAxpy {   // p += beta x, r += beta ax; returns |r|, r^2
-    const double *scal, *x, *a;
+    const double *scal;
+    const T *x, *a;
     double *p, *r;
     __device__ void operator()(int n, double *v) const {
         const double beta = scal[S_BETA];
-        p[n] = p[n] + beta * x[n];
-        const double rn = r[n] + beta * a[n];
+        p[n] = p[n] + beta * (double)x[n];
+        const double rn = r[n] + beta * (double)a[n];
         r[n] = rn;
         v[0] = fabs(rn);
         v[1] = rn * rn;
     }
 };
-template <int NQ>
+template <int NQ, class T>
 struct ProdDots {
-    const double *ar;
-    VecList ax;
+    const T *ar;
+    const T *ax[MPG_MAX_LORD];
     int i;
     __device__ void operator()(int n, double *v) const {
-        const double a = ar[n];
+        const double a = (double)ar[n];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) v[q] = q < i ? ax.v[q][n] * a : 0.0;
+        for (int q = 0; q < NQ; ++q) v[q] = q < i ? (double)ax[q][n] * a : 0.0;
     }
 };
+template <class T>
 struct ProdQ {
-    const double *qr;
+    const T *qr;
     __device__ void operator()(int n, double *v) const {
-        v[0] = qr[n] * qr[n];
-        v[1] = fabs(qr[n]);
+        const double q = (double)qr[n];
+        v[0] = q * q;
+        v[1] = fabs(q);
     }
 };
 
+template <class T>
 int gcr_dots(mpg_handle h, int i) {
-    VecList ax{};
-    for (int q = 0; q < h->P.lord; ++q) ax.v[q] = h->ax[q];
     FinDel fin{h->scal, i};
-    if (i <= 4) return reduce<4>(h, 0u, ProdDots<4>{h->ar, ax, i}, fin);
-    if (i <= 8) return reduce<8>(h, 0u, ProdDots<8>{h->ar, ax, i}, fin);
-    return reduce<16>(h, 0u, ProdDots<16>{h->ar, ax, i}, fin);
+    if (i <= 4) {
+        ProdDots<4, T> pd{Buf<T>::ar(h), {}, i};
+        for (int q = 0; q < h->P.lord; ++q) pd.ax[q] = Buf<T>::ax(h, q);
+        return reduce<4>(h, 0u, pd, fin);
+    }
+    if (i <= 8) {
+        ProdDots<8, T> pd{Buf<T>::ar(h), {}, i};
+        for (int q = 0; q < h->P.lord; ++q) pd.ax[q] = Buf<T>::ax(h, q);
+        return reduce<8>(h, 0u, pd, fin);
+    }
+    ProdDots<16, T> pd{Buf<T>::ar(h), {}, i};
+    for (int q = 0; q < h->P.lord; ++q) pd.ax[q] = Buf<T>::ax(h, q);
+    return reduce<16>(h, 0u, pd, fin);
 }
 
 // x(:,i+1) = qr + sum del(ii) x(:,ii), ax likewise (ref.f:1914-1923), or the restart collapse
 // into x(:,1) (ref.f:1924-1937), with the next iteration's r.ax and ax.ax (ref.f:1881-1884)
 // reduced in the same pass.  I = number of previous directions, known at compile time.
-template <int I, bool RESTART>
+template <class T>
+struct VecListT {
+    T *v[MPG_MAX_LORD];
+};
+
+template <int I, bool RESTART, class T>
 struct ProdUpdate {
-    const double *scal, *qr, *ar, *r;
-    VecList x, ax;
-    double *xo, *axo;
+    const double *scal;
+    const T *qr, *ar;
+    const double *r;
+    VecListT<T> x, ax;
+    T *xo, *axo;
     __device__ void operator()(int n, double *v) const {
         double a, b;
         if (RESTART) {
-            a = qr[n] + scal[S_DEL] * x.v[0][n];
-            b = ar[n] + scal[S_DEL] * ax.v[0][n];
+            a = (double)qr[n] + scal[S_DEL] * (double)x.v[0][n];
+            b = (double)ar[n] + scal[S_DEL] * (double)ax.v[0][n];
 #pragma unroll
             for (int ii = 1; ii < I; ++ii) {
                 const double d = scal[S_DEL + ii];
-                a = a + d * x.v[ii][n];
-                b = b + d * ax.v[ii][n];
+                a = a + d * (double)x.v[ii][n];
+                b = b + d * (double)ax.v[ii][n];
             }
         } else {
-            a = qr[n];
-            b = ar[n];
+            a = (double)qr[n];
+            b = (double)ar[n];
 #pragma unroll
             for (int ii = 0; ii < I; ++ii) {
                 const double d = scal[S_DEL + ii];
-                a = a + d * x.v[ii][n];
-                b = b + d * ax.v[ii][n];
+                a = a + d * (double)x.v[ii][n];
+                b = b + d * (double)ax.v[ii][n];
             }
         }
-        xo[n] = a;
-        axo[n] = b;
-        v[0] = r[n] * b;
-        v[1] = b * b;
+        const T at = (T)a, bt = (T)b;
+        xo[n] = at;
+        axo[n] = bt;
+        const double bs = (double)bt;        // the stored direction, as the next iteration reads it
+        v[0] = r[n] * bs;
+        v[1] = bs * bs;
     }
 };
 
-template <int I>
+template <int I, class T>
 int gcr_update_n(mpg_handle h, int lord) {
-    VecList x{}, ax{};
-    for (int q = 0; q < lord; ++q) { x.v[q] = h->x[q]; ax.v[q] = h->ax[q]; }
+    VecListT<T> x{}, ax{};
+    for (int q = 0; q < lord; ++q) { x.v[q] = Buf<T>::x(h, q); ax.v[q] = Buf<T>::ax(h, q); }
     if (I < lord) {
-        ProdUpdate<I, false> pu{h->scal, h->qr, h->ar, h->r, x, ax, h->x[I], h->ax[I]};
+        ProdUpdate<I, false, T> pu{h->scal, Buf<T>::qr(h), Buf<T>::ar(h), h->r, x, ax, Buf<T>::x(h, I), Buf<T>::ax(h, I)};
         return reduce<2>(h, 0u, pu, FinBeta{h->scal, I});
     }
-    ProdUpdate<I, true> pu{h->scal, h->qr, h->ar, h->r, x, ax, h->x[0], h->ax[0]};
+    ProdUpdate<I, true, T> pu{h->scal, Buf<T>::qr(h), Buf<T>::ar(h), h->r, x, ax, Buf<T>::x(h, 0), Buf<T>::ax(h, 0)};
     return reduce<2>(h, 0u, pu, FinBeta{h->scal, 0});
 }
 
+template <class T>
 int gcr_update(mpg_handle h, int i, int lord) {
     switch (i) {
-        case 1: return gcr_update_n<1>(h, lord);
-        case 2: return gcr_update_n<2>(h, lord);
-        case 3: return gcr_update_n<3>(h, lord);
-        case 4: return gcr_update_n<4>(h, lord);
-        case 5: return gcr_update_n<5>(h, lord);
-        case 6: return gcr_update_n<6>(h, lord);
-        case 7: return gcr_update_n<7>(h, lord);
-        case 8: return gcr_update_n<8>(h, lord);
-        case 9: return gcr_update_n<9>(h, lord);
-        case 10: return gcr_update_n<10>(h, lord);
-        case 11: return gcr_update_n<11>(h, lord);
-        case 12: return gcr_update_n<12>(h, lord);
-        case 13: return gcr_update_n<13>(h, lord);
-        case 14: return gcr_update_n<14>(h, lord);
-        case 15: return gcr_update_n<15>(h, lord);
-        default: return gcr_update_n<16>(h, lord);
+        case 1: return gcr_update_n<1, T>(h, lord);
+        case 2: return gcr_update_n<2, T>(h, lord);
+        case 3: return gcr_update_n<3, T>(h, lord);
+        case 4: return gcr_update_n<4, T>(h, lord);
+        case 5: return gcr_update_n<5, T>(h, lord);
+        case 6: return gcr_update_n<6, T>(h, lord);
+        case 7: return gcr_update_n<7, T>(h, lord);
+        case 8: return gcr_update_n<8, T>(h, lord);
+        case 9: return gcr_update_n<9, T>(h, lord);
+        case 10: return gcr_update_n<10, T>(h, lord);
+        case 11: return gcr_update_n<11, T>(h, lord);
+        case 12: return gcr_update_n<12, T>(h, lord);
+        case 13: return gcr_update_n<13, T>(h, lord);
+        case 14: return gcr_update_n<14, T>(h, lord);
+        case 15: return gcr_update_n<15, T>(h, lord);
+        default: return gcr_update_n<16, T>(h, lord);
     }
 }
 
-// gcrk(p, u1, v1, w1, u2, v2, w2, impfl) — ref.f:1776-1972
-int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const double *w1, double *u2,
-            double *v2, double *w2, int impfl) {
+// gcrk(p, u1, v1, w1, u2, v2, w2, impfl) — ref.f:1776-1972.  T is the storage type of the
+// directions x, ax and of qr, ar (double; float in mixed precision); p, r, every inner product,
+// the coefficients and the stopping test are FP64 in both.
+template <class T>
+int op_gcrk_t(mpg_handle h, double *p, const double *u1, const double *v1, const double *w1, double *u2,
+              double *v2, double *w2, int impfl) {
+    using B = Buf<T>;
     const mpg_params &P = h->P;
     const int N = h->N, lord = P.lord, itmn = P.itmn > 0 ? P.itmn : 3;
     const double eps = P.eps0 / P.delt, epa = 1.e-38;
     int nlc = 0, rc;
     if ((rc = op_prfr(h, p, u1, v1, w1, u2, v2, w2, impfl))) return rc;
     if ((rc = op_div(h, u2, v2, w2, h->r, -1))) return rc;
-    if ((rc = op_precon(h, h->r, h->qr, h->ar, P.iprc, impfl, false))) return rc;
-    if ((rc = reduce<3>(h, 0x2u, ProdNorm0{h->qr, h->r}, FinEps{h->scal}))) return rc;
+    if ((rc = op_precon_gcr<T>(h, h->r, impfl))) return rc;
+    if ((rc = reduce<3>(h, 0x2u, ProdNorm0<T>{B::qr(h), h->r}, FinEps{h->scal}))) return rc;
     if ((rc = fetch_result(h, 3))) return rc;
     double rl20 = h->h_res[2] > epa ? h->h_res[2] : epa;
     {
         KTIME(KT_MISC);
-        k_copy<<<grid(N), kThreads, 0, h->st>>>(N, h->qr, h->x[0]);
+        k_copy<T, T><<<grid(N), kThreads, 0, h->st>>>(N, B::qr(h), B::x(h, 0));
     }
-    if ((rc = op_laplc(h, h->x[0], h->ax[0], impfl))) return rc;
+    if ((rc = op_laplc_t<T>(h, B::x(h, 0), B::ax(h, 0), impfl))) return rc;
     int status = MPG_GCR_MAXIT;
     double dvmx = 0., rl2 = 0.;
-    VecList xl{}, axl{};
-    for (int q = 0; q < lord; ++q) { xl.v[q] = h->x[q]; axl.v[q] = h->ax[q]; }
     for (int it = 1; it <= P.itr && status == MPG_GCR_MAXIT; ++it) {
         for (int i = 1; i <= lord; ++i) {
             if (it == 1 && i == 1)      // later iterations get (r.ax, ax.ax) from gcr_update
-                if ((rc = reduce<2>(h, 0u, ProdDot2{h->r, h->ax[0]}, FinBeta{h->scal, 0}))) return rc;
-            if ((rc = reduce<2>(h, 0x1u, ProdAxpy{h->scal, h->x[i - 1], h->ax[i - 1], p, h->r}, NoFin{})))
+                if ((rc = reduce<2>(h, 0u, ProdDot2<T>{h->r, B::ax(h, 0)}, FinBeta{h->scal, 0}))) return rc;
+            if ((rc = reduce<2>(h, 0x1u, ProdAxpy<T>{h->scal, B::x(h, i - 1), B::ax(h, i - 1), p, h->r}, NoFin{})))
                 return rc;
             if ((rc = fetch_result(h, 2))) return rc;
             dvmx = h->h_res[0] > -1.e15 ? h->h_res[0] : -1.e15;
@@ -486,16 +584,15 @@ int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const d
             if (dvmx <= eps && it >= itmn) { status = MPG_GCR_CONVERGED; break; }
             if (rl2 >= rl20) { status = MPG_GCR_STALLED; break; }
             rl20 = rl2 > epa ? rl2 : epa;
-            if ((rc = op_precon(h, h->r, h->qr, h->ar, P.iprc, impfl, false))) return rc;
-            if ((rc = op_laplc(h, h->qr, h->ar, impfl))) return rc;
+            if ((rc = op_precon_gcr<T>(h, h->r, impfl))) return rc;
+            if ((rc = op_laplc_t<T>(h, B::qr(h), B::ar(h), impfl))) return rc;
             nlc = nlc + 1;
-            if ((rc = gcr_dots(h, i))) return rc;
+            if ((rc = gcr_dots<T>(h, i))) return rc;
             // direction update fused with the next iteration's (r.ax, ax.ax) reduction
-            if ((rc = gcr_update(h, i, lord))) return rc;
-            if ((rc = check_launch("gcr update"))) return rc;
+            if ((rc = gcr_update<T>(h, i, lord))) return rc;
         }
     }
-    if ((rc = reduce<2>(h, 0x2u, ProdQ{h->qr}, NoFin{}))) return rc;
+    if ((rc = reduce<2>(h, 0x2u, ProdQ<T>{B::qr(h)}, NoFin{}))) return rc;
     if ((rc = fetch_result(h, 2))) return rc;
     double eer = h->h_res[0], eem = h->h_res[1] > -1.e15 ? h->h_res[1] : -1.e15;
     double s0[3];
@@ -512,46 +609,84 @@ int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const d
     return MPG_OK;
 }
 
+int op_gcrk(mpg_handle h, double *p, const double *u1, const double *v1, const double *w1, double *u2,
+            double *v2, double *w2, int impfl) {
+    if (h->P.precision == MPG_PREC_MIXED) return op_gcrk_t<float>(h, p, u1, v1, w1, u2, v2, w2, impfl);
+    return op_gcrk_t<double>(h, p, u1, v1, w1, u2, v2, w2, impfl);
+}
+
 // ------------------------------------------------------------------------------ MPDATA
-int op_aun(mpg_handle h) {
+// scratch of MPDATA in the intermediate type T
+template <class T> struct MpBuf;
+template <> struct MpBuf<double> {
+    static MpScratch &S(mpg_handle h) { return h->S; }
+    static double *psi1(mpg_handle h) { return h->psi1; }
+    static double *g(mpg_handle h, int d) { return h->g3[d]; }
+    static double *mx(mpg_handle h) { return h->mx; }
+    static double *mn(mpg_handle h) { return h->mn; }
+};
+template <> struct MpBuf<float> {
+    static MpScratchT<float> &S(mpg_handle h) { return h->Sf; }
+    static float *psi1(mpg_handle h) { return h->psi1f; }
+    static float *g(mpg_handle h, int d) { return h->g3f[d]; }
+    static float *mx(mpg_handle h) { return h->mxf; }
+    static float *mn(mpg_handle h) { return h->mnf; }
+};
+
+template <class T>
+int op_aun_t(mpg_handle h) {
     U3 U{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}};
     const int nt = h->NE2 * h->L + h->N;
     {
         KTIME(KT_AUN);
-        k_aun<<<grid(nt), kThreads, 0, h->st>>>(h->M, h->S, U);
+        k_aun<T><<<grid(nt), kThreads, 0, h->st>>>(h->M, MpBuf<T>::S(h), U);
     }
     return check_launch("aun");
 }
+int op_aun(mpg_handle h) {
+    return h->P.precision == MPG_PREC_MIXED ? op_aun_t<float>(h) : op_aun_t<double>(h);
+}
 
-int op_mpdata_field(mpg_handle h, double *psi) {
-    const double dt = h->P.delt;
-    const double *vol = h->vol, *rh0 = h->f[MPG_F_RH0];
+// one mpdatamper call; T is the type of the face fluxes and the intermediate node fields
+template <class T>
+int op_mpdata_field_t(mpg_handle h, double *psi) {
+    using B = MpBuf<T>;
+    using G = Buf<T>;
+    const T dt = (T)h->P.delt;
+    const T *vol = G::vol(h), *rh0 = G::rh0(h);
     const int N = h->N;
+    auto &S = B::S(h);
     {
         KTIME(KT_MP_DONOR);
-        k_mp_donor<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, psi, vol, rh0, dt, h->psi1);
+        k_mp_donor<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h));
     }
     {
         KTIME(KT_MP_GRADB);
-        k_mp_grad_bounds<<<grid(N), kThreads, 0, h->st>>>(h->M, h->psi1, h->g3[0], h->g3[1], h->g3[2], h->mx, h->mn);
+        k_mp_grad_bounds<T><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), B::g(h, 0), B::g(h, 1), B::g(h, 2),
+                                                             B::mx(h), B::mn(h));
     }
-    AntiArgs A{h->psi1, h->g3[0], h->g3[1], h->g3[2], vol, rh0,
-               U3{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}}, dt};
+    AntiArgs<T> A{B::psi1(h), B::g(h, 0), B::g(h, 1), B::g(h, 2), vol, rh0,
+                  U3{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}}, dt};
     const int nt = h->NE2 * h->L + h->N;
     {
         KTIME(KT_MP_ANTI);
-        k_mp_anti<<<grid(nt), kThreads, 0, h->st>>>(h->M, h->S, A);
+        k_mp_anti<T><<<grid(nt), kThreads, 0, h->st>>>(h->M, S, A);
     }
     // cp, cn reuse the gradient buffers (dead after the antidiffusive fluxes)
     {
         KTIME(KT_MP_CPCN);
-        k_mp_cpcn<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, h->psi1, h->mx, h->mn, vol, rh0, dt, h->g3[0], h->g3[1]);
+        k_mp_cpcn<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::mx(h), B::mn(h), vol, rh0, dt,
+                                                      B::g(h, 0), B::g(h, 1));
     }
     {
         KTIME(KT_MP_PASS2);
-        k_mp_pass2<<<grid(N), kThreads, 0, h->st>>>(h->M, h->S, h->psi1, h->g3[0], h->g3[1], vol, rh0, dt, psi);
+        k_mp_pass2<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::g(h, 0), B::g(h, 1), vol, rh0, dt,
+                                                       psi);
     }
     return check_launch("mpdata");
+}
+int op_mpdata_field(mpg_handle h, double *psi) {
+    return h->P.precision == MPG_PREC_MIXED ? op_mpdata_field_t<float>(h, psi) : op_mpdata_field_t<double>(h, psi);
 }
 
 Fields make_fields(mpg_handle h) {
@@ -797,21 +932,54 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
         if ((rc = dalloc(h, &h->F[q], N))) return fail(rc);
     for (int q = 0; q < prm->lord; ++q)
         if ((rc = dalloc(h, &h->x[q], N)) || (rc = dalloc(h, &h->ax[q], N))) return fail(rc);
+    if (prm->precision == MPG_PREC_MIXED) {
+        for (int q = 0; q < prm->lord; ++q)
+            if ((rc = dalloc(h, &h->xf[q], N)) || (rc = dalloc(h, &h->axf[q], N))) return fail(rc);
+        if ((rc = dalloc(h, &h->qrf, N)) || (rc = dalloc(h, &h->arf, N))) return fail(rc);
+        for (int q = 0; q < 3; ++q)
+            if ((rc = dalloc(h, &h->Ff[q], N))) return fail(rc);
+        auto tof = [](const std::vector<double> &v) {
+            std::vector<float> o(v.size());
+            for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
+            return o;
+        };
+        float *vf, *rf, *cf;
+        if ((rc = upload(h, &vf, tof(hm.vol))) || (rc = upload(h, &rf, tof(h->hs.rh0))) ||
+            (rc = upload(h, &cf, tof(h->hs.coefw))))
+            return fail(rc);
+        h->volf = vf; h->rh0f = rf; h->coefwf = cf;
+        for (int d = 0; d < 3; ++d) {
+            float *a, *b;
+            if ((rc = upload(h, &a, tof(hm.Sh[d]))) || (rc = upload(h, &b, tof(hm.Sv[d])))) return fail(rc);
+            M.Shf[d] = a; M.Svf[d] = b;
+        }
+    }
     if ((rc = dalloc(h, &h->scal, S_COUNT)) || (rc = dalloc(h, &h->part, (size_t)kRedBlocks * kMaxQ)) ||
         (rc = dalloc(h, &h->result, kMaxQ)) || (rc = dalloc(h, &h->counter, 1)))
         return fail(rc);
     e = cudaMallocHost((void **)&h->h_res, sizeof(double) * kMaxQ);
     if (e != cudaSuccess) return fail(mpg_fail(MPG_ERR_NOMEM, "cudaMallocHost"));
-    // MPDATA scratch
+    // MPDATA scratch in the precision of the run
     const size_t nh = (size_t)h->NE2 * h->L;
-    double *aunh, *aunv, *Ah, *Av;
-    if ((rc = dalloc(h, &aunh, nh)) || (rc = dalloc(h, &aunv, N)) || (rc = dalloc(h, &Ah, nh)) ||
-        (rc = dalloc(h, &Av, N)) || (rc = dalloc(h, &h->psi1, N)) || (rc = dalloc(h, &h->mx, N)) ||
-        (rc = dalloc(h, &h->mn, N)))
-        return fail(rc);
-    for (int q = 0; q < 3; ++q)
-        if ((rc = dalloc(h, &h->g3[q], N))) return fail(rc);
-    h->S = MpScratch{aunh, aunv, Ah, Av, h->d_e2a, h->d_e2b};
+    if (prm->precision == MPG_PREC_MIXED) {
+        float *aunh, *aunv, *Ah, *Av;
+        if ((rc = dalloc(h, &aunh, nh)) || (rc = dalloc(h, &aunv, N)) || (rc = dalloc(h, &Ah, nh)) ||
+            (rc = dalloc(h, &Av, N)) || (rc = dalloc(h, &h->psi1f, N)) || (rc = dalloc(h, &h->mxf, N)) ||
+            (rc = dalloc(h, &h->mnf, N)))
+            return fail(rc);
+        for (int q = 0; q < 3; ++q)
+            if ((rc = dalloc(h, &h->g3f[q], N))) return fail(rc);
+        h->Sf = MpScratchT<float>{aunh, aunv, Ah, Av, h->d_e2a, h->d_e2b};
+    } else {
+        double *aunh, *aunv, *Ah, *Av;
+        if ((rc = dalloc(h, &aunh, nh)) || (rc = dalloc(h, &aunv, N)) || (rc = dalloc(h, &Ah, nh)) ||
+            (rc = dalloc(h, &Av, N)) || (rc = dalloc(h, &h->psi1, N)) || (rc = dalloc(h, &h->mx, N)) ||
+            (rc = dalloc(h, &h->mn, N)))
+            return fail(rc);
+        for (int q = 0; q < 3; ++q)
+            if ((rc = dalloc(h, &h->g3[q], N))) return fail(rc);
+        h->S = MpScratch{aunh, aunv, Ah, Av, h->d_e2a, h->d_e2b};
+    }
     if ((rc = upload(h, &h->d_iperm, hm.iperm))) return fail(rc);
     if ((rc = dalloc(h, &h->dbuf, h->hs.la[0].size()))) return fail(rc);
     e = cudaStreamSynchronize(h->st);

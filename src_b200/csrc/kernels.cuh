@@ -77,6 +77,14 @@ __device__ __forceinline__ void for_faces(const ColMesh &M, int c, int k, int n,
 __device__ __forceinline__ const double *spick(const ColMesh &M, int d, bool vert) {
     return vert ? M.Sv[d] : M.Sh[d];
 }
+// face vectors in the storage type of a kernel instantiation (FP32 copies in mixed precision)
+template <class T> struct SPick;
+template <> struct SPick<double> {
+    __device__ static const double *get(const ColMesh &M, int d, bool vert) { return vert ? M.Sv[d] : M.Sh[d]; }
+};
+template <> struct SPick<float> {
+    __device__ static const float *get(const ColMesh &M, int d, bool vert) { return vert ? M.Svf[d] : M.Shf[d]; }
+};
 
 // Boundary entries of node (c,k), in reference order.
 template <class V>
@@ -88,82 +96,86 @@ __device__ __forceinline__ void for_boundary(const ColMesh &M, int c, int k, V &
     }
 }
 
-struct V4 { double a, b, c, d; };
-struct V6 { double a, b, c, d, e, f; };
+template <class T> struct V4T { T a, b, c, d; };
+template <class T> struct V6T { T a, b, c, d, e, f; };
+using V4 = V4T<double>;
+using V6 = V6T<double>;
 
 // derivative (ref.f:3943-4022) of phi for the three components at once:
 // g_d = sum over faces of (+/-) S_d * ((phi_n + phi_j) * 0.5)
-__device__ __forceinline__ void grad3(const ColMesh &M, const double *__restrict__ phi, int c, int k,
-                                      int n, double &gx, double &gy, double &gz) {
-    const double pn = phi[n];
-    double ax = 0., ay = 0., az = 0.;
+template <class T>
+__device__ __forceinline__ void grad3(const ColMesh &M, const T *__restrict__ phi, int c, int k, int n,
+                                      T &gx, T &gy, T &gz) {
+    const T pn = phi[n];
+    T ax = 0., ay = 0., az = 0.;
     for_faces(M, c, k, n,
         [&](const Face &f) {
-            return V4{__ldg(spick(M, 0, f.vert) + f.si), __ldg(spick(M, 1, f.vert) + f.si),
-                      __ldg(spick(M, 2, f.vert) + f.si), phi[f.j]};
+            return V4T<T>{__ldg(SPick<T>::get(M, 0, f.vert) + f.si), __ldg(SPick<T>::get(M, 1, f.vert) + f.si),
+                          __ldg(SPick<T>::get(M, 2, f.vert) + f.si), phi[f.j]};
         },
-        [&](const Face &f, const V4 &v) {
-            const double u = (pn + v.d) * 0.5;
-            const double tx = v.a * u, ty = v.b * u, tz = v.c * u;
+        [&](const Face &f, const V4T<T> &v) {
+            const T u = (pn + v.d) * T(0.5);
+            const T tx = v.a * u, ty = v.b * u, tz = v.c * u;
             if (f.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
             else       { ax = ax + tx; ay = ay + ty; az = az + tz; }
         });
     if (M.iper == 0) {                                  // closure, ref.f:4007-4014
         for_boundary(M, c, k, [&](const BEntry &be) {
-            ax = ax + be.sbb[0] * pn;
-            ay = ay + be.sbb[1] * pn;
-            az = az + be.sbb[2] * pn;
+            ax = ax + T(be.sbb[0]) * pn;
+            ay = ay + T(be.sbb[1]) * pn;
+            az = az + T(be.sbb[2]) * pn;
         });
     }
     gx = ax; gy = ay; gz = az;
 }
 
 // derivative(fx,1), derivative(fy,2), derivative(fz,3) of three fields (the divergence)
-template <class FX>
-__device__ __forceinline__ void div3(const ColMesh &M, FX f, int c, int k, int n,
-                                     double &dx, double &dy, double &dz) {
-    double fnx, fny, fnz;
+template <class T, class FX>
+__device__ __forceinline__ void div3(const ColMesh &M, FX f, int c, int k, int n, T &dx, T &dy, T &dz) {
+    T fnx, fny, fnz;
     f(n, fnx, fny, fnz);
-    double ax = 0., ay = 0., az = 0.;
+    T ax = 0., ay = 0., az = 0.;
     for_faces(M, c, k, n,
         [&](const Face &fc) {
-            V6 v;
-            v.a = __ldg(spick(M, 0, fc.vert) + fc.si);
-            v.b = __ldg(spick(M, 1, fc.vert) + fc.si);
-            v.c = __ldg(spick(M, 2, fc.vert) + fc.si);
+            V6T<T> v;
+            v.a = __ldg(SPick<T>::get(M, 0, fc.vert) + fc.si);
+            v.b = __ldg(SPick<T>::get(M, 1, fc.vert) + fc.si);
+            v.c = __ldg(SPick<T>::get(M, 2, fc.vert) + fc.si);
             f(fc.j, v.d, v.e, v.f);
             return v;
         },
-        [&](const Face &fc, const V6 &v) {
-            const double tx = v.a * ((fnx + v.d) * 0.5);
-            const double ty = v.b * ((fny + v.e) * 0.5);
-            const double tz = v.c * ((fnz + v.f) * 0.5);
+        [&](const Face &fc, const V6T<T> &v) {
+            const T tx = v.a * ((fnx + v.d) * T(0.5));
+            const T ty = v.b * ((fny + v.e) * T(0.5));
+            const T tz = v.c * ((fnz + v.f) * T(0.5));
             if (fc.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
             else        { ax = ax + tx; ay = ay + ty; az = az + tz; }
         });
     if (M.iper == 0) {
         for_boundary(M, c, k, [&](const BEntry &be) {
-            ax = ax + be.sbb[0] * fnx;
-            ay = ay + be.sbb[1] * fny;
-            az = az + be.sbb[2] * fnz;
+            ax = ax + T(be.sbb[0]) * fnx;
+            ay = ay + T(be.sbb[1]) * fny;
+            az = az + T(be.sbb[2]) * fnz;
         });
     }
     dx = ax; dy = ay; dz = az;
 }
 
 // bcv (ref.f:1583-1643) applied to one node
+template <class T>
 __device__ __forceinline__ void bcv_node(const ColMesh &M, int c, int k, int n, const double *ue, double flag,
-                                         double &u, double &v, double &w) {
+                                         T &u, T &v, T &w) {
     const bool per = (M.iper == 2);
     for_boundary(M, c, k, [&](const BEntry &be) {
         const int t = be.type;
         if (t == 11 || (!per && (t == 5 || t == 6))) {
-            const double vn = u * be.anp[0] + v * be.anp[1] + w * be.anp[2];
-            u = u - be.anp[0] * vn;
-            v = v - be.anp[1] * vn;
-            w = w - be.anp[2] * vn;
+            const T a0 = T(be.anp[0]), a1 = T(be.anp[1]), a2 = T(be.anp[2]);
+            const T vn = u * a0 + v * a1 + w * a2;
+            u = u - a0 * vn;
+            v = v - a1 * vn;
+            w = w - a2 * vn;
         }
-        if (!per && (t == 7 || t == 8)) u = ue[n] * flag;
+        if (!per && (t == 7 || t == 8)) u = T(ue[n] * flag);
     });
 }
 
@@ -180,7 +192,7 @@ __device__ __forceinline__ void bcv_node(const ColMesh &M, int c, int k, int n, 
 __global__ void GATHER_BOUNDS k_derivative(ColMesh M, const double *__restrict__ phi, double *__restrict__ out, int idx) {
     NODE_BEGIN
     double gx, gy, gz;
-    grad3(M, phi, c, k, n, gx, gy, gz);
+    grad3<double>(M, phi, c, k, n, gx, gy, gz);
     out[n] = idx == 1 ? gx : idx == 2 ? gy : gz;
 }
 
@@ -189,35 +201,38 @@ __global__ void k_bcv(ColMesh M, double *u, double *v, double *w, const double *
     NODE_BEGIN
     if (__ldg(&M.bptr[c]) == __ldg(&M.bptr[c + 1])) return;
     double a = u[n], b = v[n], d = w[n];
-    bcv_node(M, c, k, n, ue, flag, a, b, d);
+    bcv_node<double>(M, c, k, n, ue, flag, a, b, d);
     u[n] = a; v[n] = b; w[n] = d;
 }
 
-// laplc first half (ref.f:1303-1338): gradient, scaling, bcv(.,0.), times rh0
-__global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const double *__restrict__ p, const double *__restrict__ vol,
-                           const double *__restrict__ rh0, const double *__restrict__ coefw,
-                           const double *__restrict__ ue, double dt, int impfl,
-                           double *__restrict__ Fx, double *__restrict__ Fy, double *__restrict__ Fz) {
+// laplc first half (ref.f:1303-1338): gradient, scaling, bcv(.,0.), times rh0.  T is the
+// storage and arithmetic type (double; float for the mixed-precision solve).
+template <class T>
+__global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const T *__restrict__ p, const T *__restrict__ vol,
+                                         const T *__restrict__ rh0, const T *__restrict__ coefw,
+                                         const double *__restrict__ ue, T dt, int impfl,
+                                         T *__restrict__ Fx, T *__restrict__ Fy, T *__restrict__ Fz) {
     NODE_BEGIN
-    double gx, gy, gz;
-    grad3(M, p, c, k, n, gx, gy, gz);
-    const double v = vol[n];
-    double dx = dt * gx / v, dy = dt * gy / v, dz = dt * gz / v;
-    dx = 0.5 * dx / 1.0;                       // (gmm*cosa)**2 == 1 for isfera = 0
-    dy = 0.5 * dy / 1.0;
-    dz = 0.5 * dz * (coefw[n] * (double)impfl + (double)(1 - impfl));
-    bcv_node(M, c, k, n, ue, 0.0, dx, dy, dz);
-    const double r = rh0[n];
+    T gx, gy, gz;
+    grad3<T>(M, p, c, k, n, gx, gy, gz);
+    const T v = vol[n];
+    T dx = dt * gx / v, dy = dt * gy / v, dz = dt * gz / v;
+    dx = T(0.5) * dx / T(1.0);                 // (gmm*cosa)**2 == 1 for isfera = 0
+    dy = T(0.5) * dy / T(1.0);
+    dz = T(0.5) * dz * (coefw[n] * (T)impfl + (T)(1 - impfl));
+    bcv_node<T>(M, c, k, n, ue, 0.0, dx, dy, dz);
+    const T r = rh0[n];
     Fx[n] = dx * r; Fy[n] = dy * r; Fz[n] = dz * r;
 }
 
 // laplc second half (ref.f:1339-1350): alap = (Dx(Fx) + Dy(Fy) + Dz(Fz)) / (vol*rh0)
-__global__ void k_lap_div(ColMesh M, const double *__restrict__ Fx, const double *__restrict__ Fy,
-                          const double *__restrict__ Fz, const double *__restrict__ vol,
-                          const double *__restrict__ rh0, double *__restrict__ alap) {
+template <class T>
+__global__ void k_lap_div(ColMesh M, const T *__restrict__ Fx, const T *__restrict__ Fy,
+                          const T *__restrict__ Fz, const T *__restrict__ vol,
+                          const T *__restrict__ rh0, T *__restrict__ alap) {
     NODE_BEGIN
-    double dx, dy, dz;
-    div3(M, [&](int j, double &a, double &b, double &d) { a = Fx[j]; b = Fy[j]; d = Fz[j]; }, c, k, n, dx, dy, dz);
+    T dx, dy, dz;
+    div3<T>(M, [&](int j, T &a, T &b, T &d) { a = Fx[j]; b = Fy[j]; d = Fz[j]; }, c, k, n, dx, dy, dz);
     alap[n] = (dx + dy + dz) / (vol[n] * rh0[n]);
 }
 
@@ -229,13 +244,13 @@ __global__ void GATHER_BOUNDS k_prfr(ColMesh M, const double *__restrict__ p, co
                        double *__restrict__ uo, double *__restrict__ vo, double *__restrict__ wo) {
     NODE_BEGIN
     double gx, gy, gz;
-    grad3(M, p, c, k, n, gx, gy, gz);
+    grad3<double>(M, p, c, k, n, gx, gy, gz);
     const double v = vol[n];
     const double dpx = gx / 1.0 / v, dpy = gy / 1.0 / v, dpz = gz / v;
     double a = us[n] - 0.5 * dt * dpx;
     double b = vs[n] - 0.5 * dt * dpy;
     double d = ws[n] - 0.5 * dt * dpz * (coefw[n] * (double)impfl + (double)(1 - impfl));
-    bcv_node(M, c, k, n, ue, 1.0, a, b, d);
+    bcv_node<double>(M, c, k, n, ue, 1.0, a, b, d);
     uo[n] = a; vo[n] = b; wo[n] = d;
 }
 
@@ -246,10 +261,10 @@ __global__ void k_div(ColMesh M, const double *__restrict__ ua, const double *__
     NODE_BEGIN
     double dx, dy, dz;
     if (iflg == -1)
-        div3(M, [&](int j, double &a, double &b, double &d) {
+        div3<double>(M, [&](int j, double &a, double &b, double &d) {
             const double r = rh0[j]; a = ua[j] * r; b = va[j] * r; d = wa[j] * r; }, c, k, n, dx, dy, dz);
     else
-        div3(M, [&](int j, double &a, double &b, double &d) { a = ua[j]; b = va[j]; d = wa[j]; }, c, k, n, dx, dy, dz);
+        div3<double>(M, [&](int j, double &a, double &b, double &d) { a = ua[j]; b = va[j]; d = wa[j]; }, c, k, n, dx, dy, dz);
     const double v = vol[n];
     rhs[n] = (double)iflg * (dx / v + dy / v + dz / v) / rh0[n];
 }
@@ -263,10 +278,11 @@ __global__ void k_div(ColMesh M, const double *__restrict__ ua, const double *__
 // With 4 KiB of shared memory per warp the kernel keeps enough warps resident to stream.
 constexpr int kLineWarps = 8;
 constexpr int kLineChunk = 16;
+template <class TO>
 __global__ void __launch_bounds__(32 * kLineWarps)
 k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__restrict__ la,
              const double *__restrict__ linv, const double *__restrict__ lcp, double omega, int acc,
-             double *__restrict__ dbuf, double *__restrict__ p) {
+             double *__restrict__ dbuf, TO *__restrict__ p) {
     __shared__ double tile[kLineWarps][32][kLineChunk + 1];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col0 = (blockIdx.x * kLineWarps + w) * 32;
@@ -311,8 +327,8 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
         for (int i = lane; i < ncols * nk; i += 32) {
             const int cc = i / nk, kk = i - cc * nk;
             const int64_t g = (int64_t)(col0 + cc) * L + k0 + kk;
-            const double prev = acc ? p[g] : 0.0;
-            p[g] = prev + omega * t[cc][kk];
+            const double prev = acc ? (double)p[g] : 0.0;
+            p[g] = (TO)(prev + omega * t[cc][kk]);
         }
         __syncwarp();
     }
@@ -435,9 +451,15 @@ __global__ void k_fill(int N, double *__restrict__ a, double v) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n < N) a[n] = v;
 }
-__global__ void k_copy(int N, const double *__restrict__ a, double *__restrict__ b) {
+template <class TA, class TB>
+__global__ void k_copy(int N, const TA *__restrict__ a, TB *__restrict__ b) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n < N) b[n] = a[n];
+    if (n < N) b[n] = (TB)a[n];
+}
+template <class T>
+__global__ void k_sub_mixed(int N, const double *__restrict__ a, const T *__restrict__ b, double *__restrict__ o) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < N) o[n] = a[n] - (double)b[n];
 }
 __global__ void k_sub(int N, const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ o) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;

@@ -18,15 +18,19 @@
 
 namespace mpgk {
 
-struct MpScratch {
-    double *aunh, *aunv;     // advective flux per face
-    double *Ah, *Av;         // antidiffusive flux per face
+// face arrays of MPDATA in the intermediate type T (double; float in mixed precision)
+template <class T>
+struct MpScratchT {
+    T *aunh, *aunv;          // advective flux per face
+    T *Ah, *Av;              // antidiffusive flux per face
     const int32_t *e2a, *e2b;
 };
+using MpScratch = MpScratchT<double>;
 
-__device__ __forceinline__ double face_aun(const double *const *uuu, int a, int b, double sx, double sy, double sz) {
-    return (uuu[0][a] + uuu[0][b]) * 0.5 * sx + (uuu[1][a] + uuu[1][b]) * 0.5 * sy
-         + (uuu[2][a] + uuu[2][b]) * 0.5 * sz;
+template <class T>
+__device__ __forceinline__ T face_aun(const double *const *uuu, int a, int b, T sx, T sy, T sz) {
+    return ((T)uuu[0][a] + (T)uuu[0][b]) * T(0.5) * sx + ((T)uuu[1][a] + (T)uuu[1][b]) * T(0.5) * sy
+         + ((T)uuu[2][a] + (T)uuu[2][b]) * T(0.5) * sz;
 }
 
 struct U3 {
@@ -34,21 +38,26 @@ struct U3 {
 };
 
 // aun for horizontal faces (thread per (e,k)) and vertical faces (thread per node)
-__global__ void k_aun(ColMesh M, MpScratch S, U3 U) {
+template <class T>
+__global__ void k_aun(ColMesh M, MpScratchT<T> S, U3 U) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int nh = M.NE2 * M.L;
     if (t < nh) {
         const int e = t / M.L, k = t - e * M.L;
         const int a = S.e2a[e] * M.L + k, b = S.e2b[e] * M.L + k;
-        S.aunh[t] = face_aun(U.u, a, b, M.Sh[0][t], M.Sh[1][t], M.Sh[2][t]);
+        S.aunh[t] = face_aun<T>(U.u, a, b, SPick<T>::get(M, 0, false)[t], SPick<T>::get(M, 1, false)[t],
+                                SPick<T>::get(M, 2, false)[t]);
     } else if (t < nh + M.N) {
         const int n = t - nh;
         const int k = n % M.L;
-        if (k + 1 < M.L) S.aunv[n] = face_aun(U.u, n, n + 1, M.Sv[0][n], M.Sv[1][n], M.Sv[2][n]);
+        if (k + 1 < M.L)
+            S.aunv[n] = face_aun<T>(U.u, n, n + 1, SPick<T>::get(M, 0, true)[n], SPick<T>::get(M, 1, true)[n],
+                                    SPick<T>::get(M, 2, true)[n]);
     }
 }
 
-__device__ __forceinline__ double face_val(const double *h, const double *v, int si, bool vert) {
+template <class T>
+__device__ __forceinline__ T face_val(const T *h, const T *v, int si, bool vert) {
     return vert ? v[si] : h[si];
 }
 
@@ -59,124 +68,135 @@ __device__ __forceinline__ bool has_boundary(const ColMesh &M, int c, int k) {
 }
 
 // donor-cell pass: fl = psi_a*max(0,aun) + psi_b*min(0,aun); a gets +fl, b gets -fl
-__global__ void k_mp_donor(ColMesh M, MpScratch S, const double *__restrict__ psi,
-                           const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
-                           double *__restrict__ psi1) {
+template <class T>
+__global__ void k_mp_donor(ColMesh M, MpScratchT<T> S, const double *__restrict__ psi,
+                           const T *__restrict__ vol, const T *__restrict__ rh0, T dt,
+                           T *__restrict__ psi1) {
     NODE_BEGIN
-    const double pn = psi[n];
-    double arh2 = 0.;
+    const T pn = (T)psi[n];
+    T arh2 = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4{(f.vert ? S.aunv : S.aunh)[f.si], psi[f.j], 0., 0.}; },
-        [&](const Face &f, const V4 &v) {
-            const double aun = v.a;
-            const double pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
-            const double fl = pa * amax(0., aun) + pb * amin(0., aun);
+        [&](const Face &f) { return V4T<T>{(f.vert ? S.aunv : S.aunh)[f.si], (T)psi[f.j], T(0), T(0)}; },
+        [&](const Face &f, const V4T<T> &v) {
+            const T aun = v.a;
+            const T pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
+            const T fl = pa * (T(0) > aun ? T(0) : aun) + pb * (T(0) < aun ? T(0) : aun);
             arh2 = f.sub ? arh2 - fl : arh2 + fl;
         });
-    if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;          // zero boundary flux, ref.f:3732-3738
+    if (has_boundary(M, c, k)) arh2 = arh2 + T(0) * T(1);      // zero boundary flux, ref.f:3732-3738
     psi1[n] = pn - arh2 * dt / vol[n] / rh0[n];
 }
 
 // gradient of psi1 (three derivative calls) and the neighbourhood max/min
-__global__ void k_mp_grad_bounds(ColMesh M, const double *__restrict__ psi1, double *__restrict__ gx,
-                                 double *__restrict__ gy, double *__restrict__ gz,
-                                 double *__restrict__ mx, double *__restrict__ mn) {
+template <class T>
+__global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, T *__restrict__ gx,
+                                 T *__restrict__ gy, T *__restrict__ gz,
+                                 T *__restrict__ mx, T *__restrict__ mn) {
     NODE_BEGIN
-    const double pn = psi1[n];
-    double ax = 0., ay = 0., az = 0., hi = -1.e15, lo = 1.e15;
+    const T pn = psi1[n];
+    T ax = 0., ay = 0., az = 0., hi = T(-1.e15), lo = T(1.e15);
     for_faces(M, c, k, n,
         [&](const Face &f) {
-            return V4{__ldg(spick(M, 0, f.vert) + f.si), __ldg(spick(M, 1, f.vert) + f.si),
-                      __ldg(spick(M, 2, f.vert) + f.si), psi1[f.j]};
+            return V4T<T>{__ldg(SPick<T>::get(M, 0, f.vert) + f.si), __ldg(SPick<T>::get(M, 1, f.vert) + f.si),
+                          __ldg(SPick<T>::get(M, 2, f.vert) + f.si), psi1[f.j]};
         },
-        [&](const Face &f, const V4 &v) {
-            const double pj = v.d;
-            const double u = (pn + pj) * 0.5;
-            const double tx = v.a * u, ty = v.b * u, tz = v.c * u;
+        [&](const Face &f, const V4T<T> &v) {
+            const T pj = v.d;
+            const T u = (pn + pj) * T(0.5);
+            const T tx = v.a * u, ty = v.b * u, tz = v.c * u;
             if (f.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
             else       { ax = ax + tx; ay = ay + ty; az = az + tz; }
-            hi = amax(amax(hi, pn), pj);
-            lo = amin(amin(lo, pn), pj);
+            hi = hi > pn ? hi : pn;
+            hi = hi > pj ? hi : pj;
+            lo = lo < pn ? lo : pn;
+            lo = lo < pj ? lo : pj;
         });
     gx[n] = ax; gy[n] = ay; gz[n] = az;
     mx[n] = hi; mn[n] = lo;
 }
 
-__device__ __forceinline__ double anti_flux(double aun, int a, int b, const double *psi1, const double *gx,
-                                            const double *gy, const double *gz, const double *vol,
-                                            const double *rh0, const double *const *uuu, double dt) {
-    const double un = fabs(aun) * (psi1[b] - psi1[a]) * 0.5;
-    const double volt = 0.5 * (vol[a] * rh0[a] + vol[b] * rh0[b]);
-    const double dpdx = 0.5 * (gx[a] + gx[b]) / volt;
-    const double dpdy = 0.5 * (gy[a] + gy[b]) / volt;
-    const double dpdz = 0.5 * (gz[a] + gz[b]) / volt;
-    const double term = (uuu[0][a] + uuu[0][b]) * 0.5 * dpdx + (uuu[1][a] + uuu[1][b]) * 0.5 * dpdy
-                      + (uuu[2][a] + uuu[2][b]) * 0.5 * dpdz;
-    return un - aun * term * dt * 0.5;
+template <class T>
+__device__ __forceinline__ T anti_flux(T aun, int a, int b, const T *psi1, const T *gx, const T *gy,
+                                       const T *gz, const T *vol, const T *rh0, const double *const *uuu, T dt) {
+    const T un = fabs(aun) * (psi1[b] - psi1[a]) * T(0.5);
+    const T volt = T(0.5) * (vol[a] * rh0[a] + vol[b] * rh0[b]);
+    const T dpdx = T(0.5) * (gx[a] + gx[b]) / volt;
+    const T dpdy = T(0.5) * (gy[a] + gy[b]) / volt;
+    const T dpdz = T(0.5) * (gz[a] + gz[b]) / volt;
+    const T term = ((T)uuu[0][a] + (T)uuu[0][b]) * T(0.5) * dpdx + ((T)uuu[1][a] + (T)uuu[1][b]) * T(0.5) * dpdy
+                 + ((T)uuu[2][a] + (T)uuu[2][b]) * T(0.5) * dpdz;
+    return un - aun * term * dt * T(0.5);
 }
 
+template <class T>
 struct AntiArgs {
-    const double *psi1, *gx, *gy, *gz, *vol, *rh0;
+    const T *psi1, *gx, *gy, *gz, *vol, *rh0;
     U3 U;
-    double dt;
+    T dt;
 };
 
-__global__ void k_mp_anti(ColMesh M, MpScratch S, AntiArgs A) {
+template <class T>
+__global__ void k_mp_anti(ColMesh M, MpScratchT<T> S, AntiArgs<T> A) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int nh = M.NE2 * M.L;
     if (t < nh) {
         const int e = t / M.L, k = t - e * M.L;
         const int a = S.e2a[e] * M.L + k, b = S.e2b[e] * M.L + k;
-        S.Ah[t] = anti_flux(S.aunh[t], a, b, A.psi1, A.gx, A.gy, A.gz, A.vol, A.rh0, A.U.u, A.dt);
+        S.Ah[t] = anti_flux<T>(S.aunh[t], a, b, A.psi1, A.gx, A.gy, A.gz, A.vol, A.rh0, A.U.u, A.dt);
     } else if (t < nh + M.N) {
         const int n = t - nh;
         const int k = n % M.L;
         if (k + 1 < M.L)
-            S.Av[n] = anti_flux(S.aunv[n], n, n + 1, A.psi1, A.gx, A.gy, A.gz, A.vol, A.rh0, A.U.u, A.dt);
+            S.Av[n] = anti_flux<T>(S.aunv[n], n, n + 1, A.psi1, A.gx, A.gy, A.gz, A.vol, A.rh0, A.U.u, A.dt);
     }
 }
 
 // in/out sums and the limiter ratios
-__global__ void k_mp_cpcn(ColMesh M, MpScratch S, const double *__restrict__ psi1,
-                          const double *__restrict__ mx, const double *__restrict__ mn,
-                          const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
-                          double *__restrict__ cp, double *__restrict__ cn) {
+template <class T>
+__global__ void k_mp_cpcn(ColMesh M, MpScratchT<T> S, const T *__restrict__ psi1,
+                          const T *__restrict__ mx, const T *__restrict__ mn,
+                          const T *__restrict__ vol, const T *__restrict__ rh0, T dt,
+                          T *__restrict__ cp, T *__restrict__ cn) {
     NODE_BEGIN
-    double rin = 0., rout = 0.;
+    T rin = 0., rout = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4{(f.vert ? S.Av : S.Ah)[f.si], 0., 0., 0.}; },
-        [&](const Face &f, const V4 &v) {
-            const double a = v.a;
-            const double pp = amax(0., a), pn = -amin(0., a);
+        [&](const Face &f) { return V4T<T>{(f.vert ? S.Av : S.Ah)[f.si], T(0), T(0), T(0)}; },
+        [&](const Face &f, const V4T<T> &v) {
+            const T a = v.a;
+            const T pp = T(0) > a ? T(0) : a, pn = -(T(0) < a ? T(0) : a);
             if (!f.sub) { rin = rin + pn; rout = rout + pp; }
             else        { rin = rin + pp; rout = rout + pn; }
         });
-    const double tol = 1.e-10;
-    const double p = psi1[n], v = vol[n], r = rh0[n];
+    const T tol = T(1.e-10);
+    const T p = psi1[n], v = vol[n], r = rh0[n];
     cp[n] = (mx[n] - p) * v * r / (rin * dt + tol);
     cn[n] = (p - mn[n]) * v * r / (rout * dt + tol);
 }
 
 // limited antidiffusive flux and the second pass
-__global__ void k_mp_pass2(ColMesh M, MpScratch S, const double *__restrict__ psi1,
-                           const double *__restrict__ cp, const double *__restrict__ cn,
-                           const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
+template <class T>
+__device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
+
+template <class T>
+__global__ void k_mp_pass2(ColMesh M, MpScratchT<T> S, const T *__restrict__ psi1,
+                           const T *__restrict__ cp, const T *__restrict__ cn,
+                           const T *__restrict__ vol, const T *__restrict__ rh0, T dt,
                            double *__restrict__ psi2) {
     NODE_BEGIN
-    const double cpn = cp[n], cnn = cn[n];
-    double arh2 = 0.;
+    const T cpn = cp[n], cnn = cn[n];
+    T arh2 = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4{(f.vert ? S.Av : S.Ah)[f.si], cp[f.j], cn[f.j], 0.}; },
-        [&](const Face &f, const V4 &v) {
-            const double a = v.a;
+        [&](const Face &f) { return V4T<T>{(f.vert ? S.Av : S.Ah)[f.si], cp[f.j], cn[f.j], T(0)}; },
+        [&](const Face &f, const V4T<T> &v) {
+            const T a = v.a;
             // canonical ends: first = this node unless sub
-            const double cpa = f.sub ? v.b : cpn, cna = f.sub ? v.c : cnn;
-            const double cpb = f.sub ? cpn : v.b, cnb = f.sub ? cnn : v.c;
-            const double lim = a > 0. ? a * amin(amin(1., cpb), cna) : a * amin(amin(1., cnb), cpa);
+            const T cpa = f.sub ? v.b : cpn, cna = f.sub ? v.c : cnn;
+            const T cpb = f.sub ? cpn : v.b, cnb = f.sub ? cnn : v.c;
+            const T lim = a > T(0) ? a * tmin(tmin(T(1), cpb), cna) : a * tmin(tmin(T(1), cnb), cpa);
             arh2 = f.sub ? arh2 - lim : arh2 + lim;
         });
-    if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;
-    psi2[n] = psi1[n] - arh2 * dt / vol[n] / rh0[n];
+    if (has_boundary(M, c, k)) arh2 = arh2 + T(0) * T(1);
+    psi2[n] = (double)(psi1[n] - arh2 * dt / vol[n] / rh0[n]);
 }
 
 // ------------------------------------------------------------------------------ mpsolver node loops
