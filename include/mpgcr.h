@@ -210,6 +210,34 @@ int mpg_get_gcr_stats(mpg_handle h, mpg_gcr_stats *stats);
 /* Wait for all work of the handle. */
 int mpg_synchronize(mpg_handle h);
 
+/* ---------------------------------------------------------------- learned preconditioner */
+/* An edge message-passing network (3 layers, 32 hidden channels, BF16 activations and weights,
+ * FP32 accumulation) that corrects the vertical-line preconditioner inside gcrk:
+ * q = M^{-1} r + net(r) (see src_b200/csrc/learned.cuh).  It is used when params.iprc == 3; the
+ * plain line preconditioner takes over for the rest of a solve if the network's output is not
+ * finite or the residual stops decreasing (mpg_gcr_stats.fallbacks counts the switches), and
+ * every solve still has to meet the same FP64 stopping test.  No counterpart in the reference.
+ * Training runs on the GPU with the library's own forward/backward kernels and Adam. */
+#define MPG_LEARNED_NPARAM 9505
+/* Initialise the weights (seeded): hidden layers random, output layer zero, so the initial
+ * network returns the plain preconditioner exactly. */
+int mpg_learned_init(mpg_handle h, int seed);
+int mpg_learned_set_params(mpg_handle h, const float *params, int n);
+int mpg_learned_get_params(mpg_handle h, float *params, int n);
+/* q = learned preconditioner applied to field r (impfl = 1 coefficients); r, q are field ids */
+int mpg_learned_forward(mpg_handle h, int r, int q);
+/* Loss 0.5*mean((y - y*)^2) for residual field r and target field t (= A^{-1} r) and its
+ * gradient w.r.t. all MPG_LEARNED_NPARAM parameters (grad may be NULL); no update. */
+int mpg_learned_grad(mpg_handle h, int r, int t, float *grad, double *loss);
+/* one Adam step on the pair (r, t) */
+int mpg_learned_train_pair(mpg_handle h, int r, int t, float lr, double *loss);
+/* Record (r_i, p_i) every `every`-th GCR iteration of plain solves with impfl = 1 (at most
+ * max_records kept; every = 0 stops recording); after a converged solve each record becomes the
+ * pair (r_i, p_i - p*), i.e. (residual, A^{-1} residual). */
+int mpg_learned_harvest(mpg_handle h, int every, int max_records);
+/* `epochs` passes of Adam steps over the recorded pairs (then the records are cleared) */
+int mpg_learned_train_records(mpg_handle h, int epochs, float lr, double *mean_loss, int *npairs);
+
 /* ---------------------------------------------------------------- allocation-free laplc */
 /* laplc(press, alap, impfl) for callers that must not allocate device memory at call time: a
  * host application whose own pool owns all device memory (a Fortran or PyTorch code with a

@@ -29,8 +29,11 @@ EXPORTS = [
     "mpg_mpdatamper", "mpg_courant", "mpg_stats", "mpg_setup", "mpg_step", "mpg_half_forcing",
     "mpg_explicit_forcing", "mpg_post_solve", "mpg_extrapolate", "mpg_get_gcr_stats",
     "mpg_synchronize", "mpg_analyze_mesh", "mpg_get_stream", "mpg_kernel_timing", "mpg_kernel_times",
-    "mpg_laplc_noalloc",
+    "mpg_laplc_noalloc", "mpg_learned_init", "mpg_learned_set_params", "mpg_learned_get_params",
+    "mpg_learned_forward", "mpg_learned_grad", "mpg_learned_train_pair", "mpg_learned_harvest",
+    "mpg_learned_train_records",
 ]
+NPARAM = 9505
 
 
 class MpgError(RuntimeError):
@@ -75,6 +78,15 @@ def lib():
         L.mpg_kernel_timing.argtypes = [vp, ip]
         L.mpg_kernel_times.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
         L.mpg_laplc_noalloc.argtypes = [vp, vp, vp, ip]
+        fp = C.POINTER(C.c_float)
+        L.mpg_learned_init.argtypes = [vp, ip]
+        L.mpg_learned_set_params.argtypes = [vp, fp, ip]
+        L.mpg_learned_get_params.argtypes = [vp, fp, ip]
+        L.mpg_learned_forward.argtypes = [vp, ip, ip]
+        L.mpg_learned_grad.argtypes = [vp, ip, ip, fp, C.POINTER(C.c_double)]
+        L.mpg_learned_train_pair.argtypes = [vp, ip, ip, C.c_float, C.POINTER(C.c_double)]
+        L.mpg_learned_harvest.argtypes = [vp, ip, ip]
+        L.mpg_learned_train_records.argtypes = [vp, ip, C.c_float, C.POINTER(C.c_double), C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -195,6 +207,41 @@ class Solver:
 
     def synchronize(self) -> None:
         _check(self.L.mpg_synchronize(self.h))
+
+    # ---------------------------------------------------------------- learned preconditioner
+    def learned_init(self, seed: int = 0) -> None:
+        _check(self.L.mpg_learned_init(self.h, seed))
+
+    def learned_params(self) -> np.ndarray:
+        out = np.empty(NPARAM, np.float32)
+        _check(self.L.mpg_learned_get_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), NPARAM))
+        return out
+
+    def learned_set_params(self, prm) -> None:
+        a = np.ascontiguousarray(prm, np.float32)
+        _check(self.L.mpg_learned_set_params(self.h, a.ctypes.data_as(C.POINTER(C.c_float)), a.size))
+
+    def learned_forward(self, r: int, q: int) -> None:
+        _check(self.L.mpg_learned_forward(self.h, r, q))
+
+    def learned_grad(self, r: int, t: int):
+        g = np.empty(NPARAM, np.float32)
+        loss = C.c_double()
+        _check(self.L.mpg_learned_grad(self.h, r, t, g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
+        return g, loss.value
+
+    def learned_train_pair(self, r: int, t: int, lr: float) -> float:
+        loss = C.c_double()
+        _check(self.L.mpg_learned_train_pair(self.h, r, t, lr, C.byref(loss)))
+        return loss.value
+
+    def learned_harvest(self, every: int, max_records: int) -> None:
+        _check(self.L.mpg_learned_harvest(self.h, every, max_records))
+
+    def learned_train_records(self, epochs: int, lr: float):
+        loss, n = C.c_double(), C.c_int()
+        _check(self.L.mpg_learned_train_records(self.h, epochs, lr, C.byref(loss), C.byref(n)))
+        return loss.value, n.value
 
     # ---------------------------------------------------------------- instrumentation
     def stream(self) -> int:

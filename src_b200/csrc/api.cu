@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "learned.cuh"
 #include "mpdata.cuh"
 #include "mpgcr_internal.h"
 
@@ -26,11 +27,11 @@ extern "C" const char *mpg_last_error(void) { return g_err.c_str(); }
 // ------------------------------------------------------------------------------ kernel timing
 enum KClass {
     KT_LAP_GRAD, KT_LAP_DIV, KT_PRFR, KT_DIV, KT_LINE, KT_REDUCE, KT_GCR_UPD, KT_AUN, KT_MP_DONOR,
-    KT_MP_GRADB, KT_MP_ANTI, KT_MP_CPCN, KT_MP_PASS2, KT_NODE, KT_COURANT, KT_MISC, KT_SOLVE, KT_COUNT
+    KT_MP_GRADB, KT_MP_ANTI, KT_MP_CPCN, KT_MP_PASS2, KT_NODE, KT_COURANT, KT_MISC, KT_NN, KT_SOLVE, KT_COUNT
 };
 static const char *kKNames[KT_COUNT] = {
     "lap_grad", "lap_div", "prfr", "div", "line_solve", "reduce", "gcr_update", "aun", "mp_donor",
-    "mp_grad_bounds", "mp_anti", "mp_cpcn", "mp_pass2", "node_loops", "courant", "misc", "pressure_solve"};
+    "mp_grad_bounds", "mp_anti", "mp_cpcn", "mp_pass2", "node_loops", "courant", "misc", "learned", "pressure_solve"};
 
 struct KTimer {
     bool on = false;
@@ -74,12 +75,29 @@ struct mpg_solver {
     MpScratchT<float> Sf{};
     float *psi1f = nullptr, *g3f[3] = {}, *mxf = nullptr, *mnf = nullptr;
     // /itero/
-    int32_t niter = 0, nitsm = 0, icount = 0, gstatus = 0;
+    int32_t niter = 0, nitsm = 0, icount = 0, gstatus = 0, last_fallbacks = 0;
     double eer = 0., eem = 0., dvmx_last = 0., rl2_last = 0.;
     double betaunstr1 = 0.;
     HostStatic hs;
     std::vector<int32_t> iperm;
     KTimer kt;
+    struct NN {
+        bool geom = false, infer = false, train = false, have_params = false;
+        float *prm = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+        __nv_bfloat16 *Wbf = nullptr;
+        float *Th = nullptr, *Tv = nullptr, *iDh = nullptr, *iDv = nullptr, *bdiag = nullptr, *feat2 = nullptr,
+              *bnd = nullptr;
+        __nv_bfloat16 *H[4] = {};
+        float *X0 = nullptr, *dH = nullptr, *dH2 = nullptr, *G0 = nullptr, *Gh = nullptr, *Gv = nullptr, *Y = nullptr;
+        __nv_bfloat16 *Xs[3] = {}, *dU = nullptr;
+        double *z = nullptr, *sc = nullptr, *pd = nullptr;
+        float *pf = nullptr;
+        int Npad = 0, adam_t = 0;
+        // harvested pairs
+        int every = 0, maxrec = 0, nrec = 0, solve_first = 0;
+        double *rec_r = nullptr, *rec_t = nullptr;
+        int fallbacks = 0;
+    } nn;
 };
 
 static cudaEvent_t kt_event(mpg_handle h) {
@@ -368,6 +386,201 @@ int op_precon_gcr(mpg_handle h, const double *r, int impfl) {
     }
 }
 
+
+// ------------------------------------------------------------------------------ learned preconditioner
+constexpr int kNNDwBlocks = 296;
+
+struct FinSigma {       // sc[0] = max|r| (the network's input scale)
+    double *sc;
+    __device__ void operator()(const double *v) const { sc[0] = v[0]; }
+};
+struct ProdAbsD {
+    const double *a;
+    __device__ void operator()(int n, double *v) const { v[0] = fabs(a[n]); }
+};
+template <class T>
+struct ProdFinite {     // max |q|; NaN turns into +inf so the host can test it
+    const T *q;
+    __device__ void operator()(int n, double *v) const {
+        const double x = (double)q[n];
+        v[0] = (x == x) ? fabs(x) : INFINITY;
+    }
+};
+
+nn::Geom nn_geom(mpg_handle h) {
+    auto &N = h->nn;
+    return nn::Geom{N.Th, N.Tv, N.iDh, N.iDv, N.bdiag, N.feat2, N.bnd};
+}
+
+int nn_alloc_infer(mpg_handle h) {
+    auto &S = h->nn;
+    int rc;
+    if (!S.geom) {
+        const size_t nh = (size_t)h->NE2 * h->L, n = h->N;
+        if ((rc = dalloc(h, &S.Th, nh)) || (rc = dalloc(h, &S.Tv, n)) || (rc = dalloc(h, &S.iDh, n)) ||
+            (rc = dalloc(h, &S.iDv, n)) || (rc = dalloc(h, &S.feat2, n)) || (rc = dalloc(h, &S.bnd, n)))
+            return rc;
+        if ((rc = upload(h, &S.bdiag, h->hs.lbabs))) return rc;
+        {
+            KTIME(KT_MISC);
+            nn::k_nn_geom_faces<<<grid((int)(nh + n)), kThreads, 0, h->st>>>(h->M, h->d_e2a, h->d_e2b, h->vol,
+                                                                            h->f[MPG_F_RH0], h->f[MPG_F_COEFW],
+                                                                            h->P.delt, S.Th, S.Tv);
+            nn::k_nn_geom_nodes<<<grid(h->N), kThreads, 0, h->st>>>(h->M, S.Th, S.Tv, S.iDh, S.iDv, S.feat2, S.bnd);
+        }
+        if ((rc = check_launch("nn geometry"))) return rc;
+        S.geom = true;
+    }
+    if (!S.infer) {
+        const size_t n = h->N;
+        if ((rc = dalloc(h, &S.prm, nn::NPARAM)) || (rc = dalloc(h, &S.Wbf, (size_t)nn::NL * nn::C * nn::K3)) ||
+            (rc = dalloc(h, &S.H[0], n * nn::C)) || (rc = dalloc(h, &S.H[1], n * nn::C)) ||
+            (rc = dalloc(h, &S.z, n)) || (rc = dalloc(h, &S.sc, 4)))
+            return rc;
+        S.infer = true;
+    }
+    return MPG_OK;
+}
+
+int nn_alloc_train(mpg_handle h) {
+    int rc = nn_alloc_infer(h);
+    if (rc) return rc;
+    auto &S = h->nn;
+    if (S.train) return MPG_OK;
+    const size_t n = h->N;
+    S.Npad = (h->N + 15) / 16 * 16;
+    const size_t np = S.Npad;
+    if ((rc = dalloc(h, &S.grad, nn::NPARAM)) || (rc = dalloc(h, &S.m1, nn::NPARAM)) ||
+        (rc = dalloc(h, &S.m2, nn::NPARAM)) || (rc = dalloc(h, &S.H[2], n * nn::C)) ||
+        (rc = dalloc(h, &S.H[3], n * nn::C)) || (rc = dalloc(h, &S.X0, n * nn::FIN)) ||
+        (rc = dalloc(h, &S.dH, n * nn::C)) || (rc = dalloc(h, &S.dH2, n * nn::C)) ||
+        (rc = dalloc(h, &S.G0, n * nn::C)) || (rc = dalloc(h, &S.Gh, n * nn::C)) ||
+        (rc = dalloc(h, &S.Gv, n * nn::C)) || (rc = dalloc(h, &S.Y, n)) || (rc = dalloc(h, &S.dU, np * nn::C)))
+        return rc;
+    for (int l = 0; l < 3; ++l)
+        if ((rc = dalloc(h, &S.Xs[l], np * nn::K3))) return rc;
+    const size_t nb = (size_t)(h->N + 255) / 256;
+    const size_t pdw = std::max((size_t)(nn::C * nn::FIN + nn::C), (size_t)(nn::C + 2));
+    if ((rc = dalloc(h, &S.pd, nb * pdw)) || (rc = dalloc(h, &S.pf, (size_t)kNNDwBlocks * (nn::C * nn::K3 + nn::C))))
+        return rc;
+    S.train = true;
+    return MPG_OK;
+}
+
+// forward pass on residual r: z = M^{-1} r (impfl coefficients), sigma, the network; q in T.
+// With `train` the activations are kept (H[0..3], X0, Xs) for the backward pass.
+template <class T>
+int nn_forward(mpg_handle h, const double *r, T *q, int impfl, bool train) {
+    auto &S = h->nn;
+    const int N = h->N;
+    int rc;
+    if ((rc = op_line<double>(h, r, S.z, impfl, 0))) return rc;
+    if ((rc = reduce<1>(h, 0x1u, ProdAbsD{r}, FinSigma{S.sc}))) return rc;
+    const nn::Geom G = nn_geom(h);
+    __nv_bfloat16 *Hin = S.H[0];
+    {
+        KTIME(KT_NN);
+        nn::k_nn_input<<<grid(N), kThreads, 0, h->st>>>(N, r, S.z, S.sc, G, S.prm, S.H[0], train ? S.X0 : nullptr);
+        const int ntiles = (N + nn::TILE - 1) / nn::TILE;
+        const int nblk = std::min((ntiles + nn::WARPS - 1) / nn::WARPS, 148 * 16);
+        for (int l = 0; l < nn::NL; ++l) {
+            __nv_bfloat16 *Hout = train ? S.H[l + 1] : S.H[(l + 1) & 1];
+            nn::k_nn_layer<<<nblk, 32 * nn::WARPS, 0, h->st>>>(h->M, G, Hin, S.Wbf + (size_t)l * nn::C * nn::K3,
+                                                               S.prm + nn::OFF_L0 + l * nn::LSTRIDE + nn::C * nn::K3,
+                                                               Hout, train ? S.Xs[l] : nullptr);
+            Hin = Hout;
+        }
+        double *qd = nullptr;
+        float *qf = nullptr;
+        if constexpr (std::is_same<T, double>::value) qd = q; else qf = q;
+        nn::k_nn_output<<<grid(N), kThreads, 0, h->st>>>(N, Hin, S.prm, S.z, S.sc, G, train ? S.Y : nullptr, qd, qf);
+    }
+    return check_launch("nn forward");
+}
+
+// backward pass for target t (after nn_forward with train = true): gradient into S.grad, loss
+int nn_backward(mpg_handle h, const double *t, double *loss) {
+    auto &S = h->nn;
+    const int N = h->N;
+    const nn::Geom G = nn_geom(h);
+    const int nb = (N + 255) / 256;
+    {
+        KTIME(KT_NN);
+        nn::k_nn_out_bwd<<<nb, 256, 0, h->st>>>(N, S.H[3], S.Y, t, S.z, S.sc, G, S.prm, S.dH, S.pd);
+        // partial columns: dw_out (C), db_out, loss
+        nn::k_nn_fold_d<<<1, 64, 0, h->st>>>(nb, nn::C + 2, nn::C + 1, S.pd, S.grad + nn::OFF_WOUT);
+    }
+    double *dl = S.sc + 1;
+    {
+        KTIME(KT_NN);
+        // sum of the per-block loss partials (column C+1) in fixed order
+        const double *pdp = S.pd;
+        k_reduce<1><<<1, kRedThreads, 0, h->st>>>(nb, 0u,
+            [=] __device__(int b, double *v) { v[0] = pdp[(size_t)b * (nn::C + 2) + nn::C + 1]; },
+            [=] __device__(const double *v) { dl[0] = v[0]; }, h->part, h->counter, nullptr);
+    }
+    const int ntiles = (N + nn::TILE - 1) / nn::TILE;
+    const int nblk = std::min((ntiles + nn::BWARPS - 1) / nn::BWARPS, 148 * 16);
+    for (int l = nn::NL - 1; l >= 0; --l) {
+        KTIME(KT_NN);
+        nn::k_nn_layer_bwd<<<nblk, 32 * nn::BWARPS, 0, h->st>>>(N, S.H[l + 1], S.dH, S.Wbf + (size_t)l * nn::C * nn::K3,
+                                                                 G, S.G0, S.Gh, S.Gv, S.dU);
+        nn::k_nn_spread<<<grid(4 * N), kThreads, 0, h->st>>>(h->M, G, S.G0, S.Gh, S.Gv, S.dH2);
+        nn::k_nn_dw<<<kNNDwBlocks, 32 * nn::WARPS, 0, h->st>>>(S.Npad, S.dU, S.Xs[l], S.pf);
+        const int width = nn::C * nn::K3 + nn::C;
+        nn::k_nn_fold_f<<<(width + 255) / 256, 256, 0, h->st>>>(kNNDwBlocks, width, width, S.pf,
+                                                                S.grad + nn::OFF_L0 + l * nn::LSTRIDE);
+        std::swap(S.dH, S.dH2);
+    }
+    {
+        KTIME(KT_NN);
+        nn::k_nn_in_bwd<<<nb, 256, 0, h->st>>>(N, S.H[0], S.dH, S.X0, S.pd);
+        const int width = nn::C * nn::FIN + nn::C;
+        nn::k_nn_fold_d<<<(width + 255) / 256, 256, 0, h->st>>>(nb, width, width, S.pd, S.grad + nn::OFF_WIN);
+    }
+    int rc = check_launch("nn backward");
+    if (rc) return rc;
+    if (loss) {
+        MPG_CUDA(cudaMemcpyAsync(loss, dl, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+        MPG_CUDA(cudaStreamSynchronize(h->st));
+    }
+    return MPG_OK;
+}
+
+int nn_adam(mpg_handle h, float lr) {
+    auto &S = h->nn;
+    S.adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - powf(b1, (float)S.adam_t), c2 = 1.f - powf(b2, (float)S.adam_t);
+    {
+        KTIME(KT_NN);
+        nn::k_nn_adam<<<(nn::NPARAM + 255) / 256, 256, 0, h->st>>>(nn::NPARAM, S.prm, S.grad, S.m1, S.m2, lr, b1, b2,
+                                                                    1e-8f, c1, c2);
+        nn::k_nn_to_bf16<<<(nn::NL * nn::C * nn::K3 + 255) / 256, 256, 0, h->st>>>(S.prm, S.Wbf);
+    }
+    return check_launch("nn adam");
+}
+
+// learned preconditioner inside gcrk; returns 1 in *fell_back when it handed over to the plain one
+template <class T>
+int op_precon_learned(mpg_handle h, const double *r, int impfl, bool &active) {
+    T *qr = Buf<T>::qr(h);
+    int rc;
+    if (active) {
+        if ((rc = nn_forward<T>(h, r, qr, impfl, false))) return rc;
+        if ((rc = reduce<1>(h, 0x1u, ProdFinite<T>{qr}, NoFin{}))) return rc;
+        if ((rc = fetch_result(h, 1))) return rc;
+        if (std::isfinite(h->h_res[0])) return MPG_OK;
+        active = false;                        // non-finite output: plain preconditioner from now on
+        h->nn.fallbacks += 1;
+    }
+    mpg_params save = h->P;
+    h->P.iprc = 2;
+    rc = op_precon_gcr<T>(h, r, impfl);
+    h->P = save;
+    return rc;
+}
+
 // ------------------------------------------------------------------------------ GCR
 struct FinEps {   // eer0, eem0, rl20 clamped by epa
     double *scal;
@@ -558,9 +771,28 @@ int op_gcrk_t(mpg_handle h, double *p, const double *u1, const double *v1, const
     const int N = h->N, lord = P.lord, itmn = P.itmn > 0 ? P.itmn : 3;
     const double eps = P.eps0 / P.delt, epa = 1.e-38;
     int nlc = 0, rc;
+    // learned preconditioner (iprc = 3): active until it fails, then the plain line solve
+    const bool learned = (P.iprc == 3);
+    bool lon = learned;
+    int fallbacks = 0;
+    if (learned) {
+        if ((rc = nn_alloc_infer(h))) return rc;
+        if (!h->nn.have_params) return mpg_fail(MPG_ERR_ARG, "iprc=3 needs network parameters (mpg_learned_init/set_params)");
+    }
+    auto precon = [&]() -> int {
+        if (!learned) return op_precon_gcr<T>(h, h->r, impfl);
+        const int before = h->nn.fallbacks;
+        const int r2 = op_precon_learned<T>(h, h->r, impfl, lon);
+        fallbacks += h->nn.fallbacks - before;
+        return r2;
+    };
+    // harvesting of (r_i, p_i) pairs for training, from plain solves with impfl = 1
+    auto &NNS = h->nn;
+    const bool harvest = NNS.every > 0 && !learned && impfl == 1 && NNS.rec_r;
+    const int first_rec = NNS.nrec;
     if ((rc = op_prfr(h, p, u1, v1, w1, u2, v2, w2, impfl))) return rc;
     if ((rc = op_div(h, u2, v2, w2, h->r, -1))) return rc;
-    if ((rc = op_precon_gcr<T>(h, h->r, impfl))) return rc;
+    if ((rc = precon())) return rc;
     if ((rc = reduce<3>(h, 0x2u, ProdNorm0<T>{B::qr(h), h->r}, FinEps{h->scal}))) return rc;
     if ((rc = fetch_result(h, 3))) return rc;
     double rl20 = h->h_res[2] > epa ? h->h_res[2] : epa;
@@ -582,9 +814,20 @@ int op_gcrk_t(mpg_handle h, double *p, const double *u1, const double *v1, const
             rl2 = h->h_res[1];
             if (!std::isfinite(dvmx) || !std::isfinite(rl2)) { status = MPG_GCR_NAN; break; }
             if (dvmx <= eps && it >= itmn) { status = MPG_GCR_CONVERGED; break; }
-            if (rl2 >= rl20) { status = MPG_GCR_STALLED; break; }
+            if (rl2 >= rl20) {
+                if (!(learned && lon)) { status = MPG_GCR_STALLED; break; }
+                lon = false;                  // no progress with the network: plain from here on
+                ++fallbacks;
+            }
             rl20 = rl2 > epa ? rl2 : epa;
-            if ((rc = op_precon_gcr<T>(h, h->r, impfl))) return rc;
+            if (harvest && nlc % NNS.every == 0 && NNS.nrec < NNS.maxrec) {
+                KTIME(KT_MISC);
+                const size_t off = (size_t)NNS.nrec * N;
+                k_copy<double, double><<<grid(N), kThreads, 0, h->st>>>(N, h->r, NNS.rec_r + off);
+                k_copy<double, double><<<grid(N), kThreads, 0, h->st>>>(N, p, NNS.rec_t + off);
+                NNS.nrec += 1;
+            }
+            if ((rc = precon())) return rc;
             if ((rc = op_laplc_t<T>(h, B::qr(h), B::ar(h), impfl))) return rc;
             nlc = nlc + 1;
             if ((rc = gcr_dots<T>(h, i))) return rc;
@@ -592,6 +835,16 @@ int op_gcrk_t(mpg_handle h, double *p, const double *u1, const double *v1, const
             if ((rc = gcr_update<T>(h, i, lord))) return rc;
         }
     }
+    if (harvest) {
+        if (status == MPG_GCR_CONVERGED) {
+            KTIME(KT_MISC);
+            for (int j = first_rec; j < NNS.nrec; ++j)     // t_j = p_j - p*  (= A^{-1} r_j)
+                k_sub<<<grid(N), kThreads, 0, h->st>>>(N, NNS.rec_t + (size_t)j * N, p, NNS.rec_t + (size_t)j * N);
+        } else {
+            NNS.nrec = first_rec;
+        }
+    }
+    h->last_fallbacks = fallbacks;
     if ((rc = reduce<2>(h, 0x2u, ProdQ<T>{B::qr(h)}, NoFin{}))) return rc;
     if ((rc = fetch_result(h, 2))) return rc;
     double eer = h->h_res[0], eem = h->h_res[1] > -1.e15 ? h->h_res[1] : -1.e15;
@@ -868,7 +1121,7 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     if (prm->lord < 1 || prm->lord > MPG_MAX_LORD) return mpg_fail(MPG_ERR_ARG, "lord out of range 1..16");
     if (prm->nscal < 0 || 4 + prm->nscal > MPG_MAX_UNK) return mpg_fail(MPG_ERR_ARG, "nscal out of range 0..12");
     if (prm->delt <= 0) return mpg_fail(MPG_ERR_ARG, "delt must be positive");
-    if (prm->iprc < 0 || prm->iprc > 2) return mpg_fail(MPG_ERR_ARG, "iprc must be 0, 1 or 2");
+    if (prm->iprc < 0 || prm->iprc > 3) return mpg_fail(MPG_ERR_ARG, "iprc must be 0, 1, 2 or 3");
     if (prm->precision != MPG_PREC_FP64 && prm->precision != MPG_PREC_MIXED)
         return mpg_fail(MPG_ERR_ARG, "precision must be MPG_PREC_FP64 or MPG_PREC_MIXED");
     HostColumnMesh hm;
@@ -1102,6 +1355,7 @@ static void fill_stats(mpg_handle h, mpg_gcr_stats *st) {
     std::memset(st, 0, sizeof(*st));
     st->niter = h->niter; st->nitsm = h->nitsm; st->icount = h->icount; st->status = h->gstatus;
     st->eer = h->eer; st->eem = h->eem; st->dvmx = h->dvmx_last; st->rl2 = h->rl2_last;
+    st->fallbacks = h->last_fallbacks;
 }
 
 extern "C" int mpg_gcrk(mpg_handle h, int p, int u1, int v1, int w1, int u2, int v2, int w2, int impfl,
@@ -1375,4 +1629,122 @@ extern "C" int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap
     k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, F0, F1, F2, h->vol, h->f[MPG_F_RH0], aout);
     k_gather_perm<<<grid(N), kThreads, 0, h->st>>>(N, h->d_perm, aout, alap);
     return check_launch("laplc_noalloc");
+}
+
+// ------------------------------------------------------------------------------ learned preconditioner API
+#include <random>
+
+extern "C" int mpg_learned_init(mpg_handle h, int seed) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    int rc = nn_alloc_infer(h);
+    if (rc) return rc;
+    std::mt19937_64 rng((uint64_t)seed * 0x9E3779B97F4A7C15ull + 12345u);
+    std::vector<float> prm(nn::NPARAM, 0.f);
+    std::normal_distribution<float> gin(0.f, std::sqrt(2.f / nn::FIN)), gl(0.f, std::sqrt(2.f / nn::K3));
+    for (int i = 0; i < nn::C * nn::FIN; ++i) prm[nn::OFF_WIN + i] = gin(rng);
+    for (int i = 0; i < nn::C; ++i) prm[nn::OFF_BIN + i] = 0.01f;
+    for (int l = 0; l < nn::NL; ++l) {
+        for (int i = 0; i < nn::C * nn::K3; ++i) prm[nn::OFF_L0 + l * nn::LSTRIDE + i] = gl(rng);
+        for (int i = 0; i < nn::C; ++i) prm[nn::OFF_L0 + l * nn::LSTRIDE + nn::C * nn::K3 + i] = 0.01f;
+    }
+    // output layer zero: the untrained network returns the plain preconditioner exactly
+    return mpg_learned_set_params(h, prm.data(), nn::NPARAM);
+}
+
+extern "C" int mpg_learned_set_params(mpg_handle h, const float *params, int n) {
+    if (!h || !params) return mpg_fail(MPG_ERR_ARG, "null argument");
+    if (n != nn::NPARAM) return mpg_fail(MPG_ERR_ARG, "expected MPG_LEARNED_NPARAM parameters");
+    int rc = nn_alloc_infer(h);
+    if (rc) return rc;
+    MPG_CUDA(cudaMemcpyAsync(h->nn.prm, params, sizeof(float) * nn::NPARAM, cudaMemcpyHostToDevice, h->st));
+    nn::k_nn_to_bf16<<<(nn::NL * nn::C * nn::K3 + 255) / 256, 256, 0, h->st>>>(h->nn.prm, h->nn.Wbf);
+    if (h->nn.train) {
+        MPG_CUDA(cudaMemsetAsync(h->nn.m1, 0, sizeof(float) * nn::NPARAM, h->st));
+        MPG_CUDA(cudaMemsetAsync(h->nn.m2, 0, sizeof(float) * nn::NPARAM, h->st));
+    }
+    h->nn.adam_t = 0;
+    h->nn.have_params = true;
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    return check_launch("set params");
+}
+
+extern "C" int mpg_learned_get_params(mpg_handle h, float *params, int n) {
+    if (!h || !params) return mpg_fail(MPG_ERR_ARG, "null argument");
+    if (n != nn::NPARAM) return mpg_fail(MPG_ERR_ARG, "expected MPG_LEARNED_NPARAM parameters");
+    if (!h->nn.have_params) return mpg_fail(MPG_ERR_ARG, "no network parameters yet");
+    MPG_CUDA(cudaMemcpyAsync(params, h->nn.prm, sizeof(float) * nn::NPARAM, cudaMemcpyDeviceToHost, h->st));
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    return MPG_OK;
+}
+
+extern "C" int mpg_learned_forward(mpg_handle h, int r, int q) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (!h->nn.have_params) return mpg_fail(MPG_ERR_ARG, "no network parameters yet");
+    FLD(rr, r);
+    FLD(qq, q);
+    if (rr == qq) return mpg_fail(MPG_ERR_ARG, "learned_forward: r and q must differ");
+    return nn_forward<double>(h, rr, qq, 1, false);
+}
+
+extern "C" int mpg_learned_grad(mpg_handle h, int r, int t, float *grad, double *loss) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (!h->nn.have_params) return mpg_fail(MPG_ERR_ARG, "no network parameters yet");
+    FLD(rr, r);
+    FLD(tt, t);
+    int rc = nn_alloc_train(h);
+    if (rc) return rc;
+    if ((rc = nn_forward<double>(h, rr, h->tres, 1, true))) return rc;
+    if ((rc = nn_backward(h, tt, loss))) return rc;
+    if (grad) {
+        MPG_CUDA(cudaMemcpyAsync(grad, h->nn.grad, sizeof(float) * nn::NPARAM, cudaMemcpyDeviceToHost, h->st));
+        MPG_CUDA(cudaStreamSynchronize(h->st));
+    }
+    return MPG_OK;
+}
+
+extern "C" int mpg_learned_train_pair(mpg_handle h, int r, int t, float lr, double *loss) {
+    int rc = mpg_learned_grad(h, r, t, nullptr, loss);
+    if (rc) return rc;
+    return nn_adam(h, lr);
+}
+
+extern "C" int mpg_learned_harvest(mpg_handle h, int every, int max_records) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (every < 0 || max_records < 0) return mpg_fail(MPG_ERR_ARG, "every and max_records must be >= 0");
+    auto &S = h->nn;
+    if (every > 0 && max_records > S.maxrec) {
+        if (S.rec_r) return mpg_fail(MPG_ERR_ARG, "harvest capacity can only be set once per handle");
+        int rc;
+        if ((rc = dalloc(h, &S.rec_r, (size_t)max_records * h->N, false)) ||
+            (rc = dalloc(h, &S.rec_t, (size_t)max_records * h->N, false)))
+            return rc;
+        S.maxrec = max_records;
+    }
+    S.every = every;
+    return MPG_OK;
+}
+
+extern "C" int mpg_learned_train_records(mpg_handle h, int epochs, float lr, double *mean_loss, int *npairs) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (!h->nn.have_params) return mpg_fail(MPG_ERR_ARG, "no network parameters yet");
+    auto &S = h->nn;
+    int rc = nn_alloc_train(h);
+    if (rc) return rc;
+    double sum = 0.;
+    for (int ep = 0; ep < epochs; ++ep) {
+        sum = 0.;
+        for (int j = 0; j < S.nrec; ++j) {
+            double l = 0.;
+            const double *rj = S.rec_r + (size_t)j * h->N, *tj = S.rec_t + (size_t)j * h->N;
+            if ((rc = nn_forward<double>(h, rj, h->tres, 1, true))) return rc;
+            if ((rc = nn_backward(h, tj, &l))) return rc;
+            if ((rc = nn_adam(h, lr))) return rc;
+            sum += l;
+        }
+    }
+    if (mean_loss) *mean_loss = S.nrec ? sum / S.nrec : 0.;
+    if (npairs) *npairs = S.nrec;
+    S.nrec = 0;
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    return MPG_OK;
 }

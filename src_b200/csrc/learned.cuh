@@ -1,0 +1,556 @@
+// Learned correction of the vertical-line preconditioner: an edge message-passing network
+// (3 layers, 32 hidden channels) evaluated and trained with the kernels below.  No counterpart
+// exists in the reference; it plugs in where gcrk calls precon (ref.f:1836, ref.f:1898).
+//
+//   z      = M^{-1} r                        (vertical-line Thomas solve, FP64)
+//   x_n    = [ r_n/s, z_n |b_n|/s, ln(Dv_n/Dh_n)/8, bnd_n ]      s = max|r|, b = line diagonal
+//   h0     = relu(W_in x + b_in)                                  4 -> 32, FP32 FMA
+//   h_l    = relu(W_l [h_{l-1}; A_h(h_{l-1}); A_v(h_{l-1})] + b_l), l = 1..3   96 -> 32
+//   A_*(h)_n = sum over horizontal (vertical) faces of (T_nj / D_n) (h_j - h_n)
+//   y      = w_out . h3 + b_out,   q = z + y s / |b|                             (returned)
+//
+// T_nj is the face coupling 0.5 dt |S|^2 rho_f / vol_f of the face (n, j), D_n its sum over the
+// node's horizontal (vertical) faces.  Activations are stored in BF16 (node-major, 32 channels =
+// 64 bytes per node, so a neighbour gather reads one contiguous 64-byte row); the 96 -> 32
+// transforms run on the tensor cores with BF16 operands and FP32 accumulation; the weight
+// gradients are reduced deterministically (per-block partials folded in a fixed order).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <mma.h>
+
+#include "kernels.cuh"
+
+namespace mpgk {
+namespace nn {
+
+constexpr int C = 32;            // hidden channels
+constexpr int FIN = 4;           // input features
+constexpr int K3 = 3 * C;        // layer input width
+constexpr int NL = 3;            // message-passing layers
+// parameter vector layout (FP32 master copy)
+constexpr int OFF_WIN = 0;                     // [C][FIN]
+constexpr int OFF_BIN = OFF_WIN + C * FIN;     // [C]
+constexpr int OFF_L0 = OFF_BIN + C;            // per layer: W [C][K3], b [C]
+constexpr int LSTRIDE = C * K3 + C;
+constexpr int OFF_WOUT = OFF_L0 + NL * LSTRIDE;  // [C]
+constexpr int OFF_BOUT = OFF_WOUT + C;           // [1]
+constexpr int NPARAM = OFF_BOUT + 1;             // 9505
+
+constexpr int WARPS = 4;                          // warps per block in the layer kernels
+constexpr int TILE = 32;                          // nodes per warp tile
+constexpr int BWARPS = 2;                         // warps per block in k_nn_layer_bwd
+
+struct Geom {
+    const float *Th;        // [NE2*L] horizontal face coupling
+    const float *Tv;        // [N] vertical face coupling (face (c,k)->(c,k+1) at c*L+k)
+    const float *iDh, *iDv; // [N] 1/sum of couplings (0 when the node has no such face)
+    const float *bdiag;     // [N] |b| of the line matrix (impfl = 1)
+    const float *feat2;     // [N] ln(Dv/Dh)/8
+    const float *bnd;       // [N] 1 at boundary nodes
+};
+
+__device__ __forceinline__ float face_T(const ColMesh &M, const Geom &G, const Face &f) {
+    return f.vert ? G.Tv[f.si] : G.Th[f.si];
+}
+
+// 8 consecutive BF16 channels as one 16-byte load
+struct alignas(16) B8 { __nv_bfloat162 v[4]; };
+// what the face loops load per face (namespace-scope types: a class declared inside the
+// loading lambda came back with a wrong layout from for_faces)
+struct RowB { B8 h; float t; };
+struct RowF { float4 lo, hi; float t; };
+
+__device__ __forceinline__ void b8_to_f(const B8 &b, float *f) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float2 t = __bfloat1622float2(b.v[i]);
+        f[2 * i] = t.x;
+        f[2 * i + 1] = t.y;
+    }
+}
+
+// ---------------------------------------------------------------------------------- forward
+// h0 = relu(W_in x + b_in); the features also go to X0 (FP32 [N][FIN]) for the backward pass
+__global__ void k_nn_input(int N, const double *__restrict__ r, const double *__restrict__ z,
+                           const double *__restrict__ sc, Geom G, const float *__restrict__ prm,
+                           __nv_bfloat16 *__restrict__ H0, float *__restrict__ X0) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const double s = sc[0] > 0. ? sc[0] : 1.;
+    float x[FIN];
+    x[0] = (float)(r[n] / s);
+    x[1] = (float)(z[n] * (double)G.bdiag[n] / s);
+    x[2] = G.feat2[n];
+    x[3] = G.bnd[n];
+    if (X0) {
+#pragma unroll
+        for (int i = 0; i < FIN; ++i) X0[(size_t)n * FIN + i] = x[i];
+    }
+    __align__(16) __nv_bfloat16 o[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        float u = prm[OFF_BIN + c];
+#pragma unroll
+        for (int i = 0; i < FIN; ++i) u += prm[OFF_WIN + c * FIN + i] * x[i];
+        o[c] = __float2bfloat16(u > 0.f ? u : 0.f);
+    }
+    const uint4 *src = reinterpret_cast<const uint4 *>(o);
+    uint4 *dst = reinterpret_cast<uint4 *>(H0 + (size_t)n * C);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dst[i] = src[i];
+}
+
+// The 96-wide layer input of node n, quarter q (channels 8q..8q+7) of each 32-channel block:
+// [h_n ; A_h(h)_n ; A_v(h)_n]
+__device__ __forceinline__ void layer_row(const ColMesh &M, const Geom &G, const __nv_bfloat16 *__restrict__ H,
+                                          int n, int q, float *self, float *ah, float *av) {
+    const int c = n / M.L, k = n - c * M.L;
+    B8 sb = *reinterpret_cast<const B8 *>(H + (size_t)n * C + 8 * q);
+    b8_to_f(sb, self);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) { ah[i] = 0.f; av[i] = 0.f; }
+    const float ih = G.iDh[n], iv = G.iDv[n];
+    for_faces(M, c, k, n,
+        [&](const Face &f) {
+            RowB p;
+            p.h = *reinterpret_cast<const B8 *>(H + (size_t)f.j * C + 8 * q);
+            p.t = face_T(M, G, f);
+            return p;
+        },
+        [&](const Face &f, const auto &p) {
+            float hj[8];
+            b8_to_f(p.h, hj);
+            const float w = p.t * (f.vert ? iv : ih);
+            if (f.vert) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) av[i] += w * (hj[i] - self[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) ah[i] += w * (hj[i] - self[i]);
+            }
+        });
+}
+
+// One message-passing layer.  Each warp builds a 32 x 96 BF16 input tile in shared memory
+// (4 lanes per node, 8 channels per lane), multiplies it by W^T (96 x 32) on the tensor cores
+// and applies bias + ReLU.  With Xs != null the input rows are also kept for the backward pass.
+__global__ void __launch_bounds__(32 * WARPS)
+k_nn_layer(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __nv_bfloat16 *__restrict__ Wbf,
+           const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Hout, __nv_bfloat16 *__restrict__ Xs) {
+    using namespace nvcuda;
+    __shared__ __align__(32) __nv_bfloat16 sW[K3 * C];             // W^T: [k][n]
+    __shared__ __align__(32) __nv_bfloat16 sX[WARPS][TILE * K3];
+    __shared__ __align__(32) float sC[WARPS][TILE * C];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < K3 * C; i += blockDim.x) {
+        const int kk = i / C, nn = i - kk * C;
+        sW[i] = Wbf[nn * K3 + kk];
+    }
+    __syncthreads();
+    const int N = M.N;
+    const int ntiles = (N + TILE - 1) / TILE;
+    for (int t = blockIdx.x * WARPS + w; t < ntiles; t += gridDim.x * WARPS) {
+        const int base = t * TILE;
+        __nv_bfloat16 *X = sX[w];
+        for (int pass = 0; pass < TILE / 8; ++pass) {
+            const int m = pass * 8 + (lane >> 2), q = lane & 3;
+            const int n = base + m;
+            float self[8], ah[8], av[8];
+            if (n < N) {
+                layer_row(M, G, Hin, n, q, self, ah, av);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) { self[i] = 0.f; ah[i] = 0.f; av[i] = 0.f; }
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                X[m * K3 + 8 * q + i] = __float2bfloat16(self[i]);
+                X[m * K3 + C + 8 * q + i] = __float2bfloat16(ah[i]);
+                X[m * K3 + 2 * C + 8 * q + i] = __float2bfloat16(av[i]);
+            }
+        }
+        __syncwarp();
+        for (int rt = 0; rt < TILE / 16; ++rt) {
+            for (int ct = 0; ct < C / 16; ++ct) {
+                wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+                wmma::fill_fragment(acc, 0.f);
+#pragma unroll
+                for (int kc = 0; kc < K3 / 16; ++kc) {
+                    wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
+                    wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b;
+                    wmma::load_matrix_sync(a, X + rt * 16 * K3 + kc * 16, K3);
+                    wmma::load_matrix_sync(b, sW + kc * 16 * C + ct * 16, C);
+                    wmma::mma_sync(acc, a, b, acc);
+                }
+                wmma::store_matrix_sync(sC[w] + rt * 16 * C + ct * 16, acc, C, wmma::mem_row_major);
+            }
+        }
+        __syncwarp();
+        // epilogue: row m = lane, 32 channels
+        {
+            const int n = base + lane;
+            if (n < N) {
+                __align__(16) __nv_bfloat16 o[C];
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const float u = sC[w][lane * C + c] + bias[c];
+                    o[c] = __float2bfloat16(u > 0.f ? u : 0.f);
+                }
+                const uint4 *src = reinterpret_cast<const uint4 *>(o);
+                uint4 *dst = reinterpret_cast<uint4 *>(Hout + (size_t)n * C);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) dst[i] = src[i];
+                if (Xs) {
+                    const uint4 *xs = reinterpret_cast<const uint4 *>(X + lane * K3);
+                    uint4 *xd = reinterpret_cast<uint4 *>(Xs + (size_t)n * K3);
+#pragma unroll
+                    for (int i = 0; i < K3 / 8; ++i) xd[i] = xs[i];
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// y = w_out . h3 + b_out;  q = z + y s / |b|;  with Y != null also keeps y
+__global__ void k_nn_output(int N, const __nv_bfloat16 *__restrict__ H3, const float *__restrict__ prm,
+                            const double *__restrict__ z, const double *__restrict__ sc, Geom G,
+                            float *__restrict__ Y, double *__restrict__ qd, float *__restrict__ qf) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    float h[C];
+    const B8 *src = reinterpret_cast<const B8 *>(H3 + (size_t)n * C);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) b8_to_f(src[i], h + 8 * i);
+    float y = prm[OFF_BOUT];
+#pragma unroll
+    for (int c = 0; c < C; ++c) y += prm[OFF_WOUT + c] * h[c];
+    if (Y) Y[n] = y;
+    const double s = sc[0] > 0. ? sc[0] : 1.;
+    const double q = z[n] + (double)y * s / (double)G.bdiag[n];
+    if (qd) qd[n] = q;
+    if (qf) qf[n] = (float)q;
+}
+
+// ---------------------------------------------------------------------------------- backward
+// loss = 0.5 * mean_n (y_n - ystar_n)^2, ystar = (t_n - z_n) |b_n| / s.  Per node: dy, the
+// gradient w.r.t. h3 (FP32 [N][C]), and block partials of dw_out, db_out and the loss.
+__global__ void __launch_bounds__(256)
+k_nn_out_bwd(int N, const __nv_bfloat16 *__restrict__ H3, const float *__restrict__ Y, const double *__restrict__ t,
+             const double *__restrict__ z, const double *__restrict__ sc, Geom G, const float *__restrict__ prm,
+             float *__restrict__ dH, double *__restrict__ part /* [gridDim][C+2] */) {
+    __shared__ double sp[256 / 32][C + 2];
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[C + 2];
+#pragma unroll
+    for (int i = 0; i < C + 2; ++i) acc[i] = 0.;
+    if (n < N) {
+        const double s = sc[0] > 0. ? sc[0] : 1.;
+        const double ystar = (t[n] - z[n]) * (double)G.bdiag[n] / s;
+        const double e = (double)Y[n] - ystar;
+        const double dy = e / (double)N;
+        float h[C];
+        const B8 *src = reinterpret_cast<const B8 *>(H3 + (size_t)n * C);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) b8_to_f(src[i], h + 8 * i);
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            acc[c] = dy * (double)h[c];
+            dH[(size_t)n * C + c] = (float)(dy * (double)prm[OFF_WOUT + c]);
+        }
+        acc[C] = dy;
+        acc[C + 1] = 0.5 * e * e / (double)N;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < C + 2; ++i) {
+        double a = acc[i];
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+        if (lane == 0) sp[wid][i] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < C + 2) {
+        double a = sp[0][threadIdx.x];
+        for (int q = 1; q < 256 / 32; ++q) a += sp[q][threadIdx.x];
+        part[(size_t)blockIdx.x * (C + 2) + threadIdx.x] = a;
+    }
+}
+
+// Layer backward, part 1: du = dH (.) [h > 0]; dX = du W (tensor cores); writes the per-node
+// gradient pieces: G0 = dX_self - dX_ah - dX_av (to the node itself), Gh = dX_ah * iDh,
+// Gv = dX_av * iDv (to be spread over the faces by k_nn_spread), and du in BF16 for dW.
+__global__ void __launch_bounds__(32 * BWARPS)
+k_nn_layer_bwd(int N, const __nv_bfloat16 *__restrict__ Hout, const float *__restrict__ dH,
+               const __nv_bfloat16 *__restrict__ Wbf, Geom G, float *__restrict__ G0, float *__restrict__ Gh,
+               float *__restrict__ Gv, __nv_bfloat16 *__restrict__ dU) {
+    using namespace nvcuda;
+    __shared__ __align__(32) __nv_bfloat16 sW[C * K3];               // W: [out][in]
+    __shared__ __align__(32) __nv_bfloat16 sD[BWARPS][TILE * C];      // du tile
+    __shared__ __align__(32) float sO[BWARPS][TILE * K3];             // dX tile
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < C * K3; i += blockDim.x) sW[i] = Wbf[i];
+    __syncthreads();
+    const int ntiles = (N + TILE - 1) / TILE;
+    for (int t = blockIdx.x * BWARPS + w; t < ntiles; t += gridDim.x * BWARPS) {
+        const int base = t * TILE;
+        {
+            const int n = base + lane;
+            __align__(16) __nv_bfloat16 du[C];
+            if (n < N) {
+                float h[C];
+                const B8 *src = reinterpret_cast<const B8 *>(Hout + (size_t)n * C);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) b8_to_f(src[i], h + 8 * i);
+#pragma unroll
+                for (int c = 0; c < C; ++c) du[c] = __float2bfloat16(h[c] > 0.f ? dH[(size_t)n * C + c] : 0.f);
+                const uint4 *s4 = reinterpret_cast<const uint4 *>(du);
+                uint4 *d4 = reinterpret_cast<uint4 *>(dU + (size_t)n * C);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) d4[i] = s4[i];
+            } else {
+#pragma unroll
+                for (int c = 0; c < C; ++c) du[c] = __float2bfloat16(0.f);
+            }
+#pragma unroll
+            for (int c = 0; c < C; ++c) sD[w][lane * C + c] = du[c];
+        }
+        __syncwarp();
+        for (int rt = 0; rt < TILE / 16; ++rt) {
+            for (int ct = 0; ct < K3 / 16; ++ct) {
+                wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
+                wmma::fill_fragment(acc, 0.f);
+#pragma unroll
+                for (int kc = 0; kc < C / 16; ++kc) {
+                    wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
+                    wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b;
+                    wmma::load_matrix_sync(a, sD[w] + rt * 16 * C + kc * 16, C);
+                    wmma::load_matrix_sync(b, sW + kc * 16 * K3 + ct * 16, K3);
+                    wmma::mma_sync(acc, a, b, acc);
+                }
+                wmma::store_matrix_sync(sO[w] + rt * 16 * K3 + ct * 16, acc, K3, wmma::mem_row_major);
+            }
+        }
+        __syncwarp();
+        {
+            const int n = base + lane;
+            if (n < N) {
+                const float ih = G.iDh[n], iv = G.iDv[n];
+                const float *o = sO[w] + lane * K3;
+#pragma unroll
+                for (int c = 0; c < C; ++c) {
+                    const float dah = ih > 0.f ? o[C + c] : 0.f, dav = iv > 0.f ? o[2 * C + c] : 0.f;
+                    G0[(size_t)n * C + c] = o[c] - dah - dav;
+                    Gh[(size_t)n * C + c] = dah * ih;
+                    Gv[(size_t)n * C + c] = dav * iv;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Layer backward, part 2: dH_prev(j) = G0(j) + sum over faces (j,n) of T_jn * G(n), with Gh for
+// horizontal and Gv for vertical faces (the transpose of the aggregation).
+__global__ void k_nn_spread(ColMesh M, Geom G, const float *__restrict__ G0, const float *__restrict__ Gh,
+                            const float *__restrict__ Gv, float *__restrict__ dHprev) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = t >> 2, q = t & 3;              // 4 threads per node, 8 channels each
+    if (n >= M.N) return;
+    const int c = n / M.L, k = n - c * M.L;
+    float a[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = G0[(size_t)n * C + 8 * q + i];
+    for_faces(M, c, k, n,
+        [&](const Face &f) {
+            RowF p;
+            const float *src = (f.vert ? Gv : Gh) + (size_t)f.j * C + 8 * q;
+            p.lo = *reinterpret_cast<const float4 *>(src);
+            p.hi = *reinterpret_cast<const float4 *>(src + 4);
+            p.t = face_T(M, G, f);
+            return p;
+        },
+        [&](const Face &f, const auto &p) {
+            a[0] += p.t * p.lo.x; a[1] += p.t * p.lo.y; a[2] += p.t * p.lo.z; a[3] += p.t * p.lo.w;
+            a[4] += p.t * p.hi.x; a[5] += p.t * p.hi.y; a[6] += p.t * p.hi.z; a[7] += p.t * p.hi.w;
+        });
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dHprev[(size_t)n * C + 8 * q + i] = a[i];
+}
+
+// dW (C x K3) = sum over nodes of du^T X; db = sum du.  Each block accumulates its node tiles on
+// the tensor cores, folds its warps in order and writes one partial (deterministic).
+__global__ void __launch_bounds__(32 * WARPS)
+k_nn_dw(int Npad, const __nv_bfloat16 *__restrict__ dU, const __nv_bfloat16 *__restrict__ Xs,
+        float *__restrict__ part /* [gridDim][C*K3 + C] */) {
+    using namespace nvcuda;
+    __shared__ __align__(32) float sAcc[C * K3];
+    __shared__ float sB[WARPS][C];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[C / 16][K3 / 16];
+#pragma unroll
+    for (int a = 0; a < C / 16; ++a)
+#pragma unroll
+        for (int b = 0; b < K3 / 16; ++b) wmma::fill_fragment(acc[a][b], 0.f);
+    float db = 0.f;
+    const int ntiles = Npad / 16;         // rows N..Npad-1 of dU and Xs are zero
+    for (int t = blockIdx.x * WARPS + w; t < ntiles; t += gridDim.x * WARPS) {
+        const int base = t * 16;
+        // A = du^T (C x 16 nodes): du tile [16][C] read as column-major (ld = C)
+#pragma unroll
+        for (int kb = 0; kb < C / 16; ++kb) {
+            wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::col_major> a;
+            wmma::load_matrix_sync(a, dU + (size_t)base * C + kb * 16, C);
+#pragma unroll
+            for (int ct = 0; ct < K3 / 16; ++ct) {
+                wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b;
+                wmma::load_matrix_sync(b, Xs + (size_t)base * K3 + ct * 16, K3);
+                wmma::mma_sync(acc[kb][ct], a, b, acc[kb][ct]);
+            }
+        }
+        for (int m = 0; m < 16; ++m) db += __bfloat162float(dU[(size_t)(base + m) * C + lane]);
+    }
+    // fold warps in order into shared memory
+    for (int i = threadIdx.x; i < C * K3; i += blockDim.x) sAcc[i] = 0.f;
+    sB[w][lane] = db;
+    __syncthreads();
+    for (int ww = 0; ww < WARPS; ++ww) {
+        if (w == ww) {
+#pragma unroll
+            for (int a = 0; a < C / 16; ++a)
+#pragma unroll
+                for (int b = 0; b < K3 / 16; ++b) {
+                    wmma::fragment<wmma::accumulator, 16, 16, 16, float> cur;
+                    wmma::load_matrix_sync(cur, sAcc + a * 16 * K3 + b * 16, K3, wmma::mem_row_major);
+                    for (int e = 0; e < cur.num_elements; ++e) cur.x[e] += acc[a][b].x[e];
+                    wmma::store_matrix_sync(sAcc + a * 16 * K3 + b * 16, cur, K3, wmma::mem_row_major);
+                }
+        }
+        __syncthreads();
+    }
+    float *pp = part + (size_t)blockIdx.x * (C * K3 + C);
+    for (int i = threadIdx.x; i < C * K3; i += blockDim.x) pp[i] = sAcc[i];
+    if (threadIdx.x < C) {
+        float s = 0.f;
+        for (int ww = 0; ww < WARPS; ++ww) s += sB[ww][threadIdx.x];
+        pp[C * K3 + threadIdx.x] = s;
+    }
+}
+
+// input layer backward: du0 = dH0 (.) [h0 > 0]; partials of dW_in (C x FIN) and db_in
+__global__ void __launch_bounds__(256)
+k_nn_in_bwd(int N, const __nv_bfloat16 *__restrict__ H0, const float *__restrict__ dH, const float *__restrict__ X0,
+            double *__restrict__ part /* [gridDim][C*FIN + C] */) {
+    __shared__ double sp[256 / 32][C * FIN + C];
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float h[C], du[C], x[FIN];
+    if (n < N) {
+        const B8 *src = reinterpret_cast<const B8 *>(H0 + (size_t)n * C);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) b8_to_f(src[i], h + 8 * i);
+#pragma unroll
+        for (int c = 0; c < C; ++c) du[c] = h[c] > 0.f ? dH[(size_t)n * C + c] : 0.f;
+#pragma unroll
+        for (int i = 0; i < FIN; ++i) x[i] = X0[(size_t)n * FIN + i];
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; ++c) du[c] = 0.f;
+#pragma unroll
+        for (int i = 0; i < FIN; ++i) x[i] = 0.f;
+    }
+    for (int c = 0; c < C; ++c) {
+        for (int i = 0; i <= FIN; ++i) {
+            double a = i < FIN ? (double)du[c] * (double)x[i] : (double)du[c];
+            for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+            if (lane == 0) sp[wid][i < FIN ? c * FIN + i : C * FIN + c] = a;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < C * FIN + C; i += blockDim.x) {
+        double a = sp[0][i];
+        for (int q = 1; q < 256 / 32; ++q) a += sp[q][i];
+        part[(size_t)blockIdx.x * (C * FIN + C) + i] = a;
+    }
+}
+
+// fold per-block partials (fixed order) into the gradient vector, offsets given per segment
+__global__ void k_nn_fold_f(int nblk, int stride, int width, const float *__restrict__ part, float *__restrict__ g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= width) return;
+    double s = 0.;
+    for (int b = 0; b < nblk; ++b) s += (double)part[(size_t)b * stride + i];
+    g[i] = (float)s;
+}
+__global__ void k_nn_fold_d(int nblk, int stride, int width, const double *__restrict__ part, float *__restrict__ g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= width) return;
+    double s = 0.;
+    for (int b = 0; b < nblk; ++b) s += part[(size_t)b * stride + i];
+    g[i] = (float)s;
+}
+
+// Adam step on the FP32 master parameters, then refresh the BF16 layer matrices
+__global__ void k_nn_adam(int np, float *__restrict__ prm, const float *__restrict__ g, float *__restrict__ m1,
+                          float *__restrict__ m2, float lr, float b1, float b2, float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    const float gi = g[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gi;
+    const float b = b2 * m2[i] + (1.f - b2) * gi * gi;
+    m1[i] = a;
+    m2[i] = b;
+    prm[i] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
+}
+
+__global__ void k_nn_to_bf16(const float *__restrict__ prm, __nv_bfloat16 *__restrict__ W) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NL * C * K3) return;
+    const int l = i / (C * K3), o = i - l * C * K3;
+    W[i] = __float2bfloat16(prm[OFF_L0 + l * LSTRIDE + o]);
+}
+
+// face couplings and per-node sums for the network (once per handle)
+__global__ void k_nn_geom_faces(ColMesh M, const int32_t *__restrict__ e2a, const int32_t *__restrict__ e2b,
+                                const double *__restrict__ vol, const double *__restrict__ rh0,
+                                const double *__restrict__ coefw, double dt, float *__restrict__ Th,
+                                float *__restrict__ Tv) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nh = M.NE2 * M.L;
+    if (t < nh) {
+        const int e = t / M.L, k = t - e * M.L;
+        const int a = e2a[e] * M.L + k, b = e2b[e] * M.L + k;
+        const double s2 = M.Sh[0][t] * M.Sh[0][t] + M.Sh[1][t] * M.Sh[1][t] + M.Sh[2][t] * M.Sh[2][t];
+        Th[t] = (float)(0.5 * dt * s2 * 0.5 * (rh0[a] + rh0[b]) / (0.5 * (vol[a] + vol[b])));
+    } else if (t < nh + M.N) {
+        const int n = t - nh;
+        const int k = n % M.L;
+        float v = 0.f;
+        if (k + 1 < M.L) {
+            const double s2 = M.Sv[0][n] * M.Sv[0][n] + M.Sv[1][n] * M.Sv[1][n]
+                            + M.Sv[2][n] * M.Sv[2][n] * 0.5 * (coefw[n] + coefw[n + 1]);
+            v = (float)(0.5 * dt * s2 * 0.5 * (rh0[n] + rh0[n + 1]) / (0.5 * (vol[n] + vol[n + 1])));
+        }
+        Tv[n] = v;
+    }
+}
+
+__global__ void k_nn_geom_nodes(ColMesh M, const float *__restrict__ Th, const float *__restrict__ Tv,
+                                float *__restrict__ iDh, float *__restrict__ iDv, float *__restrict__ feat2,
+                                float *__restrict__ bnd) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M.N) return;
+    const int c = n / M.L, k = n - c * M.L;
+    float dh = 0.f, dv = 0.f;
+    for_faces(M, c, k, n, [&](const Face &f) { return f.vert ? Tv[f.si] : Th[f.si]; },
+              [&](const Face &f, float t) {
+                  if (f.vert) dv += t; else dh += t;
+              });
+    iDh[n] = dh > 0.f ? 1.f / dh : 0.f;
+    iDv[n] = dv > 0.f ? 1.f / dv : 0.f;
+    feat2[n] = (dh > 0.f && dv > 0.f) ? logf(dv / dh) / 8.f : 0.f;
+    bnd[n] = (k == 0 || k == M.L - 1) ? 1.f : 0.f;
+}
+
+}  // namespace nn
+}  // namespace mpgk

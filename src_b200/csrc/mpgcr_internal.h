@@ -87,6 +87,7 @@ struct HostStatic {
     // line preconditioner, per impfl, in the column-interleaved layout used by the solve kernel:
     // sub-diagonal a, inverse pivot 1/m and c' of the Thomas factorisation
     std::vector<double> la[2], lm[2], lcp[2];
+    std::vector<float> lbabs;       // |diagonal| of the line matrix for impfl = 1 (node order)
 };
 
 int mpg_host_static(const mpg_params *P, const mpg_mesh_ref *m, const HostColumnMesh &cm,

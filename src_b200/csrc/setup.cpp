@@ -459,6 +459,10 @@ int mpg_host_static(const mpg_params *P, const mpg_mesh_ref *m, const HostColumn
             c[n] = Tc[q][i] / vr;
             b[n] = (dh - a[n]) - c[n];
         }
+        if (q == 1) {
+            hs->lbabs.resize(N);
+            for (int n = 0; n < N; ++n) hs->lbabs[n] = (float)std::fabs(b[n]);
+        }
         size_t nint_sz = (size_t)((NC + 31) / 32) * 32 * L;
         hs->la[q].assign(nint_sz, 0.);
         hs->lm[q].assign(nint_sz, 1.);

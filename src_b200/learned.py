@@ -1,0 +1,69 @@
+"""Training and evaluation driver for the learned correction of the vertical-line preconditioner.
+
+The network, its forward and backward passes and the Adam update live in the CUDA library
+(src_b200/csrc/learned.cuh); this module only sequences them:
+
+  1. run plain solves (iprc=2) with harvesting on: every `every`-th GCR iteration the library
+     records the residual r_i and the iterate p_i; after the solve converges each record becomes
+     the pair (r_i, p_i - p*), i.e. (residual, A^{-1} residual);
+  2. train on the recorded pairs with Adam (`epochs` passes), then keep stepping;
+  3. use the trained weights with iprc=3, where gcrk applies q = M^{-1} r + net(r) and falls back
+     to the plain line solve if the network stops making progress.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from .api import Solver
+from .cabi import F_UNK, RunParams
+
+
+def train(refmesh, params: RunParams, steps: int = 6, every: int = 4, max_records: int = 48,
+          epochs: int = 3, lr: float = 2e-3, seed: int = 0, scalar=None, device: int = 0, log=None):
+    """Harvest pairs from `steps` plain time steps and train on them; returns (weights, history)."""
+    P = RunParams(**{**params.__dict__, "iprc": 2})
+    hist = []
+    with Solver(P, refmesh, device=device) as s:
+        s.setup()
+        if scalar is not None and P.nscal:
+            s.set(F_UNK + 4, scalar)
+        s.learned_init(seed)
+        s.learned_harvest(every, max_records)
+        t0 = time.time()
+        for k in range(steps):
+            s.step(diag=False)
+            loss, n = s.learned_train_records(epochs, lr)
+            hist.append({"step": k, "pairs": n, "loss": loss, "t": time.time() - t0})
+            if log:
+                log(hist[-1])
+        s.learned_harvest(0, 0)
+        return s.learned_params(), hist
+
+
+def compare(refmesh, params: RunParams, weights, steps: int = 5, warm: int = 2, scalar=None, device: int = 0):
+    """GCR iterations and time per step, plain vs learned, over the same steps after `warm`."""
+    out = {}
+    for name, iprc in (("plain", 2), ("learned", 3)):
+        P = RunParams(**{**params.__dict__, "iprc": iprc})
+        with Solver(P, refmesh, device=device) as s:
+            if iprc == 3:
+                s.learned_set_params(weights)
+            s.setup()
+            if scalar is not None and P.nscal:
+                s.set(F_UNK + 4, scalar)
+            for _ in range(warm):
+                s.step(diag=False)
+            s.synchronize()
+            its, fb = [], 0
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                d = s.step()
+                its.append(d.niter1 + d.niter)
+                fb += s.gcr_stats().fallbacks
+            s.synchronize()
+            dt = time.perf_counter() - t0
+            out[name] = {"iters_per_step": float(np.mean(its)), "ms_per_step": 1000 * dt / steps,
+                         "fallbacks": fb, "u": s.get(F_UNK)}
+    return out
