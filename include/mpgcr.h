@@ -74,6 +74,10 @@ typedef struct mpg_params {
     int32_t nscal;               /* passive scalars advected after unk(:,1..4)                      */
     int32_t precision;           /* MPG_PREC_FP64 or MPG_PREC_MIXED                                 */
     int32_t itmn;                /* minimum restart cycles before the convergence test (3, ref.f:1809) */
+    double  nn_rate;             /* iprc = 3: the network keeps being used while ||r||_2 after m GCR
+                                  * iterations (m >= lord) is at most nn_rate^m times its initial
+                                  * value; otherwise the plain line preconditioner takes over for
+                                  * the rest of the solve.  <= 0 selects 0.98.                      */
 } mpg_params;
 
 #define MPG_PREC_FP64  0
@@ -110,6 +114,8 @@ typedef struct mpg_gcr_stats {         /* /itero/ (ref.f:1953-1963) plus the exi
     double  rl2;                       /* final sum r^2                          */
     int32_t fallbacks;                 /* learned-preconditioner fallbacks taken */
     int32_t pad;
+    double  rate;                      /* per-iteration contraction of ||r||_2 over the solve:
+                                        * (rl2 / rl2_initial)^(1/(2*niter))                 */
 } mpg_gcr_stats;
 
 typedef struct mpg_diag {              /* per-step diagnostics printed by mpsolver (ref.f:456-459) */
@@ -121,6 +127,9 @@ typedef struct mpg_diag {              /* per-step diagnostics printed by mpsolv
     double stats[16];                  /* umx,umn,uav,usd, vmx.., wmx.., tmx,tmn,tav,tsd (ref.f:2904) */
     double mass[8];                    /* sum(vol*rh0*unk(:,k)) for the prognostic fields (FP64)  */
     double smin[4], smax[4];           /* min/max of the first passive scalars                     */
+    double rate1;                      /* mpg_gcr_stats.rate of the step's first pressure solve    */
+    int32_t fallbacks;                 /* learned-preconditioner fallbacks in the step's solves    */
+    int32_t pad;
 } mpg_diag;
 
 typedef struct mpg_info {
@@ -178,6 +187,11 @@ int mpg_derivative(mpg_handle h, int unk, int out, int idx);
 int mpg_bcv(mpg_handle h, int u, int v, int w, double flag);
 /* laplc(press, alap, impfl)                             ref.f:1288-1353 */
 int mpg_laplc(mpg_handle h, int press, int alap, int impfl);
+/* Adjoint of laplc in the inner product <u,v>_W = sum vol*rh0*u*v: out such that
+ * <laplc(u), y>_W = <u, out>_W for every u (the transposes of the derivative passes, of the
+ * metric scaling and of bcv's projections, applied in reverse order).  Used to train the
+ * learned preconditioner on the residual norm; no counterpart in the reference. */
+int mpg_laplc_adjoint(mpg_handle h, int y, int out, int impfl);
 /* prfr(press, ustr, vstr, wstr, uout, vout, wout, impfl) ref.f:1536-1580 */
 int mpg_prfr(mpg_handle h, int press, int ustr, int vstr, int wstr,
              int uout, int vout, int wout, int impfl);
@@ -226,8 +240,19 @@ int mpg_learned_set_params(mpg_handle h, const float *params, int n);
 int mpg_learned_get_params(mpg_handle h, float *params, int n);
 /* q = learned preconditioner applied to field r (impfl = 1 coefficients); r, q are field ids */
 int mpg_learned_forward(mpg_handle h, int r, int q);
-/* Loss 0.5*mean((y - y*)^2) for residual field r and target field t (= A^{-1} r) and its
- * gradient w.r.t. all MPG_LEARNED_NPARAM parameters (grad may be NULL); no update. */
+/* Training loss (mpg_learned_loss selects it):
+ *   MPG_NN_LOSS_RESIDUAL (default): 0.5*min_a ||r - a A q||_W^2 / ||r||_W^2 with A = laplc
+ *       (impfl = 1), W = vol*rh0 and q the preconditioner output: the residual left by the best
+ *       GCR step along q, which like GCR ignores the scale of q.  Since A t = r for the pair
+ *       (r, t = A^{-1} r), it measures the error of a q against t in the A^T W A-norm, so t
+ *       itself is not read;
+ *   MPG_NN_LOSS_ERROR: 0.5*mean((y - y*)^2), the network output y regressed on the scaled
+ *       error y* = (t - M^{-1} r)|b|/max|r| of the pair.
+ * mpg_learned_grad returns the loss for residual field r and target field t and its gradient
+ * w.r.t. all MPG_LEARNED_NPARAM parameters (grad may be NULL); no update. */
+#define MPG_NN_LOSS_RESIDUAL 0
+#define MPG_NN_LOSS_ERROR    1
+int mpg_learned_loss(mpg_handle h, int mode);
 int mpg_learned_grad(mpg_handle h, int r, int t, float *grad, double *loss);
 /* one Adam step on the pair (r, t) */
 int mpg_learned_train_pair(mpg_handle h, int r, int t, float lr, double *loss);

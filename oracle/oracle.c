@@ -41,7 +41,7 @@ struct orc {
     double *f[MPG_F_COUNT];
     /* /itero/ */
     int niter, nitsm, icount, gstatus;
-    double eer, eem, dvmx_last, rl2_last;
+    double eer, eem, dvmx_last, rl2_last, rate_last;
     /* vertical structure (NEW line preconditioner) */
     int *up, *dn, *colstart, ncol;
     int *colnodes;
@@ -480,6 +480,8 @@ void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const doubl
     eer0 = AMAX(eer0, epa);
     eem0 = AMAX(eem0, epa);
     rl20 = AMAX(rl20, epa);
+    const double rl2_init = rl20;
+    int nupd = 0;                                              /* updates of p and r (for the rate) */
     for (int k = 0; k < nml; ++k) x[0][k] = qr[k];
     orc_laplc(o, x[0], ax[0], impfl);
     int status = MPG_GCR_MAXIT;
@@ -504,6 +506,7 @@ void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const doubl
                 t1[k] = r[k] * r[k];
             }
             rl2 = rsum(o, t1, nml);
+            ++nupd;
             if (!(dvmx == dvmx) || !(rl2 == rl2)) { status = MPG_GCR_NAN; goto done; }
             if (dvmx <= eps && it >= itmn) { status = MPG_GCR_CONVERGED; goto done; }
             if (rl2 >= rl20) { status = MPG_GCR_STALLED; goto done; }
@@ -554,6 +557,8 @@ done:;
     o->gstatus = status;
     o->dvmx_last = dvmx;
     o->rl2_last = rl2;
+    /* not in the reference: per-iteration contraction of ||r||_2 over the solve */
+    o->rate_last = (nupd > 0 && rl2 > 0. && isfinite(rl2)) ? pow(rl2 / rl2_init, 0.5 / nupd) : 0.;
     if (st) orc_get_gcr_stats(o, st);
     for (int i = 0; i < lord; ++i) { free(x[i]); free(ax[i]); }
     free(x); free(ax); free(ax2); free(axar); free(del); free(r); free(qr); free(ar);
@@ -563,7 +568,7 @@ void orc_get_gcr_stats(orc *o, mpg_gcr_stats *st) {
     memset(st, 0, sizeof(*st));
     st->niter = o->niter; st->nitsm = o->nitsm; st->icount = o->icount;
     st->status = o->gstatus; st->eer = o->eer; st->eem = o->eem;
-    st->dvmx = o->dvmx_last; st->rl2 = o->rl2_last;
+    st->dvmx = o->dvmx_last; st->rl2 = o->rl2_last; st->rate = o->rate_last;
 }
 
 /* ------------------------------------------------------------------ mpdatamper ref.f:3617-3941 */
@@ -1032,6 +1037,7 @@ void orc_step(orc *o, mpg_diag *diag) {
     for (int k = 0; k < 4 + P->nscal; ++k)                     /* ref.f:314-319 */
         orc_mpdatamper(o, f[MPG_F_UNK + k], k + 1);
     int mtrimx = 2, niter1 = 0;
+    double rate1 = 0.;
     for (int mtri = 1; mtri <= mtrimx; ++mtri) {
         for (int ip = 0; ip < n; ++ip) {                       /* ref.f:323-359 */
             double frm1 = 0., frm2 = 0., frm3 = 0.;
@@ -1054,7 +1060,7 @@ void orc_step(orc *o, mpg_diag *diag) {
         int imp = implgw;                                      /* ref.f:361-365 */
         orc_gcrk(o, f[MPG_F_PRPOT], unk1[0], unk1[1], unk1[2], uuu[0], uuu[1], uuu[2], imp, NULL);
         orc_prfr(o, f[MPG_F_PRPOT], unk1[0], unk1[1], unk1[2], uuu[0], uuu[1], uuu[2], imp);
-        if (mtri == 1) niter1 = o->niter;
+        if (mtri == 1) { niter1 = o->niter; rate1 = o->rate_last; }
         for (int ip = 0; ip < n; ++ip) {                       /* ref.f:367-383 */
             ud[0][ip] = uuu[0][ip] * o->gmm[ip] * o->cosa[ip];
             ud[1][ip] = uuu[1][ip] * o->gmm[ip];
@@ -1098,6 +1104,7 @@ void orc_step(orc *o, mpg_diag *diag) {
     orc_courant(o, 1, &dd);
     orc_stats(o, &dd);
     dd.niter1 = niter1;
+    dd.rate1 = rate1;
     if (diag) *diag = dd;
 }
 

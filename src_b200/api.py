@@ -31,7 +31,7 @@ EXPORTS = [
     "mpg_synchronize", "mpg_analyze_mesh", "mpg_get_stream", "mpg_kernel_timing", "mpg_kernel_times",
     "mpg_laplc_noalloc", "mpg_learned_init", "mpg_learned_set_params", "mpg_learned_get_params",
     "mpg_learned_forward", "mpg_learned_grad", "mpg_learned_train_pair", "mpg_learned_harvest",
-    "mpg_learned_train_records",
+    "mpg_learned_train_records", "mpg_learned_loss", "mpg_laplc_adjoint",
 ]
 NPARAM = 9505
 
@@ -59,6 +59,7 @@ def lib():
         L.mpg_derivative.argtypes = [vp, ip, ip, ip]
         L.mpg_bcv.argtypes = [vp, ip, ip, ip, dp]
         L.mpg_laplc.argtypes = [vp, ip, ip, ip]
+        L.mpg_laplc_adjoint.argtypes = [vp, ip, ip, ip]
         L.mpg_prfr.argtypes = [vp] + [ip] * 8
         L.mpg_div.argtypes = [vp, ip, ip, ip, ip, ip, vp]
         L.mpg_precon.argtypes = [vp, ip, ip, ip, ip, ip]
@@ -87,6 +88,7 @@ def lib():
         L.mpg_learned_train_pair.argtypes = [vp, ip, ip, C.c_float, C.POINTER(C.c_double)]
         L.mpg_learned_harvest.argtypes = [vp, ip, ip]
         L.mpg_learned_train_records.argtypes = [vp, ip, C.c_float, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.mpg_learned_loss.argtypes = [vp, ip]
         _lib = L
     return _lib
 
@@ -159,6 +161,10 @@ class Solver:
 
     def laplc(self, press: int, alap: int, impfl: int) -> None:
         _check(self.L.mpg_laplc(self.h, press, alap, impfl))
+
+    def laplc_adjoint(self, y: int, out: int, impfl: int) -> None:
+        """Adjoint of laplc in the vol*rh0-weighted inner product."""
+        _check(self.L.mpg_laplc_adjoint(self.h, y, out, impfl))
 
     def prfr(self, press, ustr, vstr, wstr, uout, vout, wout, impfl) -> None:
         _check(self.L.mpg_prfr(self.h, press, ustr, vstr, wstr, uout, vout, wout, impfl))
@@ -234,6 +240,10 @@ class Solver:
         loss = C.c_double()
         _check(self.L.mpg_learned_train_pair(self.h, r, t, lr, C.byref(loss)))
         return loss.value
+
+    def learned_loss(self, mode: int) -> None:
+        """0: residual norm ||A q - r||_W (default), 1: regression on the scaled error."""
+        _check(self.L.mpg_learned_loss(self.h, mode))
 
     def learned_harvest(self, every: int, max_records: int) -> None:
         _check(self.L.mpg_learned_harvest(self.h, every, max_records))

@@ -31,6 +31,7 @@ class MpgParams(C.Structure):
         ("implgw", C.c_int32), ("lipps", C.c_int32),
         ("strat", C.c_double), ("tetbar", C.c_double), ("g", C.c_double),
         ("iprc", C.c_int32), ("nscal", C.c_int32), ("precision", C.c_int32), ("itmn", C.c_int32),
+        ("nn_rate", C.c_double),
     ]
 
 
@@ -53,7 +54,7 @@ class MpgGcrStats(C.Structure):
     _fields_ = [
         ("niter", C.c_int32), ("nitsm", C.c_int32), ("icount", C.c_int32), ("status", C.c_int32),
         ("eer", C.c_double), ("eem", C.c_double), ("dvmx", C.c_double), ("rl2", C.c_double),
-        ("fallbacks", C.c_int32), ("pad", C.c_int32),
+        ("fallbacks", C.c_int32), ("pad", C.c_int32), ("rate", C.c_double),
     ]
 
     def as_dict(self):
@@ -68,6 +69,7 @@ class MpgDiag(C.Structure):
         ("eer", C.c_double), ("eem", C.c_double),
         ("stats", C.c_double * 16), ("mass", C.c_double * 8),
         ("smin", C.c_double * 4), ("smax", C.c_double * 4),
+        ("rate1", C.c_double), ("fallbacks", C.c_int32), ("pad", C.c_int32),
     ]
 
     def as_dict(self):
@@ -145,6 +147,7 @@ class RunParams:
     nscal: int = 0
     precision: int = 0
     itmn: int = 3
+    nn_rate: float = 0.0
 
     def to_c(self) -> MpgParams:
         p = MpgParams()

@@ -76,7 +76,7 @@ struct mpg_solver {
     float *psi1f = nullptr, *g3f[3] = {}, *mxf = nullptr, *mnf = nullptr;
     // /itero/
     int32_t niter = 0, nitsm = 0, icount = 0, gstatus = 0, last_fallbacks = 0;
-    double eer = 0., eem = 0., dvmx_last = 0., rl2_last = 0.;
+    double eer = 0., eem = 0., dvmx_last = 0., rl2_last = 0., rate_last = 0.;
     double betaunstr1 = 0.;
     HostStatic hs;
     std::vector<int32_t> iperm;
@@ -97,6 +97,10 @@ struct mpg_solver {
         int every = 0, maxrec = 0, nrec = 0, solve_first = 0;
         double *rec_r = nullptr, *rec_t = nullptr;
         int fallbacks = 0;
+        // residual-norm training: q, e = A q - r and A^T W e (FP64)
+        int loss_mode = MPG_NN_LOSS_RESIDUAL;
+        double *qd = nullptr, *ed = nullptr, *dq = nullptr;
+        int *err = nullptr;          // set by the tensor-core layer when its wait gave up
     } nn;
 };
 
@@ -171,17 +175,6 @@ int upload(mpg_handle h, T **p, const std::vector<T> &v) {
 
 inline int grid(int n) { return (n + kThreads - 1) / kThreads; }
 
-// launch a column-gather kernel template with the level-chunk count of the mesh
-#define COLL(kern, ...)                                                                      \
-    do {                                                                                     \
-        const dim3 g_((h->NC + kColWarps - 1) / kColWarps), b_(kColThreads);                 \
-        switch (h->kch) {                                                                    \
-            case 1: kern<1><<<g_, b_, 0, h->st>>>(__VA_ARGS__); break;                        \
-            case 2: kern<2><<<g_, b_, 0, h->st>>>(__VA_ARGS__); break;                        \
-            case 3: kern<3><<<g_, b_, 0, h->st>>>(__VA_ARGS__); break;                        \
-            default: kern<4><<<g_, b_, 0, h->st>>>(__VA_ARGS__); break;                       \
-        }                                                                                    \
-    } while (0)
 
 // field pointer, allocated (zeroed) on first use
 double *fld(mpg_handle h, int fid) {
@@ -243,9 +236,37 @@ template <> struct Buf<float> {
     static const float *coefw(mpg_handle h) { return h->coefwf; }
 };
 
+#ifndef MPG_LAP_CW
+#define MPG_LAP_CW 0
+#endif
+template <class T, int NS>
+void launch_laplc_cw(mpg_handle h, const T *p, T *alap, int impfl) {
+    using B = Buf<T>;
+    const int nb = (h->NC + kCWWarps - 1) / kCWWarps;
+    {
+        KTIME(KT_LAP_GRAD);
+        k_lap_grad_cw<T, NS><<<nb, 32 * kCWWarps, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
+                                                              (T)h->P.delt, impfl, B::F(h, 0), B::F(h, 1), B::F(h, 2));
+    }
+    {
+        KTIME(KT_LAP_DIV);
+        k_lap_div_cw<T, NS><<<nb, 32 * kCWWarps, 0, h->st>>>(h->M, B::F(h, 0), B::F(h, 1), B::F(h, 2), B::vol(h),
+                                                             B::rh0(h), alap);
+    }
+}
+
 template <class T>
 int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
     using B = Buf<T>;
+    if (MPG_LAP_CW && h->kch <= 4) {
+        switch (h->kch) {
+            case 1: launch_laplc_cw<T, 1>(h, p, alap, impfl); break;
+            case 2: launch_laplc_cw<T, 2>(h, p, alap, impfl); break;
+            case 3: launch_laplc_cw<T, 3>(h, p, alap, impfl); break;
+            default: launch_laplc_cw<T, 4>(h, p, alap, impfl); break;
+        }
+        return check_launch("laplc");
+    }
     {
         KTIME(KT_LAP_GRAD);
         k_lap_grad<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
@@ -259,6 +280,18 @@ int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
     return check_launch("laplc");
 }
 int op_laplc(mpg_handle h, const double *p, double *alap, int impfl) { return op_laplc_t<double>(h, p, alap, impfl); }
+
+// A^T W y (divw = false) or the W-adjoint W^{-1} A^T W y (divw = true), W = vol*rh0, A = laplc
+int op_laplc_adj(mpg_handle h, const double *y, double *out, int impfl, bool divw) {
+    {
+        KTIME(KT_MISC);
+        k_lapT_grad<<<grid(h->N), kThreads, 0, h->st>>>(h->M, y, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW],
+                                                        h->P.delt, impfl, h->F[0], h->F[1], h->F[2]);
+        k_lapT_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, h->F[0], h->F[1], h->F[2], h->vol, h->f[MPG_F_RH0],
+                                                       divw ? 1 : 0, out);
+    }
+    return check_launch("laplc adjoint");
+}
 
 int op_prfr(mpg_handle h, const double *p, const double *us, const double *vs, const double *ws, double *uo,
             double *vo, double *wo, int impfl) {
@@ -435,7 +468,7 @@ int nn_alloc_infer(mpg_handle h) {
         const size_t n = h->N;
         if ((rc = dalloc(h, &S.prm, nn::NPARAM)) || (rc = dalloc(h, &S.Wbf, (size_t)nn::NL * nn::C * nn::K3)) ||
             (rc = dalloc(h, &S.H[0], n * nn::C)) || (rc = dalloc(h, &S.H[1], n * nn::C)) ||
-            (rc = dalloc(h, &S.z, n)) || (rc = dalloc(h, &S.sc, 4)))
+            (rc = dalloc(h, &S.z, n)) || (rc = dalloc(h, &S.sc, 4)) || (rc = dalloc(h, &S.err, 1)))
             return rc;
         S.infer = true;
     }
@@ -455,7 +488,8 @@ int nn_alloc_train(mpg_handle h) {
         (rc = dalloc(h, &S.H[3], n * nn::C)) || (rc = dalloc(h, &S.X0, n * nn::FIN)) ||
         (rc = dalloc(h, &S.dH, n * nn::C)) || (rc = dalloc(h, &S.dH2, n * nn::C)) ||
         (rc = dalloc(h, &S.G0, n * nn::C)) || (rc = dalloc(h, &S.Gh, n * nn::C)) ||
-        (rc = dalloc(h, &S.Gv, n * nn::C)) || (rc = dalloc(h, &S.Y, n)) || (rc = dalloc(h, &S.dU, np * nn::C)))
+        (rc = dalloc(h, &S.Gv, n * nn::C)) || (rc = dalloc(h, &S.Y, n)) || (rc = dalloc(h, &S.dU, np * nn::C)) ||
+        (rc = dalloc(h, &S.qd, n)) || (rc = dalloc(h, &S.ed, n)) || (rc = dalloc(h, &S.dq, n)))
         return rc;
     for (int l = 0; l < 3; ++l)
         if ((rc = dalloc(h, &S.Xs[l], np * nn::K3))) return rc;
@@ -481,13 +515,13 @@ int nn_forward(mpg_handle h, const double *r, T *q, int impfl, bool train) {
     {
         KTIME(KT_NN);
         nn::k_nn_input<<<grid(N), kThreads, 0, h->st>>>(N, r, S.z, S.sc, G, S.prm, S.H[0], train ? S.X0 : nullptr);
-        const int ntiles = (N + nn::TILE - 1) / nn::TILE;
-        const int nblk = std::min((ntiles + nn::WARPS - 1) / nn::WARPS, 148 * 16);
+        const int ntiles = (N + nn::TCM - 1) / nn::TCM;
+        const int nblk = std::min(ntiles, 148 * 3);
         for (int l = 0; l < nn::NL; ++l) {
             __nv_bfloat16 *Hout = train ? S.H[l + 1] : S.H[(l + 1) & 1];
-            nn::k_nn_layer<<<nblk, 32 * nn::WARPS, 0, h->st>>>(h->M, G, Hin, S.Wbf + (size_t)l * nn::C * nn::K3,
-                                                               S.prm + nn::OFF_L0 + l * nn::LSTRIDE + nn::C * nn::K3,
-                                                               Hout, train ? S.Xs[l] : nullptr);
+            nn::k_nn_layer_tc<<<nblk, nn::TC_THREADS, 0, h->st>>>(h->M, G, Hin, S.Wbf + (size_t)l * nn::C * nn::K3,
+                                                                  S.prm + nn::OFF_L0 + l * nn::LSTRIDE + nn::C * nn::K3,
+                                                                  Hout, train ? S.Xs[l] : nullptr, S.err);
             Hin = Hout;
         }
         double *qd = nullptr;
@@ -498,20 +532,21 @@ int nn_forward(mpg_handle h, const double *r, T *q, int impfl, bool train) {
     return check_launch("nn forward");
 }
 
-// backward pass for target t (after nn_forward with train = true): gradient into S.grad, loss
-int nn_backward(mpg_handle h, const double *t, double *loss) {
+// backward pass (after nn_forward with train = true): gradient into S.grad and the loss.  Either
+// for target t (error loss) or from dL/dq = dq * sc[2] (residual loss, loss already in sc[1]).
+int nn_backward(mpg_handle h, const double *t, const double *dq, double *loss) {
     auto &S = h->nn;
     const int N = h->N;
     const nn::Geom G = nn_geom(h);
     const int nb = (N + 255) / 256;
     {
         KTIME(KT_NN);
-        nn::k_nn_out_bwd<<<nb, 256, 0, h->st>>>(N, S.H[3], S.Y, t, S.z, S.sc, G, S.prm, S.dH, S.pd);
+        nn::k_nn_out_bwd<<<nb, 256, 0, h->st>>>(N, S.H[3], S.Y, t, dq, S.z, S.sc, G, S.prm, S.dH, S.pd);
         // partial columns: dw_out (C), db_out, loss
         nn::k_nn_fold_d<<<1, 64, 0, h->st>>>(nb, nn::C + 2, nn::C + 1, S.pd, S.grad + nn::OFF_WOUT);
     }
     double *dl = S.sc + 1;
-    {
+    if (!dq) {
         KTIME(KT_NN);
         // sum of the per-block loss partials (column C+1) in fixed order
         const double *pdp = S.pd;
@@ -559,6 +594,58 @@ int nn_adam(mpg_handle h, float lr) {
         nn::k_nn_to_bf16<<<(nn::NL * nn::C * nn::K3 + 255) / 256, 256, 0, h->st>>>(S.prm, S.Wbf);
     }
     return check_launch("nn adam");
+}
+
+// Residual loss of a preconditioner output q: the residual left by the best GCR step along q,
+// L = 0.5 min_alpha ||r - alpha A q||_W^2 / ||r||_W^2 = 0.5 (1 - <Aq,r>_W^2 / (||Aq||_W^2 ||r||_W^2)).
+// It does not depend on the scale of q, as GCR does not.  With a = A q, alpha = <a,r>/<a,a> and
+// e = alpha a - r, dL/dq = (alpha / ||r||^2) A^T W e (alpha is optimal, so its own variation drops).
+// Reduction: v = (<a,r>_W, <a,a>_W, <r,r>_W) -> sc[1] = L, sc[2] = alpha/||r||^2, sc[3] = alpha.
+struct ProdWLoss {
+    const double *a, *r, *vol, *rh0;
+    __device__ void operator()(int n, double *v) const {
+        const double w = vol[n] * rh0[n];
+        v[0] = w * a[n] * r[n];
+        v[1] = w * a[n] * a[n];
+        v[2] = w * r[n] * r[n];
+    }
+};
+struct FinWLoss {
+    double *sc;
+    __device__ void operator()(const double *v) const {
+        const double aa = v[1] > 0. ? v[1] : 1., rr = v[2] > 0. ? v[2] : 1.;
+        const double alpha = v[0] / aa;
+        const double c2 = v[0] * v[0] / (aa * rr);
+        sc[1] = 0.5 * (1. - (c2 < 1. ? c2 : 1.));
+        sc[2] = alpha / rr;
+        sc[3] = alpha;
+    }
+};
+// e = sc[3] a - r
+__global__ void k_step_residual(int N, const double *__restrict__ sc, const double *__restrict__ a,
+                                const double *__restrict__ r, double *__restrict__ e) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < N) e[n] = sc[3] * a[n] - r[n];
+}
+
+// loss and gradient for residual r (and target t for the error loss) with the selected loss
+int nn_grad(mpg_handle h, const double *r, const double *t, double *loss) {
+    auto &S = h->nn;
+    int rc;
+    if (S.loss_mode == MPG_NN_LOSS_ERROR) {
+        if ((rc = nn_forward<double>(h, r, h->tres, 1, true))) return rc;
+        return nn_backward(h, t, nullptr, loss);
+    }
+    // residual loss: q = net(r), a = A q, e = alpha a - r, dL/dq = (alpha/||r||^2) A^T W e
+    if ((rc = nn_forward<double>(h, r, S.qd, 1, true))) return rc;
+    if ((rc = op_laplc(h, S.qd, S.ed, 1))) return rc;
+    if ((rc = reduce<3>(h, 0u, ProdWLoss{S.ed, r, h->vol, h->f[MPG_F_RH0]}, FinWLoss{S.sc}))) return rc;
+    {
+        KTIME(KT_NN);
+        k_step_residual<<<grid(h->N), kThreads, 0, h->st>>>(h->N, S.sc, S.ed, r, S.ed);
+    }
+    if ((rc = op_laplc_adj(h, S.ed, S.dq, 1, false))) return rc;
+    return nn_backward(h, nullptr, S.dq, loss);
 }
 
 // learned preconditioner inside gcrk; returns 1 in *fell_back when it handed over to the plain one
@@ -796,6 +883,10 @@ int op_gcrk_t(mpg_handle h, double *p, const double *u1, const double *v1, const
     if ((rc = reduce<3>(h, 0x2u, ProdNorm0<T>{B::qr(h), h->r}, FinEps{h->scal}))) return rc;
     if ((rc = fetch_result(h, 3))) return rc;
     double rl20 = h->h_res[2] > epa ? h->h_res[2] : epa;
+    const double rl2_init = rl20;
+    // learned preconditioner: kept while ||r||_2 after m updates is <= nn_rate^m of its start
+    const double nn_rate = P.nn_rate > 0. ? P.nn_rate : 0.98;
+    int nupd = 0;
     {
         KTIME(KT_MISC);
         k_copy<T, T><<<grid(N), kThreads, 0, h->st>>>(N, B::qr(h), B::x(h, 0));
@@ -812,8 +903,13 @@ int op_gcrk_t(mpg_handle h, double *p, const double *u1, const double *v1, const
             if ((rc = fetch_result(h, 2))) return rc;
             dvmx = h->h_res[0] > -1.e15 ? h->h_res[0] : -1.e15;
             rl2 = h->h_res[1];
+            ++nupd;
             if (!std::isfinite(dvmx) || !std::isfinite(rl2)) { status = MPG_GCR_NAN; break; }
             if (dvmx <= eps && it >= itmn) { status = MPG_GCR_CONVERGED; break; }
+            if (learned && lon && nupd >= lord && std::sqrt(rl2 / rl2_init) > std::pow(nn_rate, (double)nupd)) {
+                lon = false;                  // slower than the required contraction: plain from here on
+                ++fallbacks;
+            }
             if (rl2 >= rl20) {
                 if (!(learned && lon)) { status = MPG_GCR_STALLED; break; }
                 lon = false;                  // no progress with the network: plain from here on
@@ -845,6 +941,7 @@ int op_gcrk_t(mpg_handle h, double *p, const double *u1, const double *v1, const
         }
     }
     h->last_fallbacks = fallbacks;
+    h->rate_last = (nupd > 0 && rl2 > 0. && std::isfinite(rl2)) ? std::pow(rl2 / rl2_init, 0.5 / nupd) : 0.;
     if ((rc = reduce<2>(h, 0x2u, ProdQ<T>{B::qr(h)}, NoFin{}))) return rc;
     if ((rc = fetch_result(h, 2))) return rc;
     double eer = h->h_res[0], eem = h->h_res[1] > -1.e15 ? h->h_res[1] : -1.e15;
@@ -1314,6 +1411,14 @@ extern "C" int mpg_laplc(mpg_handle h, int press, int alap, int impfl) {
     return op_laplc(h, a, b, impfl);
 }
 
+extern "C" int mpg_laplc_adjoint(mpg_handle h, int y, int out, int impfl) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    FLD(yy, y);
+    FLD(oo, out);
+    if (yy == oo) return mpg_fail(MPG_ERR_ARG, "laplc_adjoint: y and out must differ");
+    return op_laplc_adj(h, yy, oo, impfl, true);
+}
+
 extern "C" int mpg_prfr(mpg_handle h, int press, int ustr, int vstr, int wstr, int uout, int vout, int wout,
                         int impfl) {
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
@@ -1356,6 +1461,7 @@ static void fill_stats(mpg_handle h, mpg_gcr_stats *st) {
     st->niter = h->niter; st->nitsm = h->nitsm; st->icount = h->icount; st->status = h->gstatus;
     st->eer = h->eer; st->eem = h->eem; st->dvmx = h->dvmx_last; st->rl2 = h->rl2_last;
     st->fallbacks = h->last_fallbacks;
+    st->rate = h->rate_last;
 }
 
 extern "C" int mpg_gcrk(mpg_handle h, int p, int u1, int v1, int w1, int u2, int v2, int w2, int impfl,
@@ -1507,7 +1613,8 @@ extern "C" int mpg_step(mpg_handle h, mpg_diag *diag) {
         if ((rc = op_mpdata_field(h, psi))) return rc;
     }
     double *prpot = fld(h, MPG_F_PRPOT);
-    int niter1 = 0;
+    int niter1 = 0, fallbacks = 0;
+    double rate1 = 0.;
     for (int mtri = 1; mtri <= 2; ++mtri) {
         if ((rc = mpg_explicit_forcing(h, mtri))) return rc;
         const int imp = h->P.implgw;
@@ -1519,12 +1626,17 @@ extern "C" int mpg_step(mpg_handle h, mpg_diag *diag) {
             if ((rc = op_prfr(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.uuu[0], F.uuu[1], F.uuu[2], imp)))
                 return rc;
         }
-        if (mtri == 1) niter1 = h->niter;
+        if (mtri == 1) { niter1 = h->niter; rate1 = h->rate_last; }
+        fallbacks += h->last_fallbacks;
         if ((rc = mpg_post_solve(h, mtri))) return rc;
     }
     if ((rc = mpg_extrapolate(h))) return rc;
     if ((rc = step_diag(h, diag))) return rc;
-    if (diag) diag->niter1 = niter1;
+    if (diag) {
+        diag->niter1 = niter1;
+        diag->rate1 = rate1;
+        diag->fallbacks = fallbacks;
+    }
     return MPG_OK;
 }
 
@@ -1693,12 +1805,18 @@ extern "C" int mpg_learned_grad(mpg_handle h, int r, int t, float *grad, double 
     FLD(tt, t);
     int rc = nn_alloc_train(h);
     if (rc) return rc;
-    if ((rc = nn_forward<double>(h, rr, h->tres, 1, true))) return rc;
-    if ((rc = nn_backward(h, tt, loss))) return rc;
+    if ((rc = nn_grad(h, rr, tt, loss))) return rc;
     if (grad) {
         MPG_CUDA(cudaMemcpyAsync(grad, h->nn.grad, sizeof(float) * nn::NPARAM, cudaMemcpyDeviceToHost, h->st));
         MPG_CUDA(cudaStreamSynchronize(h->st));
     }
+    return MPG_OK;
+}
+
+extern "C" int mpg_learned_loss(mpg_handle h, int mode) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    if (mode != MPG_NN_LOSS_RESIDUAL && mode != MPG_NN_LOSS_ERROR) return mpg_fail(MPG_ERR_ARG, "unknown loss mode");
+    h->nn.loss_mode = mode;
     return MPG_OK;
 }
 
@@ -1736,8 +1854,7 @@ extern "C" int mpg_learned_train_records(mpg_handle h, int epochs, float lr, dou
         for (int j = 0; j < S.nrec; ++j) {
             double l = 0.;
             const double *rj = S.rec_r + (size_t)j * h->N, *tj = S.rec_t + (size_t)j * h->N;
-            if ((rc = nn_forward<double>(h, rj, h->tres, 1, true))) return rc;
-            if ((rc = nn_backward(h, tj, &l))) return rc;
+            if ((rc = nn_grad(h, rj, tj, &l))) return rc;
             if ((rc = nn_adam(h, lr))) return rc;
             sum += l;
         }

@@ -51,7 +51,10 @@ __device__ __forceinline__ Face decode_face(int2 en, int n, int k, int L) {
     return f;
 }
 
-template <int U = 2, class LD, class AC>
+#ifndef MPG_GATHER_U
+#define MPG_GATHER_U 2
+#endif
+template <int U = MPG_GATHER_U, class LD, class AC>
 __device__ __forceinline__ void for_faces(const ColMesh &M, int c, int k, int n, LD &&load, AC &&acc) {
     const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
     const int L = M.L;
@@ -102,8 +105,11 @@ using V4 = V4T<double>;
 using V6 = V6T<double>;
 
 // derivative (ref.f:3943-4022) of phi for the three components at once:
-// g_d = sum over faces of (+/-) S_d * ((phi_n + phi_j) * 0.5)
-template <class T>
+// g_d = sum over faces of (+/-) S_d * ((phi_n + phi_j) * 0.5).
+// With DIFF the transpose of that matrix is applied instead: since the other end of a face
+// carries the opposite sign, (B_d^T y)_n = sum over faces of (+/-) S_d * ((y_n - y_j) * 0.5),
+// plus the same closure term.
+template <class T, bool DIFF = false>
 __device__ __forceinline__ void grad3(const ColMesh &M, const T *__restrict__ phi, int c, int k, int n,
                                       T &gx, T &gy, T &gz) {
     const T pn = phi[n];
@@ -114,7 +120,7 @@ __device__ __forceinline__ void grad3(const ColMesh &M, const T *__restrict__ ph
                           __ldg(SPick<T>::get(M, 2, f.vert) + f.si), phi[f.j]};
         },
         [&](const Face &f, const V4T<T> &v) {
-            const T u = (pn + v.d) * T(0.5);
+            const T u = (DIFF ? pn - v.d : pn + v.d) * T(0.5);
             const T tx = v.a * u, ty = v.b * u, tz = v.c * u;
             if (f.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
             else       { ax = ax + tx; ay = ay + ty; az = az + tz; }
@@ -129,8 +135,9 @@ __device__ __forceinline__ void grad3(const ColMesh &M, const T *__restrict__ ph
     gx = ax; gy = ay; gz = az;
 }
 
-// derivative(fx,1), derivative(fy,2), derivative(fz,3) of three fields (the divergence)
-template <class T, class FX>
+// derivative(fx,1), derivative(fy,2), derivative(fz,3) of three fields (the divergence);
+// with DIFF the transposed matrices, as in grad3
+template <class T, bool DIFF = false, class FX>
 __device__ __forceinline__ void div3(const ColMesh &M, FX f, int c, int k, int n, T &dx, T &dy, T &dz) {
     T fnx, fny, fnz;
     f(n, fnx, fny, fnz);
@@ -145,9 +152,9 @@ __device__ __forceinline__ void div3(const ColMesh &M, FX f, int c, int k, int n
             return v;
         },
         [&](const Face &fc, const V6T<T> &v) {
-            const T tx = v.a * ((fnx + v.d) * T(0.5));
-            const T ty = v.b * ((fny + v.e) * T(0.5));
-            const T tz = v.c * ((fnz + v.f) * T(0.5));
+            const T tx = v.a * ((DIFF ? fnx - v.d : fnx + v.d) * T(0.5));
+            const T ty = v.b * ((DIFF ? fny - v.e : fny + v.e) * T(0.5));
+            const T tz = v.c * ((DIFF ? fnz - v.f : fnz + v.f) * T(0.5));
             if (fc.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
             else        { ax = ax + tx; ay = ay + ty; az = az + tz; }
         });
@@ -179,9 +186,39 @@ __device__ __forceinline__ void bcv_node(const ColMesh &M, int c, int k, int n, 
     });
 }
 
+// transpose of bcv_node with flag = 0: the same symmetric projections (and zeroed u at
+// types 7/8), visited in reverse order
+template <class T>
+__device__ __forceinline__ void bcv_node_adj(const ColMesh &M, int c, int k, T &u, T &v, T &w) {
+    const bool per = (M.iper == 2);
+    const int beg = __ldg(&M.bptr[c]), end = __ldg(&M.bptr[c + 1]);
+    for (int b = end - 1; b >= beg; --b) {
+        const BEntry &be = M.bent[b];
+        if (be.k != k) continue;
+        const int t = be.type;
+        if (!per && (t == 7 || t == 8)) u = T(0);
+        if (t == 11 || (!per && (t == 5 || t == 6))) {
+            const T a0 = T(be.anp[0]), a1 = T(be.anp[1]), a2 = T(be.anp[2]);
+            const T vn = u * a0 + v * a1 + w * a2;
+            u = u - a0 * vn;
+            v = v - a1 * vn;
+            w = w - a2 * vn;
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------ operators
 // latency-bound gathers that fit 40 registers without spilling: keep 6 blocks (48 warps) per SM
-#define GATHER_BOUNDS __launch_bounds__(kThreads, 6)
+#ifndef MPG_GATHER_MINB
+#define MPG_GATHER_MINB 6
+#endif
+#define GATHER_BOUNDS __launch_bounds__(kThreads, MPG_GATHER_MINB)
+// the divergence gathers load six values per face
+#ifdef MPG_DIV_MINB
+#define DIV_BOUNDS __launch_bounds__(kThreads, MPG_DIV_MINB)
+#else
+#define DIV_BOUNDS
+#endif
 
 #define NODE_BEGIN                                                            \
     const int n = blockIdx.x * blockDim.x + threadIdx.x;                      \
@@ -227,13 +264,196 @@ __global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const T *__restrict__ p, con
 
 // laplc second half (ref.f:1339-1350): alap = (Dx(Fx) + Dy(Fy) + Dz(Fz)) / (vol*rh0)
 template <class T>
-__global__ void k_lap_div(ColMesh M, const T *__restrict__ Fx, const T *__restrict__ Fy,
+__global__ void DIV_BOUNDS k_lap_div(ColMesh M, const T *__restrict__ Fx, const T *__restrict__ Fy,
                           const T *__restrict__ Fz, const T *__restrict__ vol,
                           const T *__restrict__ rh0, T *__restrict__ alap) {
     NODE_BEGIN
     T dx, dy, dz;
     div3<T>(M, [&](int j, T &a, T &b, T &d) { a = Fx[j]; b = Fy[j]; d = Fz[j]; }, c, k, n, dx, dy, dz);
     alap[n] = (dx + dy + dz) / (vol[n] * rh0[n]);
+}
+
+// ------------------------------------------------------------------------------ column-warp laplc
+// The same two halves of laplc with one warp per column: lane l holds levels l, l+32, ... (NS
+// slots).  The warp walks its column's adjacency list once (uniform branches, one broadcast load
+// per entry) and loads a face's operands for all NS slots before accumulating any, so a thread
+// has 4*NS (divergence: 6*NS) independent loads in flight per face where a node-per-thread
+// gather has 4 (6) behind each adjacency load.  Every node adds its terms in the same order as
+// k_lap_grad/k_lap_div, so the results are bit-identical to them.
+constexpr int kCWWarps = 8;
+
+template <class T, int NS>
+__global__ void __launch_bounds__(32 * kCWWarps)
+k_lap_grad_cw(ColMesh M, const T *__restrict__ p, const T *__restrict__ vol, const T *__restrict__ rh0,
+              const T *__restrict__ coefw, const double *__restrict__ ue, T dt, int impfl,
+              T *__restrict__ Fx, T *__restrict__ Fy, T *__restrict__ Fz) {
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kCWWarps + (threadIdx.x >> 5);
+    if (c >= M.NC) return;
+    const int L = M.L, base = c * L;
+    T pn[NS], ax[NS], ay[NS], az[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int k = lane + 32 * s;
+        pn[s] = k < L ? p[base + k] : T(0);
+        ax[s] = T(0); ay[s] = T(0); az[s] = T(0);
+    }
+    const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
+    const T *Sh0 = SPick<T>::get(M, 0, false), *Sh1 = SPick<T>::get(M, 1, false), *Sh2 = SPick<T>::get(M, 2, false);
+    const T *Sv0 = SPick<T>::get(M, 0, true), *Sv1 = SPick<T>::get(M, 1, true), *Sv2 = SPick<T>::get(M, 2, true);
+    for (int j = beg; j < end; ++j) {
+        const int2 en = __ldg(&M.cadj[j]);
+        const bool vert = en.x < 0, below = en.x == MPG_ADJ_BELOW;
+        const bool sub = vert ? below : ((en.x & 1) != 0);
+        T sx[NS], sy[NS], sz[NS], pj[NS];
+        bool ok[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int k = lane + 32 * s;
+            const int n = base + k;
+            ok[s] = k < L && (!vert || (below ? k > 0 : k + 1 < L));
+            const int si = vert ? (below ? n - 1 : n) : (en.x >> 1) * L + k;
+            const int jj = vert ? (below ? n - 1 : n + 1) : en.y * L + k;
+            if (ok[s]) {
+                sx[s] = __ldg((vert ? Sv0 : Sh0) + si);
+                sy[s] = __ldg((vert ? Sv1 : Sh1) + si);
+                sz[s] = __ldg((vert ? Sv2 : Sh2) + si);
+                pj[s] = p[jj];
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            if (!ok[s]) continue;
+            const T u = (pn[s] + pj[s]) * T(0.5);
+            const T tx = sx[s] * u, ty = sy[s] * u, tz = sz[s] * u;
+            if (sub) { ax[s] = ax[s] - tx; ay[s] = ay[s] - ty; az[s] = az[s] - tz; }
+            else     { ax[s] = ax[s] + tx; ay[s] = ay[s] + ty; az[s] = az[s] + tz; }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int k = lane + 32 * s;
+        if (k >= L) continue;
+        const int n = base + k;
+        T gx = ax[s], gy = ay[s], gz = az[s];
+        if (M.iper == 0) {
+            for_boundary(M, c, k, [&](const BEntry &be) {
+                gx = gx + T(be.sbb[0]) * pn[s];
+                gy = gy + T(be.sbb[1]) * pn[s];
+                gz = gz + T(be.sbb[2]) * pn[s];
+            });
+        }
+        const T v = vol[n];
+        T dx = dt * gx / v, dy = dt * gy / v, dz = dt * gz / v;
+        dx = T(0.5) * dx / T(1.0);
+        dy = T(0.5) * dy / T(1.0);
+        dz = T(0.5) * dz * (coefw[n] * (T)impfl + (T)(1 - impfl));
+        bcv_node<T>(M, c, k, n, ue, 0.0, dx, dy, dz);
+        const T r = rh0[n];
+        Fx[n] = dx * r; Fy[n] = dy * r; Fz[n] = dz * r;
+    }
+}
+
+template <class T, int NS>
+__global__ void __launch_bounds__(32 * kCWWarps)
+k_lap_div_cw(ColMesh M, const T *__restrict__ Fx, const T *__restrict__ Fy, const T *__restrict__ Fz,
+             const T *__restrict__ vol, const T *__restrict__ rh0, T *__restrict__ alap) {
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kCWWarps + (threadIdx.x >> 5);
+    if (c >= M.NC) return;
+    const int L = M.L, base = c * L;
+    T fx[NS], fy[NS], fz[NS], ax[NS], ay[NS], az[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int k = lane + 32 * s;
+        const bool in = k < L;
+        fx[s] = in ? Fx[base + k] : T(0);
+        fy[s] = in ? Fy[base + k] : T(0);
+        fz[s] = in ? Fz[base + k] : T(0);
+        ax[s] = T(0); ay[s] = T(0); az[s] = T(0);
+    }
+    const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
+    const T *Sh0 = SPick<T>::get(M, 0, false), *Sh1 = SPick<T>::get(M, 1, false), *Sh2 = SPick<T>::get(M, 2, false);
+    const T *Sv0 = SPick<T>::get(M, 0, true), *Sv1 = SPick<T>::get(M, 1, true), *Sv2 = SPick<T>::get(M, 2, true);
+    for (int j = beg; j < end; ++j) {
+        const int2 en = __ldg(&M.cadj[j]);
+        const bool vert = en.x < 0, below = en.x == MPG_ADJ_BELOW;
+        const bool sub = vert ? below : ((en.x & 1) != 0);
+        T sx[NS], sy[NS], sz[NS], gx[NS], gy[NS], gz[NS];
+        bool ok[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int k = lane + 32 * s;
+            const int n = base + k;
+            ok[s] = k < L && (!vert || (below ? k > 0 : k + 1 < L));
+            const int si = vert ? (below ? n - 1 : n) : (en.x >> 1) * L + k;
+            const int jj = vert ? (below ? n - 1 : n + 1) : en.y * L + k;
+            if (ok[s]) {
+                sx[s] = __ldg((vert ? Sv0 : Sh0) + si);
+                sy[s] = __ldg((vert ? Sv1 : Sh1) + si);
+                sz[s] = __ldg((vert ? Sv2 : Sh2) + si);
+                gx[s] = Fx[jj];
+                gy[s] = Fy[jj];
+                gz[s] = Fz[jj];
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            if (!ok[s]) continue;
+            const T tx = sx[s] * ((fx[s] + gx[s]) * T(0.5));
+            const T ty = sy[s] * ((fy[s] + gy[s]) * T(0.5));
+            const T tz = sz[s] * ((fz[s] + gz[s]) * T(0.5));
+            if (sub) { ax[s] = ax[s] - tx; ay[s] = ay[s] - ty; az[s] = az[s] - tz; }
+            else     { ax[s] = ax[s] + tx; ay[s] = ay[s] + ty; az[s] = az[s] + tz; }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int k = lane + 32 * s;
+        if (k >= L) continue;
+        const int n = base + k;
+        T dx = ax[s], dy = ay[s], dz = az[s];
+        if (M.iper == 0) {
+            for_boundary(M, c, k, [&](const BEntry &be) {
+                dx = dx + T(be.sbb[0]) * fx[s];
+                dy = dy + T(be.sbb[1]) * fy[s];
+                dz = dz + T(be.sbb[2]) * fz[s];
+            });
+        }
+        alap[n] = (dx + dy + dz) / (vol[n] * rh0[n]);
+    }
+}
+
+// Adjoint of laplc in the inner product weighted by W = vol*rh0.  laplc is
+// A = diag(1/W) sum_d B_d rh0 P S1 B_d (B_d: derivative matrix of component d, S1: the dt/2,
+// coefw and 1/vol scaling, P: bcv's projections), so A^T W y = sum_d B_d^T S1 P^T rh0 B_d^T y.
+// First half: G_d = S1 P^T rh0 B_d^T y.
+__global__ void GATHER_BOUNDS k_lapT_grad(ColMesh M, const double *__restrict__ y, const double *__restrict__ vol,
+                                          const double *__restrict__ rh0, const double *__restrict__ coefw,
+                                          double dt, int impfl, double *__restrict__ Gx, double *__restrict__ Gy,
+                                          double *__restrict__ Gz) {
+    NODE_BEGIN
+    double hx, hy, hz;
+    grad3<double, true>(M, y, c, k, n, hx, hy, hz);
+    const double r = rh0[n];
+    hx = hx * r; hy = hy * r; hz = hz * r;
+    bcv_node_adj<double>(M, c, k, hx, hy, hz);
+    const double v = vol[n];
+    Gx[n] = 0.5 * dt * hx / v;
+    Gy[n] = 0.5 * dt * hy / v;
+    Gz[n] = 0.5 * dt * hz * (coefw[n] * (double)impfl + (double)(1 - impfl)) / v;
+}
+
+// Second half: out = sum_d B_d^T G_d, divided by W when divw (then <A u, y>_W = <u, out>_W).
+__global__ void k_lapT_div(ColMesh M, const double *__restrict__ Gx, const double *__restrict__ Gy,
+                           const double *__restrict__ Gz, const double *__restrict__ vol,
+                           const double *__restrict__ rh0, int divw, double *__restrict__ out) {
+    NODE_BEGIN
+    double dx, dy, dz;
+    div3<double, true>(M, [&](int j, double &a, double &b, double &d) { a = Gx[j]; b = Gy[j]; d = Gz[j]; },
+                       c, k, n, dx, dy, dz);
+    const double s = dx + dy + dz;
+    out[n] = divw ? s / (vol[n] * rh0[n]) : s;
 }
 
 // prfr (ref.f:1536-1580)
@@ -301,6 +521,7 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
         }
         __syncwarp();
         if (own) {
+#pragma unroll 8
             for (int kk = 0; kk < nk; ++kk) {
                 const int k = k0 + kk;
                 const int64_t li = line_index(c, k, L);
@@ -316,6 +537,7 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
     for (int k0 = last0; k0 >= 0; k0 -= kLineChunk) {
         const int nk = min(kLineChunk, L - k0);
         if (own) {
+#pragma unroll 8
             for (int kk = nk - 1; kk >= 0; --kk) {
                 const int k = k0 + kk;
                 const int64_t li = line_index(c, k, L);

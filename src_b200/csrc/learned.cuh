@@ -59,6 +59,7 @@ struct alignas(16) B8 { __nv_bfloat162 v[4]; };
 // what the face loops load per face (namespace-scope types: a class declared inside the
 // loading lambda came back with a wrong layout from for_faces)
 struct RowB { B8 h; float t; };
+struct RowB2 { B8 a, b; float t; };
 struct RowF { float4 lo, hi; float t; };
 
 __device__ __forceinline__ void b8_to_f(const B8 &b, float *f) {
@@ -213,6 +214,216 @@ k_nn_layer(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __nv_
     }
 }
 
+// ------------------------------------------------------------------ tcgen05 layer (forward)
+// One CTA of 256 threads takes tiles of 128 consecutive nodes.  Thread (warp w, lane l) owns node
+// row m = 32*(w%4) + l of the tile and channel half hf = w/4 (16 channels): it gathers its half of
+// the 96-wide layer input [h_n; A_h(h)_n; A_v(h)_n] and stores it to shared memory in the
+// canonical K-major layout of the tensor-core operands (8x8 BF16 core matrices of 128 contiguous
+// bytes; core (row group g, K chunk kc) at (kc*16 + g)*128 bytes), so the 32 lanes of a warp
+// write 512 contiguous bytes.  One thread then issues the 128x32x96 product X W^T as six
+// tcgen05.mma (kind::f16, BF16 operands, FP32 accumulator in tensor memory, 32 columns) and
+// commits it to an mbarrier; every thread waits, reads its row half back with tcgen05.ld
+// (warp w reads TMEM lanes 32*(w%4)..+31, columns 16*hf..+15), adds the bias, applies ReLU and
+// stores 32 bytes of BF16.
+constexpr int TCM = 128;                    // nodes per tile = TMEM lanes = UMMA M
+constexpr int TC_THREADS = 256;
+constexpr int TC_KC = K3 / 8;               // 12 K chunks of 8 channels
+constexpr uint32_t TC_A_LBO = 16 * 128;     // A: next K chunk (16 row groups of 128 B)
+constexpr uint32_t TC_B_LBO = 4 * 128;      // B: next K chunk (4 row groups)
+constexpr uint32_t TC_SBO = 128;            // next 8-row group
+constexpr uint32_t TC_TMEM_COLS = 32;
+constexpr long long TC_SPIN_MAX = 1ll << 22;  // bound on the mbarrier wait (then the output is NaN)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: canonical K-major layout without swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor: D F32, A and B BF16, both K-major, N = 32, M = 128
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(C >> 3) << 17) |
+                              ((uint32_t)(TCM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t tc_core_off(int row, int kc, int groups) {
+    return (uint32_t)((kc * groups + (row >> 3)) * 128 + (row & 7) * 16);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 3)
+k_nn_layer_tc(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __nv_bfloat16 *__restrict__ Wbf,
+              const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Hout, __nv_bfloat16 *__restrict__ Xs,
+              int *__restrict__ err) {
+    __shared__ __align__(1024) uint8_t sA[TCM * K3 * 2];      // 24 KB
+    __shared__ __align__(1024) uint8_t sB[C * K3 * 2];        // 6 KB
+    __shared__ float sBias[C];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const int m = 32 * (w & 3) + lane, hf = w >> 2;
+    // weights W [C][K3] (row n = output channel, K contiguous) -> canonical layout, 16 B per thread
+    for (int i = tid; i < C * TC_KC; i += TC_THREADS) {
+        const int n = i / TC_KC, kc = i - n * TC_KC;
+        *reinterpret_cast<uint4 *>(sB + tc_core_off(n, kc, C / 8)) =
+            *reinterpret_cast<const uint4 *>(Wbf + (size_t)n * K3 + kc * 8);
+    }
+    if (tid < C) sBias[tid] = bias[tid];
+    if (w == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_base)), "r"(TC_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
+    const int N = M.N;
+    const int ntiles = (N + TCM - 1) / TCM;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const int n = t * TCM + m;
+        // ---- gather: [h ; sum w (h_j - h)] for this thread's 16 channels
+        float ah[16], av[16];
+        B8 s0, s1;                                  // own row half, kept packed during the gather
+#pragma unroll
+        for (int i = 0; i < 16; ++i) { ah[i] = 0.f; av[i] = 0.f; }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { s0.v[i] = __floats2bfloat162_rn(0.f, 0.f); s1.v[i] = s0.v[i]; }
+        if (n < N) {
+            const int c = n / M.L, k = n - c * M.L;
+            const B8 *sp = reinterpret_cast<const B8 *>(Hin + (size_t)n * C + 16 * hf);
+            s0 = sp[0];
+            s1 = sp[1];
+            float wh = 0.f, wv = 0.f;
+            const float ih = G.iDh[n], iv = G.iDv[n];
+            for_faces(M, c, k, n,
+                [&](const Face &f) {
+                    RowB2 p;
+                    const B8 *src = reinterpret_cast<const B8 *>(Hin + (size_t)f.j * C + 16 * hf);
+                    p.a = src[0];
+                    p.b = src[1];
+                    p.t = face_T(M, G, f);
+                    return p;
+                },
+                [&](const Face &f, const RowB2 &p) {
+                    float hj[16];
+                    b8_to_f(p.a, hj);
+                    b8_to_f(p.b, hj + 8);
+                    if (f.vert) {
+                        const float wt = p.t * iv;
+                        wv += wt;
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) av[i] += wt * hj[i];
+                    } else {
+                        const float wt = p.t * ih;
+                        wh += wt;
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) ah[i] += wt * hj[i];
+                    }
+                });
+            float self[16];
+            b8_to_f(s0, self);
+            b8_to_f(s1, self + 8);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                ah[i] -= wh * self[i];
+                av[i] -= wv * self[i];
+            }
+        }
+        // ---- operand tile: chunks (self: 2hf, 2hf+1), (A_h: 4+..), (A_v: 8+..)
+#pragma unroll
+        for (int part = 0; part < 3; ++part) {
+#pragma unroll
+            for (int h2 = 0; h2 < 2; ++h2) {
+                B8 o;
+                if (part == 0) {
+                    o = h2 ? s1 : s0;
+                } else {
+                    const float *src = part == 1 ? ah : av;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        o.v[i] = __floats2bfloat162_rn(src[8 * h2 + 2 * i], src[8 * h2 + 2 * i + 1]);
+                }
+                const int kc = 4 * part + 2 * hf + h2;
+                *reinterpret_cast<B8 *>(sA + tc_core_off(m, kc, TCM / 8)) = o;
+                if (Xs && n < N) *reinterpret_cast<B8 *>(Xs + (size_t)n * K3 + 8 * kc) = o;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int s = 0; s < K3 / 16; ++s) {
+                const uint64_t ad = umma_desc(aBase + 2 * s * TC_A_LBO, TC_A_LBO, TC_SBO);
+                const uint64_t bd = umma_desc(bBase + 2 * s * TC_B_LBO, TC_B_LBO, TC_SBO);
+                const uint32_t acc = s > 0 ? 1u : 0u;
+                asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+                             :: "r"(tmem), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(smem_u32(&bar)) : "memory");
+        }
+        // ---- wait for the product (bounded)
+        {
+            uint32_t done = 0;
+            long long spins = 0;
+            while (!done) {
+                asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                             "selp.u32 %0, 1, 0, p;\n\t}\n"
+                             : "=r"(done) : "r"(smem_u32(&bar)), "r"(phase) : "memory");
+                if (!done && ++spins > TC_SPIN_MAX) break;
+            }
+            // the whole CTA leaves together if any thread gave up
+            if (__syncthreads_or(!done)) {
+                ok = false;
+                if (tid == 0) atomicExch(err, 1);
+            }
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // ---- epilogue: TMEM lanes 32*(w%4).., columns 16*hf..
+        uint32_t r[16];
+        {
+            const uint32_t taddr = tmem + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)(16 * hf);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                           "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        }
+        if (n < N) {
+            B8 o[2];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                float u0 = ok ? __uint_as_float(r[2 * i]) + sBias[16 * hf + 2 * i] : __int_as_float(0x7fc00000);
+                float u1 = ok ? __uint_as_float(r[2 * i + 1]) + sBias[16 * hf + 2 * i + 1] : __int_as_float(0x7fc00000);
+                u0 = u0 > 0.f ? u0 : (u0 == u0 ? 0.f : u0);
+                u1 = u1 > 0.f ? u1 : (u1 == u1 ? 0.f : u1);
+                o[i >> 2].v[i & 3] = __floats2bfloat162_rn(u0, u1);
+            }
+            B8 *dst = reinterpret_cast<B8 *>(Hout + (size_t)n * C + 16 * hf);
+            dst[0] = o[0];
+            dst[1] = o[1];
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (w == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_TMEM_COLS));
+}
+
 // y = w_out . h3 + b_out;  q = z + y s / |b|;  with Y != null also keeps y
 __global__ void k_nn_output(int N, const __nv_bfloat16 *__restrict__ H3, const float *__restrict__ prm,
                             const double *__restrict__ z, const double *__restrict__ sc, Geom G,
@@ -234,12 +445,14 @@ __global__ void k_nn_output(int N, const __nv_bfloat16 *__restrict__ H3, const f
 }
 
 // ---------------------------------------------------------------------------------- backward
-// loss = 0.5 * mean_n (y_n - ystar_n)^2, ystar = (t_n - z_n) |b_n| / s.  Per node: dy, the
-// gradient w.r.t. h3 (FP32 [N][C]), and block partials of dw_out, db_out and the loss.
+// Error loss (dq == null): loss = 0.5 * mean_n (y_n - ystar_n)^2, ystar = (t_n - z_n) |b_n| / s.
+// Residual loss (dq != null): dq is dL/dq up to the factor sc[2]; since q = z + y s / |b|,
+// dy = dq sc[2] s / |b|.  Per node: dy, the gradient w.r.t. h3 (FP32 [N][C]), and block
+// partials of dw_out, db_out and (error loss only) the loss.
 __global__ void __launch_bounds__(256)
 k_nn_out_bwd(int N, const __nv_bfloat16 *__restrict__ H3, const float *__restrict__ Y, const double *__restrict__ t,
-             const double *__restrict__ z, const double *__restrict__ sc, Geom G, const float *__restrict__ prm,
-             float *__restrict__ dH, double *__restrict__ part /* [gridDim][C+2] */) {
+             const double *__restrict__ dq, const double *__restrict__ z, const double *__restrict__ sc, Geom G,
+             const float *__restrict__ prm, float *__restrict__ dH, double *__restrict__ part /* [gridDim][C+2] */) {
     __shared__ double sp[256 / 32][C + 2];
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[C + 2];
@@ -247,9 +460,14 @@ k_nn_out_bwd(int N, const __nv_bfloat16 *__restrict__ H3, const float *__restric
     for (int i = 0; i < C + 2; ++i) acc[i] = 0.;
     if (n < N) {
         const double s = sc[0] > 0. ? sc[0] : 1.;
-        const double ystar = (t[n] - z[n]) * (double)G.bdiag[n] / s;
-        const double e = (double)Y[n] - ystar;
-        const double dy = e / (double)N;
+        double dy, e = 0.;
+        if (dq) {
+            dy = dq[n] * sc[2] * s / (double)G.bdiag[n];
+        } else {
+            const double ystar = (t[n] - z[n]) * (double)G.bdiag[n] / s;
+            e = (double)Y[n] - ystar;
+            dy = e / (double)N;
+        }
         float h[C];
         const B8 *src = reinterpret_cast<const B8 *>(H3 + (size_t)n * C);
 #pragma unroll

@@ -6,9 +6,13 @@ The network, its forward and backward passes and the Adam update live in the CUD
   1. run plain solves (iprc=2) with harvesting on: every `every`-th GCR iteration the library
      records the residual r_i and the iterate p_i; after the solve converges each record becomes
      the pair (r_i, p_i - p*), i.e. (residual, A^{-1} residual);
-  2. train on the recorded pairs with Adam (`epochs` passes), then keep stepping;
-  3. use the trained weights with iprc=3, where gcrk applies q = M^{-1} r + net(r) and falls back
-     to the plain line solve if the network stops making progress.
+  2. train on the recorded pairs with Adam (`epochs` passes), then keep stepping.  The default
+     loss is the residual norm ||A q - r||_W / ||r||_W of the preconditioner output q, i.e. the
+     A^T W A-norm of q's error against the pair's A^{-1} r;
+  3. use the trained weights with iprc=3, where gcrk applies q = M^{-1} r + net(r) and hands over
+     to the plain line solve if the network does not contract the residual by at least
+     `nn_rate` per iteration (the plain solves' own contraction is returned as a natural
+     choice for it).
 """
 from __future__ import annotations
 
@@ -21,25 +25,36 @@ from .cabi import F_UNK, RunParams
 
 
 def train(refmesh, params: RunParams, steps: int = 6, every: int = 4, max_records: int = 48,
-          epochs: int = 3, lr: float = 2e-3, seed: int = 0, scalar=None, device: int = 0, log=None):
-    """Harvest pairs from `steps` plain time steps and train on them; returns (weights, history)."""
+          epochs: int = 3, lr: float = 2e-3, seed: int = 0, scalar=None, device: int = 0, log=None,
+          loss: int = 0, init=None):
+    """Harvest pairs from `steps` plain time steps and train on them.
+
+    Returns (weights, history, plain_rate): plain_rate is the geometric mean over the steps of
+    the first pressure solve's per-iteration residual contraction."""
     P = RunParams(**{**params.__dict__, "iprc": 2})
     hist = []
     with Solver(P, refmesh, device=device) as s:
         s.setup()
         if scalar is not None and P.nscal:
             s.set(F_UNK + 4, scalar)
-        s.learned_init(seed)
+        if init is None:
+            s.learned_init(seed)
+        else:
+            s.learned_set_params(init)
+        s.learned_loss(loss)
         s.learned_harvest(every, max_records)
         t0 = time.time()
         for k in range(steps):
-            s.step(diag=False)
-            loss, n = s.learned_train_records(epochs, lr)
-            hist.append({"step": k, "pairs": n, "loss": loss, "t": time.time() - t0})
+            d = s.step()
+            mean_loss, n = s.learned_train_records(epochs, lr)
+            hist.append({"step": k, "pairs": n, "loss": mean_loss, "iters": (d.niter1, d.niter),
+                         "rate1": d.rate1, "t": time.time() - t0})
             if log:
                 log(hist[-1])
         s.learned_harvest(0, 0)
-        return s.learned_params(), hist
+        rates = [h["rate1"] for h in hist if h["rate1"] > 0]
+        plain_rate = float(np.exp(np.mean(np.log(rates)))) if rates else 0.0
+        return s.learned_params(), hist, plain_rate
 
 
 def compare(refmesh, params: RunParams, weights, steps: int = 5, warm: int = 2, scalar=None, device: int = 0):
@@ -61,7 +76,7 @@ def compare(refmesh, params: RunParams, weights, steps: int = 5, warm: int = 2, 
             for _ in range(steps):
                 d = s.step()
                 its.append(d.niter1 + d.niter)
-                fb += s.gcr_stats().fallbacks
+                fb += d.fallbacks
             s.synchronize()
             dt = time.perf_counter() - t0
             out[name] = {"iters_per_step": float(np.mean(its)), "ms_per_step": 1000 * dt / steps,

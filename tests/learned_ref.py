@@ -127,15 +127,20 @@ def forward(prm, r, z, geo: Geometry, rnd=True):
     return {"s": s, "x": x, "H": H, "Xs": Xs, "y": y, "q": q}
 
 
-def backward(prm, fw, t, z, geo: Geometry, rnd=True):
+def backward(prm, fw, t, z, geo: Geometry, rnd=True, dy=None):
+    """Gradient of the error loss for target t, or, with `dy` given, of any loss whose
+    derivative w.r.t. the network output y is dy (the loss is then returned as None)."""
     R = bf16 if rnd else (lambda a: np.asarray(a, np.float64))
     Win, bin_, Ws, bs, wout, bout = unpack(prm)
-    n = len(t)
     g = np.zeros(NPARAM)
-    ystar = (t - z) * geo.bdiag.astype(np.float64) / fw["s"]
-    e = fw["y"] - ystar
-    loss = 0.5 * np.sum(e * e) / n
-    dy = e / n
+    if dy is None:
+        n = len(t)
+        ystar = (t - z) * geo.bdiag.astype(np.float64) / fw["s"]
+        e = fw["y"] - ystar
+        loss = 0.5 * np.sum(e * e) / n
+        dy = e / n
+    else:
+        loss = None
     H = fw["H"]
     g[OFF_WOUT:OFF_WOUT + C] = dy @ H[3].astype(np.float64)
     g[OFF_BOUT] = dy.sum()

@@ -70,6 +70,55 @@ def test_laplc_bitwise(pair, impfl):
 
 
 @pytest.mark.parametrize("impfl", [0, 1])
+def test_laplc_adjoint(impfl):
+    """laplc_adjoint(y) = W^{-1} A^T W y with A assembled column by column from the oracle's laplc
+    on a 6x6x5 mesh (W = vol*rh0); for impfl = 0 the operator is W-self-adjoint, so the adjoint
+    equals laplc itself."""
+    from src_b200 import mesh
+    cm = mesh.generate(6, L=5, seed=3, h0=400.0)
+    rm = cm.to_reference()
+    P = RunParams(delt=10.0)
+    o = Oracle(P, rm)
+    o.setup()
+    N = rm.npoin
+    A = np.zeros((N, N))
+    for j in range(N):
+        e = np.zeros(N)
+        e[j] = 1.0
+        A[:, j] = o.laplc(e, impfl)
+    w = rm.vol * o.get(F_RH0)
+    y = np.random.default_rng(7).standard_normal(N)
+    want = (A.T @ (w * y)) / w
+    with Solver(P, rm) as s:
+        s.setup()
+        s.set(W0, y)
+        s.laplc_adjoint(W0, W1, impfl)
+        got = s.get(W1)
+        s.laplc(W0, W2, impfl)
+        ly = s.get(W2)
+    assert rel(got, want) < 1e-12
+    if impfl == 0:
+        assert rel(got, ly) < 1e-12
+
+
+@pytest.mark.parametrize("impfl", [0, 1])
+def test_laplc_adjoint_identity(pair, impfl):
+    """<laplc(u), y>_W = <u, laplc_adjoint(y)>_W on the larger meshes."""
+    cm, rm, o, s = pair
+    rng = np.random.default_rng(8)
+    u, y = rng.standard_normal(rm.npoin), rng.standard_normal(rm.npoin)
+    s.set(W0, u)
+    s.set(W1, y)
+    s.laplc(W0, W2, impfl)
+    s.laplc_adjoint(W1, W3, impfl)
+    w = rm.vol * s.get(F_RH0)
+    au, aty = s.get(W2), s.get(W3)
+    lhs, rhs = np.sum(w * au * y), np.sum(w * u * aty)
+    scale = np.sqrt(np.sum(w * au * au) * np.sum(w * y * y))
+    assert abs(lhs - rhs) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("impfl", [0, 1])
 def test_prfr_bitwise(pair, impfl):
     cm, rm, o, s = pair
     rng = np.random.default_rng(2)
