@@ -138,6 +138,19 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def learned_weights(name, rm, device):
+    """Weights of the learned preconditioner: the committed training run when present (trained by
+    `python -m src_b200.learned` on the 256x256x81 family), else a short training on this
+    workload's own plain solves (untimed).  Returns (params, nn_rate, description)."""
+    from src_b200 import learned
+    if os.path.exists(learned.WEIGHTS):
+        w, rate = learned.load_weights()
+        return w, rate, os.path.relpath(learned.WEIGHTS, ROOT)
+    w, hist, rate = learned.train(rm, build_params(name), steps=3, every=4, max_records=48, epochs=2,
+                                  device=device)
+    return w, rate, "trained here on 3 plain steps of this workload"
+
+
 def cpu_sample(steps, warmup):
     """Oracle (CPU restatement, 1 thread) full steps of the 48x48x41 workload."""
     from oracle.oracle import Oracle
@@ -250,6 +263,7 @@ def main():
     ms = e0.elapsed_time(e1)
     kt = s.kernel_times()
     s.kernel_timing(False)
+    ref_fields = {k: s.get(F_UNK + k) for k in range(4)} if not args.no_variants else None
     ms_max = ms
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -329,9 +343,15 @@ def main():
     # ---------------- variants on the same workload (reported beside the headline FP64 path)
     variants = {}
     if not args.no_variants:
-        for vname, prec in (("mixed", 1),):
+        for vname, prec, iprc in (("mixed", 1, 2), ("learned_mixed", 1, 3)):
             Pv = build_params(name, precision=prec)
+            Pv.iprc = iprc
+            weights_src = None
+            if iprc == 3:
+                weights, Pv.nn_rate, weights_src = learned_weights(name, rm, local)
             sv = Solver(Pv, rm, device=local)
+            if iprc == 3:
+                sv.learned_set_params(weights)
             sv.setup()
             if Pv.nscal:
                 sv.set(F_UNK + 4, gaussian_scalar(rm))
@@ -344,10 +364,11 @@ def main():
             sv.kernel_timing(True)
             a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a0.record(stream_v)
-            vit = []
+            vit, vfb = [], 0
             for _ in range(args.steps):
                 dv = sv.step()
                 vit.append((dv.niter1, dv.niter))
+                vfb += dv.fallbacks
             a1.record(stream_v)
             a1.synchronize()
             barrier()
@@ -358,14 +379,24 @@ def main():
                 vms = float(t.item())
             vkt = sv.kernel_times()
             vsolve = vkt.get("pressure_solve", (1, 0.0))
+            err = {}
+            for k, nm in enumerate(("u", "v", "w", "theta")):
+                a, b = sv.get(F_UNK + k), ref_fields[k]
+                err[nm] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
             variants[vname] = {
                 "value": world * args.steps / (vms / 1000.0), "unit": "steps/s",
                 "ms_per_step": vms / args.steps,
                 "ms_per_pressure_solve": round(vsolve[1] / max(vsolve[0], 1), 3),
                 "gcr_iters_per_solve": round(float(np.mean([a for p in vit for a in p])), 2),
                 "speedup_vs_fp64": round((world * args.steps / (vms / 1000.0)) / value, 3),
+                "rel_l2_vs_fp64": err,
+                "kernels_ms": {k: round(v[1], 2) for k, v in vkt.items()},
                 "precision": "FP32 face vectors, MPDATA fluxes, GCR directions and operator; "
                              "FP64 p, r, inner products, coefficients, stopping test, Thomas solves, mass sums"}
+            if iprc == 3:
+                variants[vname].update({"fallbacks": vfb, "nn_rate": Pv.nn_rate, "weights": weights_src,
+                                        "network": "3 message-passing layers x 32 channels, BF16 tcgen05 "
+                                                   "forward, corrects the vertical-line preconditioner"})
             sv.close()
 
     cpu = None

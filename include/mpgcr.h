@@ -229,8 +229,9 @@ int mpg_synchronize(mpg_handle h);
  * FP32 accumulation) that corrects the vertical-line preconditioner inside gcrk:
  * q = M^{-1} r + net(r) (see src_b200/csrc/learned.cuh).  It is used when params.iprc == 3; the
  * plain line preconditioner takes over for the rest of a solve if the network's output is not
- * finite or the residual stops decreasing (mpg_gcr_stats.fallbacks counts the switches), and
- * every solve still has to meet the same FP64 stopping test.  No counterpart in the reference.
+ * finite, the residual stops decreasing, or ||r||_2 after m iterations exceeds params.nn_rate^m
+ * of its start (mpg_gcr_stats.fallbacks counts the switches), and every solve still has to meet
+ * the same FP64 stopping test.  Meshes of at most 128 levels.  No counterpart in the reference.
  * Training runs on the GPU with the library's own forward/backward kernels and Adam. */
 #define MPG_LEARNED_NPARAM 9505
 /* Initialise the weights (seeded): hidden layers random, output layer zero, so the initial

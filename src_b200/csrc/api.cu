@@ -62,7 +62,8 @@ struct mpg_solver {
     double *r = nullptr, *qr = nullptr, *ar = nullptr, *x[MPG_MAX_LORD] = {}, *ax[MPG_MAX_LORD] = {};
     double *F[3] = {}, *tres = nullptr;
     // mixed precision: FP32 directions, operator intermediates and node metrics
-    float *xf[MPG_MAX_LORD] = {}, *axf[MPG_MAX_LORD] = {}, *qrf = nullptr, *arf = nullptr, *Ff[3] = {};
+    float *xf[MPG_MAX_LORD] = {}, *axf[MPG_MAX_LORD] = {}, *qrf = nullptr, *arf = nullptr;
+    float4 *Ff4 = nullptr;                           // packed laplc fluxes (mixed precision)
     float *volf = nullptr, *rh0f = nullptr, *coefwf = nullptr;
     double *scal = nullptr, *part = nullptr, *result = nullptr, *h_res = nullptr;
     unsigned int *counter = nullptr;
@@ -220,7 +221,7 @@ template <> struct Buf<double> {
     static double *ax(mpg_handle h, int q) { return h->ax[q]; }
     static double *qr(mpg_handle h) { return h->qr; }
     static double *ar(mpg_handle h) { return h->ar; }
-    static double *F(mpg_handle h, int d) { return h->F[d]; }
+    static Flux<double> F(mpg_handle h) { return Flux<double>{h->F[0], h->F[1], h->F[2]}; }
     static const double *vol(mpg_handle h) { return h->vol; }
     static const double *rh0(mpg_handle h) { return h->f[MPG_F_RH0]; }
     static const double *coefw(mpg_handle h) { return h->f[MPG_F_COEFW]; }
@@ -230,51 +231,23 @@ template <> struct Buf<float> {
     static float *ax(mpg_handle h, int q) { return h->axf[q]; }
     static float *qr(mpg_handle h) { return h->qrf; }
     static float *ar(mpg_handle h) { return h->arf; }
-    static float *F(mpg_handle h, int d) { return h->Ff[d]; }
+    static Flux<float> F(mpg_handle h) { return Flux<float>{h->Ff4}; }
     static const float *vol(mpg_handle h) { return h->volf; }
     static const float *rh0(mpg_handle h) { return h->rh0f; }
     static const float *coefw(mpg_handle h) { return h->coefwf; }
 };
 
-#ifndef MPG_LAP_CW
-#define MPG_LAP_CW 0
-#endif
-template <class T, int NS>
-void launch_laplc_cw(mpg_handle h, const T *p, T *alap, int impfl) {
-    using B = Buf<T>;
-    const int nb = (h->NC + kCWWarps - 1) / kCWWarps;
-    {
-        KTIME(KT_LAP_GRAD);
-        k_lap_grad_cw<T, NS><<<nb, 32 * kCWWarps, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
-                                                              (T)h->P.delt, impfl, B::F(h, 0), B::F(h, 1), B::F(h, 2));
-    }
-    {
-        KTIME(KT_LAP_DIV);
-        k_lap_div_cw<T, NS><<<nb, 32 * kCWWarps, 0, h->st>>>(h->M, B::F(h, 0), B::F(h, 1), B::F(h, 2), B::vol(h),
-                                                             B::rh0(h), alap);
-    }
-}
-
 template <class T>
 int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
     using B = Buf<T>;
-    if (MPG_LAP_CW && h->kch <= 4) {
-        switch (h->kch) {
-            case 1: launch_laplc_cw<T, 1>(h, p, alap, impfl); break;
-            case 2: launch_laplc_cw<T, 2>(h, p, alap, impfl); break;
-            case 3: launch_laplc_cw<T, 3>(h, p, alap, impfl); break;
-            default: launch_laplc_cw<T, 4>(h, p, alap, impfl); break;
-        }
-        return check_launch("laplc");
-    }
     {
         KTIME(KT_LAP_GRAD);
         k_lap_grad<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
-                                                          (T)h->P.delt, impfl, B::F(h, 0), B::F(h, 1), B::F(h, 2));
+                                                          (T)h->P.delt, impfl, B::F(h));
     }
     {
         KTIME(KT_LAP_DIV);
-        k_lap_div<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, B::F(h, 0), B::F(h, 1), B::F(h, 2), B::vol(h),
+        k_lap_div<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, B::F(h), B::vol(h),
                                                          B::rh0(h), alap);
     }
     return check_launch("laplc");
@@ -468,7 +441,8 @@ int nn_alloc_infer(mpg_handle h) {
         const size_t n = h->N;
         if ((rc = dalloc(h, &S.prm, nn::NPARAM)) || (rc = dalloc(h, &S.Wbf, (size_t)nn::NL * nn::C * nn::K3)) ||
             (rc = dalloc(h, &S.H[0], n * nn::C)) || (rc = dalloc(h, &S.H[1], n * nn::C)) ||
-            (rc = dalloc(h, &S.z, n)) || (rc = dalloc(h, &S.sc, 4)) || (rc = dalloc(h, &S.err, 1)))
+            (rc = dalloc(h, &S.z, n)) || (rc = dalloc(h, &S.sc, 4)) || (rc = dalloc(h, &S.err, 1)) ||
+            (rc = dalloc(h, &S.X0, n * nn::FIN)))
             return rc;
         S.infer = true;
     }
@@ -485,7 +459,7 @@ int nn_alloc_train(mpg_handle h) {
     const size_t np = S.Npad;
     if ((rc = dalloc(h, &S.grad, nn::NPARAM)) || (rc = dalloc(h, &S.m1, nn::NPARAM)) ||
         (rc = dalloc(h, &S.m2, nn::NPARAM)) || (rc = dalloc(h, &S.H[2], n * nn::C)) ||
-        (rc = dalloc(h, &S.H[3], n * nn::C)) || (rc = dalloc(h, &S.X0, n * nn::FIN)) ||
+        (rc = dalloc(h, &S.H[3], n * nn::C)) ||
         (rc = dalloc(h, &S.dH, n * nn::C)) || (rc = dalloc(h, &S.dH2, n * nn::C)) ||
         (rc = dalloc(h, &S.G0, n * nn::C)) || (rc = dalloc(h, &S.Gh, n * nn::C)) ||
         (rc = dalloc(h, &S.Gv, n * nn::C)) || (rc = dalloc(h, &S.Y, n)) || (rc = dalloc(h, &S.dU, np * nn::C)) ||
@@ -501,6 +475,25 @@ int nn_alloc_train(mpg_handle h) {
     return MPG_OK;
 }
 
+// the three message-passing layers over the columns (input layer fused into the first, output
+// layer into the last); with `train` every activation the backward pass reads is kept
+template <int NS>
+void nn_layers(mpg_handle h, const nn::Geom &G, double *qd, float *qf, bool train) {
+    auto &S = h->nn;
+    const int nb = std::min(h->NC, 148 * 5);
+    const size_t W = (size_t)nn::C * nn::K3;
+    nn::k_nn_col<NS, true, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, nullptr, S.X0, S.Wbf, S.prm, 0, nullptr, nullptr, S.H[1], nullptr, nullptr,
+        train ? S.H[0] : nullptr, train ? S.Xs[0] : nullptr, nullptr, S.err);
+    __nv_bfloat16 *h2 = train ? S.H[2] : S.H[0];
+    nn::k_nn_col<NS, false, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, S.H[1], nullptr, S.Wbf + W, S.prm, 1, nullptr, nullptr, h2, nullptr, nullptr,
+        nullptr, train ? S.Xs[1] : nullptr, nullptr, S.err);
+    nn::k_nn_col<NS, false, true><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, h2, nullptr, S.Wbf + 2 * W, S.prm, 2, S.z, S.sc, train ? S.H[3] : nullptr, qd, qf,
+        nullptr, train ? S.Xs[2] : nullptr, train ? S.Y : nullptr, S.err);
+}
+
 // forward pass on residual r: z = M^{-1} r (impfl coefficients), sigma, the network; q in T.
 // With `train` the activations are kept (H[0..3], X0, Xs) for the backward pass.
 template <class T>
@@ -508,26 +501,22 @@ int nn_forward(mpg_handle h, const double *r, T *q, int impfl, bool train) {
     auto &S = h->nn;
     const int N = h->N;
     int rc;
+    if (h->L > nn::COL_MAXL) return mpg_fail(MPG_ERR_UNSUPPORTED, "learned preconditioner: more than 128 levels");
     if ((rc = op_line<double>(h, r, S.z, impfl, 0))) return rc;
     if ((rc = reduce<1>(h, 0x1u, ProdAbsD{r}, FinSigma{S.sc}))) return rc;
     const nn::Geom G = nn_geom(h);
-    __nv_bfloat16 *Hin = S.H[0];
+    double *qd = nullptr;
+    float *qf = nullptr;
+    if constexpr (std::is_same<T, double>::value) qd = q; else qf = q;
     {
         KTIME(KT_NN);
-        nn::k_nn_input<<<grid(N), kThreads, 0, h->st>>>(N, r, S.z, S.sc, G, S.prm, S.H[0], train ? S.X0 : nullptr);
-        const int ntiles = (N + nn::TCM - 1) / nn::TCM;
-        const int nblk = std::min(ntiles, 148 * 3);
-        for (int l = 0; l < nn::NL; ++l) {
-            __nv_bfloat16 *Hout = train ? S.H[l + 1] : S.H[(l + 1) & 1];
-            nn::k_nn_layer_tc<<<nblk, nn::TC_THREADS, 0, h->st>>>(h->M, G, Hin, S.Wbf + (size_t)l * nn::C * nn::K3,
-                                                                  S.prm + nn::OFF_L0 + l * nn::LSTRIDE + nn::C * nn::K3,
-                                                                  Hout, train ? S.Xs[l] : nullptr, S.err);
-            Hin = Hout;
+        nn::k_nn_features<<<grid(N), kThreads, 0, h->st>>>(N, r, S.z, S.sc, G, S.X0);
+        switch ((h->L + 31) / 32) {
+            case 1: nn_layers<1>(h, G, qd, qf, train); break;
+            case 2: nn_layers<2>(h, G, qd, qf, train); break;
+            case 3: nn_layers<3>(h, G, qd, qf, train); break;
+            default: nn_layers<4>(h, G, qd, qf, train); break;
         }
-        double *qd = nullptr;
-        float *qf = nullptr;
-        if constexpr (std::is_same<T, double>::value) qd = q; else qf = q;
-        nn::k_nn_output<<<grid(N), kThreads, 0, h->st>>>(N, Hin, S.prm, S.z, S.sc, G, train ? S.Y : nullptr, qd, qf);
     }
     return check_launch("nn forward");
 }
@@ -1286,8 +1275,7 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
         for (int q = 0; q < prm->lord; ++q)
             if ((rc = dalloc(h, &h->xf[q], N)) || (rc = dalloc(h, &h->axf[q], N))) return fail(rc);
         if ((rc = dalloc(h, &h->qrf, N)) || (rc = dalloc(h, &h->arf, N))) return fail(rc);
-        for (int q = 0; q < 3; ++q)
-            if ((rc = dalloc(h, &h->Ff[q], N))) return fail(rc);
+        if ((rc = dalloc(h, &h->Ff4, N))) return fail(rc);
         auto tof = [](const std::vector<double> &v) {
             std::vector<float> o(v.size());
             for (size_t i = 0; i < v.size(); ++i) o[i] = (float)v[i];
@@ -1298,11 +1286,15 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
             (rc = upload(h, &cf, tof(h->hs.coefw))))
             return fail(rc);
         h->volf = vf; h->rh0f = rf; h->coefwf = cf;
-        for (int d = 0; d < 3; ++d) {
-            float *a, *b;
-            if ((rc = upload(h, &a, tof(hm.Sh[d]))) || (rc = upload(h, &b, tof(hm.Sv[d])))) return fail(rc);
-            M.Shf[d] = a; M.Svf[d] = b;
-        }
+        auto pack = [](const std::vector<double> *S) {
+            std::vector<float4> o(S[0].size());
+            for (size_t i = 0; i < o.size(); ++i)
+                o[i] = make_float4((float)S[0][i], (float)S[1][i], (float)S[2][i], 0.f);
+            return o;
+        };
+        float4 *a, *b;
+        if ((rc = upload(h, &a, pack(hm.Sh))) || (rc = upload(h, &b, pack(hm.Sv)))) return fail(rc);
+        M.Shf4 = a; M.Svf4 = b;
     }
     if ((rc = dalloc(h, &h->scal, S_COUNT)) || (rc = dalloc(h, &h->part, (size_t)kRedBlocks * kMaxQ)) ||
         (rc = dalloc(h, &h->result, kMaxQ)) || (rc = dalloc(h, &h->counter, 1)))
@@ -1736,9 +1728,10 @@ extern "C" int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap
     // every scratch element read below is written earlier in this call, so nothing needs clearing
     const int N = h->N;
     k_scatter_perm<<<grid(N), kThreads, 0, h->st>>>(N, h->d_perm, press, pin);
+    const Flux<double> F{F0, F1, F2};
     k_lap_grad<<<grid(h->N), kThreads, 0, h->st>>>(h->M, pin, h->vol, h->f[MPG_F_RH0], h->f[MPG_F_COEFW], h->ue,
-                                                h->P.delt, impfl, F0, F1, F2);
-    k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, F0, F1, F2, h->vol, h->f[MPG_F_RH0], aout);
+                                                h->P.delt, impfl, F);
+    k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, F, h->vol, h->f[MPG_F_RH0], aout);
     k_gather_perm<<<grid(N), kThreads, 0, h->st>>>(N, h->d_perm, aout, alap);
     return check_launch("laplc_noalloc");
 }

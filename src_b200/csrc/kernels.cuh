@@ -19,7 +19,10 @@
 namespace mpgk {
 
 constexpr int kThreads = 256;
-constexpr int kRedBlocks = 592;          // 4 x 148 SMs
+#ifndef MPG_RED_BLOCKS
+#define MPG_RED_BLOCKS 592
+#endif
+constexpr int kRedBlocks = MPG_RED_BLOCKS;   // 4 x 148 SMs
 constexpr int kRedThreads = 256;
 constexpr int kMaxQ = 24;                // quantities per reduction
 
@@ -80,13 +83,39 @@ __device__ __forceinline__ void for_faces(const ColMesh &M, int c, int k, int n,
 __device__ __forceinline__ const double *spick(const ColMesh &M, int d, bool vert) {
     return vert ? M.Sv[d] : M.Sh[d];
 }
-// face vectors in the storage type of a kernel instantiation (FP32 copies in mixed precision)
-template <class T> struct SPick;
-template <> struct SPick<double> {
-    __device__ static const double *get(const ColMesh &M, int d, bool vert) { return vert ? M.Sv[d] : M.Sh[d]; }
+// face vector si (horizontal or vertical) in the storage type of a kernel instantiation: three
+// FP64 arrays, or in mixed precision one packed float4 (x, y, z, 0) per face, so an FP32 gather
+// issues one 16-byte load per face instead of three 4-byte ones
+template <class T> struct FaceVec;
+template <> struct FaceVec<double> {
+    __device__ static void load(const ColMesh &M, bool vert, int si, double &x, double &y, double &z) {
+        x = __ldg((vert ? M.Sv[0] : M.Sh[0]) + si);
+        y = __ldg((vert ? M.Sv[1] : M.Sh[1]) + si);
+        z = __ldg((vert ? M.Sv[2] : M.Sh[2]) + si);
+    }
 };
-template <> struct SPick<float> {
-    __device__ static const float *get(const ColMesh &M, int d, bool vert) { return vert ? M.Svf[d] : M.Shf[d]; }
+template <> struct FaceVec<float> {
+    __device__ static void load(const ColMesh &M, bool vert, int si, float &x, float &y, float &z) {
+        const float4 v = __ldg((vert ? M.Svf4 : M.Shf4) + si);
+        x = v.x; y = v.y; z = v.z;
+    }
+};
+
+// the three flux components between the halves of laplc: three FP64 arrays, or one packed
+// float4 per node in mixed precision (one 16-byte load per neighbour)
+template <class T> struct Flux;
+template <> struct Flux<double> {
+    double *x, *y, *z;
+    __device__ void store(int n, double a, double b, double c) const { x[n] = a; y[n] = b; z[n] = c; }
+    __device__ void load(int n, double &a, double &b, double &c) const { a = x[n]; b = y[n]; c = z[n]; }
+};
+template <> struct Flux<float> {
+    float4 *v;
+    __device__ void store(int n, float a, float b, float c) const { v[n] = make_float4(a, b, c, 0.f); }
+    __device__ void load(int n, float &a, float &b, float &c) const {
+        const float4 t = v[n];
+        a = t.x; b = t.y; c = t.z;
+    }
 };
 
 // Boundary entries of node (c,k), in reference order.
@@ -116,8 +145,10 @@ __device__ __forceinline__ void grad3(const ColMesh &M, const T *__restrict__ ph
     T ax = 0., ay = 0., az = 0.;
     for_faces(M, c, k, n,
         [&](const Face &f) {
-            return V4T<T>{__ldg(SPick<T>::get(M, 0, f.vert) + f.si), __ldg(SPick<T>::get(M, 1, f.vert) + f.si),
-                          __ldg(SPick<T>::get(M, 2, f.vert) + f.si), phi[f.j]};
+            V4T<T> v;
+            FaceVec<T>::load(M, f.vert, f.si, v.a, v.b, v.c);
+            v.d = phi[f.j];
+            return v;
         },
         [&](const Face &f, const V4T<T> &v) {
             const T u = (DIFF ? pn - v.d : pn + v.d) * T(0.5);
@@ -145,9 +176,7 @@ __device__ __forceinline__ void div3(const ColMesh &M, FX f, int c, int k, int n
     for_faces(M, c, k, n,
         [&](const Face &fc) {
             V6T<T> v;
-            v.a = __ldg(SPick<T>::get(M, 0, fc.vert) + fc.si);
-            v.b = __ldg(SPick<T>::get(M, 1, fc.vert) + fc.si);
-            v.c = __ldg(SPick<T>::get(M, 2, fc.vert) + fc.si);
+            FaceVec<T>::load(M, fc.vert, fc.si, v.a, v.b, v.c);
             f(fc.j, v.d, v.e, v.f);
             return v;
         },
@@ -247,8 +276,7 @@ __global__ void k_bcv(ColMesh M, double *u, double *v, double *w, const double *
 template <class T>
 __global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const T *__restrict__ p, const T *__restrict__ vol,
                                          const T *__restrict__ rh0, const T *__restrict__ coefw,
-                                         const double *__restrict__ ue, T dt, int impfl,
-                                         T *__restrict__ Fx, T *__restrict__ Fy, T *__restrict__ Fz) {
+                                         const double *__restrict__ ue, T dt, int impfl, Flux<T> F) {
     NODE_BEGIN
     T gx, gy, gz;
     grad3<T>(M, p, c, k, n, gx, gy, gz);
@@ -259,169 +287,17 @@ __global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const T *__restrict__ p, con
     dz = T(0.5) * dz * (coefw[n] * (T)impfl + (T)(1 - impfl));
     bcv_node<T>(M, c, k, n, ue, 0.0, dx, dy, dz);
     const T r = rh0[n];
-    Fx[n] = dx * r; Fy[n] = dy * r; Fz[n] = dz * r;
+    F.store(n, dx * r, dy * r, dz * r);
 }
 
 // laplc second half (ref.f:1339-1350): alap = (Dx(Fx) + Dy(Fy) + Dz(Fz)) / (vol*rh0)
 template <class T>
-__global__ void DIV_BOUNDS k_lap_div(ColMesh M, const T *__restrict__ Fx, const T *__restrict__ Fy,
-                          const T *__restrict__ Fz, const T *__restrict__ vol,
-                          const T *__restrict__ rh0, T *__restrict__ alap) {
+__global__ void DIV_BOUNDS k_lap_div(ColMesh M, const Flux<T> F, const T *__restrict__ vol,
+                                     const T *__restrict__ rh0, T *__restrict__ alap) {
     NODE_BEGIN
     T dx, dy, dz;
-    div3<T>(M, [&](int j, T &a, T &b, T &d) { a = Fx[j]; b = Fy[j]; d = Fz[j]; }, c, k, n, dx, dy, dz);
+    div3<T>(M, [&](int j, T &a, T &b, T &d) { F.load(j, a, b, d); }, c, k, n, dx, dy, dz);
     alap[n] = (dx + dy + dz) / (vol[n] * rh0[n]);
-}
-
-// ------------------------------------------------------------------------------ column-warp laplc
-// The same two halves of laplc with one warp per column: lane l holds levels l, l+32, ... (NS
-// slots).  The warp walks its column's adjacency list once (uniform branches, one broadcast load
-// per entry) and loads a face's operands for all NS slots before accumulating any, so a thread
-// has 4*NS (divergence: 6*NS) independent loads in flight per face where a node-per-thread
-// gather has 4 (6) behind each adjacency load.  Every node adds its terms in the same order as
-// k_lap_grad/k_lap_div, so the results are bit-identical to them.
-constexpr int kCWWarps = 8;
-
-template <class T, int NS>
-__global__ void __launch_bounds__(32 * kCWWarps)
-k_lap_grad_cw(ColMesh M, const T *__restrict__ p, const T *__restrict__ vol, const T *__restrict__ rh0,
-              const T *__restrict__ coefw, const double *__restrict__ ue, T dt, int impfl,
-              T *__restrict__ Fx, T *__restrict__ Fy, T *__restrict__ Fz) {
-    const int lane = threadIdx.x & 31;
-    const int c = blockIdx.x * kCWWarps + (threadIdx.x >> 5);
-    if (c >= M.NC) return;
-    const int L = M.L, base = c * L;
-    T pn[NS], ax[NS], ay[NS], az[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        const int k = lane + 32 * s;
-        pn[s] = k < L ? p[base + k] : T(0);
-        ax[s] = T(0); ay[s] = T(0); az[s] = T(0);
-    }
-    const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
-    const T *Sh0 = SPick<T>::get(M, 0, false), *Sh1 = SPick<T>::get(M, 1, false), *Sh2 = SPick<T>::get(M, 2, false);
-    const T *Sv0 = SPick<T>::get(M, 0, true), *Sv1 = SPick<T>::get(M, 1, true), *Sv2 = SPick<T>::get(M, 2, true);
-    for (int j = beg; j < end; ++j) {
-        const int2 en = __ldg(&M.cadj[j]);
-        const bool vert = en.x < 0, below = en.x == MPG_ADJ_BELOW;
-        const bool sub = vert ? below : ((en.x & 1) != 0);
-        T sx[NS], sy[NS], sz[NS], pj[NS];
-        bool ok[NS];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const int k = lane + 32 * s;
-            const int n = base + k;
-            ok[s] = k < L && (!vert || (below ? k > 0 : k + 1 < L));
-            const int si = vert ? (below ? n - 1 : n) : (en.x >> 1) * L + k;
-            const int jj = vert ? (below ? n - 1 : n + 1) : en.y * L + k;
-            if (ok[s]) {
-                sx[s] = __ldg((vert ? Sv0 : Sh0) + si);
-                sy[s] = __ldg((vert ? Sv1 : Sh1) + si);
-                sz[s] = __ldg((vert ? Sv2 : Sh2) + si);
-                pj[s] = p[jj];
-            }
-        }
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            if (!ok[s]) continue;
-            const T u = (pn[s] + pj[s]) * T(0.5);
-            const T tx = sx[s] * u, ty = sy[s] * u, tz = sz[s] * u;
-            if (sub) { ax[s] = ax[s] - tx; ay[s] = ay[s] - ty; az[s] = az[s] - tz; }
-            else     { ax[s] = ax[s] + tx; ay[s] = ay[s] + ty; az[s] = az[s] + tz; }
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        const int k = lane + 32 * s;
-        if (k >= L) continue;
-        const int n = base + k;
-        T gx = ax[s], gy = ay[s], gz = az[s];
-        if (M.iper == 0) {
-            for_boundary(M, c, k, [&](const BEntry &be) {
-                gx = gx + T(be.sbb[0]) * pn[s];
-                gy = gy + T(be.sbb[1]) * pn[s];
-                gz = gz + T(be.sbb[2]) * pn[s];
-            });
-        }
-        const T v = vol[n];
-        T dx = dt * gx / v, dy = dt * gy / v, dz = dt * gz / v;
-        dx = T(0.5) * dx / T(1.0);
-        dy = T(0.5) * dy / T(1.0);
-        dz = T(0.5) * dz * (coefw[n] * (T)impfl + (T)(1 - impfl));
-        bcv_node<T>(M, c, k, n, ue, 0.0, dx, dy, dz);
-        const T r = rh0[n];
-        Fx[n] = dx * r; Fy[n] = dy * r; Fz[n] = dz * r;
-    }
-}
-
-template <class T, int NS>
-__global__ void __launch_bounds__(32 * kCWWarps)
-k_lap_div_cw(ColMesh M, const T *__restrict__ Fx, const T *__restrict__ Fy, const T *__restrict__ Fz,
-             const T *__restrict__ vol, const T *__restrict__ rh0, T *__restrict__ alap) {
-    const int lane = threadIdx.x & 31;
-    const int c = blockIdx.x * kCWWarps + (threadIdx.x >> 5);
-    if (c >= M.NC) return;
-    const int L = M.L, base = c * L;
-    T fx[NS], fy[NS], fz[NS], ax[NS], ay[NS], az[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        const int k = lane + 32 * s;
-        const bool in = k < L;
-        fx[s] = in ? Fx[base + k] : T(0);
-        fy[s] = in ? Fy[base + k] : T(0);
-        fz[s] = in ? Fz[base + k] : T(0);
-        ax[s] = T(0); ay[s] = T(0); az[s] = T(0);
-    }
-    const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
-    const T *Sh0 = SPick<T>::get(M, 0, false), *Sh1 = SPick<T>::get(M, 1, false), *Sh2 = SPick<T>::get(M, 2, false);
-    const T *Sv0 = SPick<T>::get(M, 0, true), *Sv1 = SPick<T>::get(M, 1, true), *Sv2 = SPick<T>::get(M, 2, true);
-    for (int j = beg; j < end; ++j) {
-        const int2 en = __ldg(&M.cadj[j]);
-        const bool vert = en.x < 0, below = en.x == MPG_ADJ_BELOW;
-        const bool sub = vert ? below : ((en.x & 1) != 0);
-        T sx[NS], sy[NS], sz[NS], gx[NS], gy[NS], gz[NS];
-        bool ok[NS];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const int k = lane + 32 * s;
-            const int n = base + k;
-            ok[s] = k < L && (!vert || (below ? k > 0 : k + 1 < L));
-            const int si = vert ? (below ? n - 1 : n) : (en.x >> 1) * L + k;
-            const int jj = vert ? (below ? n - 1 : n + 1) : en.y * L + k;
-            if (ok[s]) {
-                sx[s] = __ldg((vert ? Sv0 : Sh0) + si);
-                sy[s] = __ldg((vert ? Sv1 : Sh1) + si);
-                sz[s] = __ldg((vert ? Sv2 : Sh2) + si);
-                gx[s] = Fx[jj];
-                gy[s] = Fy[jj];
-                gz[s] = Fz[jj];
-            }
-        }
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            if (!ok[s]) continue;
-            const T tx = sx[s] * ((fx[s] + gx[s]) * T(0.5));
-            const T ty = sy[s] * ((fy[s] + gy[s]) * T(0.5));
-            const T tz = sz[s] * ((fz[s] + gz[s]) * T(0.5));
-            if (sub) { ax[s] = ax[s] - tx; ay[s] = ay[s] - ty; az[s] = az[s] - tz; }
-            else     { ax[s] = ax[s] + tx; ay[s] = ay[s] + ty; az[s] = az[s] + tz; }
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        const int k = lane + 32 * s;
-        if (k >= L) continue;
-        const int n = base + k;
-        T dx = ax[s], dy = ay[s], dz = az[s];
-        if (M.iper == 0) {
-            for_boundary(M, c, k, [&](const BEntry &be) {
-                dx = dx + T(be.sbb[0]) * fx[s];
-                dy = dy + T(be.sbb[1]) * fy[s];
-                dz = dz + T(be.sbb[2]) * fz[s];
-            });
-        }
-        alap[n] = (dx + dy + dz) / (vol[n] * rh0[n]);
-    }
 }
 
 // Adjoint of laplc in the inner product weighted by W = vol*rh0.  laplc is
@@ -498,6 +374,7 @@ __global__ void k_div(ColMesh M, const double *__restrict__ ua, const double *__
 // With 4 KiB of shared memory per warp the kernel keeps enough warps resident to stream.
 constexpr int kLineWarps = 8;
 constexpr int kLineChunk = 16;
+constexpr int kLinePre = 8;
 template <class TO>
 __global__ void __launch_bounds__(32 * kLineWarps)
 k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__restrict__ la,
@@ -521,12 +398,22 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
         }
         __syncwarp();
         if (own) {
-#pragma unroll 8
-            for (int kk = 0; kk < nk; ++kk) {
-                const int k = k0 + kk;
-                const int64_t li = line_index(c, k, L);
-                d = (k == 0) ? t[lane][kk] * linv[li] : (t[lane][kk] - la[li] * d) * linv[li];
-                dbuf[li] = d;
+            // coefficients of kLinePre levels are loaded before the dependent chain uses them
+            for (int kb = 0; kb < nk; kb += kLinePre) {
+                double A[kLinePre], Mi[kLinePre];
+#pragma unroll
+                for (int i = 0; i < kLinePre; ++i) {
+                    const int64_t li = line_index(c, k0 + kb + i, L);
+                    A[i] = kb + i < nk ? la[li] : 0.;
+                    Mi[i] = kb + i < nk ? linv[li] : 0.;
+                }
+#pragma unroll
+                for (int i = 0; i < kLinePre; ++i) {
+                    if (kb + i >= nk) break;
+                    const int k = k0 + kb + i;
+                    d = (k == 0) ? t[lane][kb + i] * Mi[i] : (t[lane][kb + i] - A[i] * d) * Mi[i];
+                    dbuf[line_index(c, k, L)] = d;
+                }
             }
         }
         __syncwarp();
@@ -537,12 +424,21 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
     for (int k0 = last0; k0 >= 0; k0 -= kLineChunk) {
         const int nk = min(kLineChunk, L - k0);
         if (own) {
-#pragma unroll 8
-            for (int kk = nk - 1; kk >= 0; --kk) {
-                const int k = k0 + kk;
-                const int64_t li = line_index(c, k, L);
-                z = (k == L - 1) ? dbuf[li] : dbuf[li] - lcp[li] * z;
-                t[lane][kk] = z;
+            for (int kb = nk - 1; kb >= 0; kb -= kLinePre) {
+                double D[kLinePre], Cp[kLinePre];
+#pragma unroll
+                for (int i = 0; i < kLinePre; ++i) {
+                    const int64_t li = line_index(c, k0 + kb - i, L);
+                    D[i] = kb - i >= 0 ? dbuf[li] : 0.;
+                    Cp[i] = kb - i >= 0 ? lcp[li] : 0.;
+                }
+#pragma unroll
+                for (int i = 0; i < kLinePre; ++i) {
+                    if (kb - i < 0) break;
+                    const int k = k0 + kb - i;
+                    z = (k == L - 1) ? D[i] : D[i] - Cp[i] * z;
+                    t[lane][kb - i] = z;
+                }
             }
         }
         __syncwarp();

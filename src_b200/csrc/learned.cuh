@@ -11,9 +11,12 @@
 //
 // T_nj is the face coupling 0.5 dt |S|^2 rho_f / vol_f of the face (n, j), D_n its sum over the
 // node's horizontal (vertical) faces.  Activations are stored in BF16 (node-major, 32 channels =
-// 64 bytes per node, so a neighbour gather reads one contiguous 64-byte row); the 96 -> 32
-// transforms run on the tensor cores with BF16 operands and FP32 accumulation; the weight
-// gradients are reduced deterministically (per-block partials folded in a fixed order).
+// 64 bytes per node; in the column layout a neighbour column's rows are one contiguous block).
+// Forward: one CTA per column, the 96 -> 32 transforms on the tensor cores with tcgen05.mma
+// (BF16 operands, FP32 accumulation in tensor memory), the input layer fused into the first
+// layer and the output layer into the last.  Backward (training only): warp-level BF16 mma
+// (wmma) with the weight gradients reduced deterministically (per-block partials folded in a
+// fixed order).
 #pragma once
 
 #include <cuda_bf16.h>
@@ -37,8 +40,8 @@ constexpr int OFF_WOUT = OFF_L0 + NL * LSTRIDE;  // [C]
 constexpr int OFF_BOUT = OFF_WOUT + C;           // [1]
 constexpr int NPARAM = OFF_BOUT + 1;             // 9505
 
-constexpr int WARPS = 4;                          // warps per block in the layer kernels
-constexpr int TILE = 32;                          // nodes per warp tile
+constexpr int WARPS = 4;                          // warps per block in k_nn_dw
+constexpr int TILE = 32;                          // nodes per warp tile of the backward kernels
 constexpr int BWARPS = 2;                         // warps per block in k_nn_layer_bwd
 
 struct Geom {
@@ -58,8 +61,6 @@ __device__ __forceinline__ float face_T(const ColMesh &M, const Geom &G, const F
 struct alignas(16) B8 { __nv_bfloat162 v[4]; };
 // what the face loops load per face (namespace-scope types: a class declared inside the
 // loading lambda came back with a wrong layout from for_faces)
-struct RowB { B8 h; float t; };
-struct RowB2 { B8 a, b; float t; };
 struct RowF { float4 lo, hi; float t; };
 
 __device__ __forceinline__ void b8_to_f(const B8 &b, float *f) {
@@ -71,162 +72,12 @@ __device__ __forceinline__ void b8_to_f(const B8 &b, float *f) {
     }
 }
 
-// ---------------------------------------------------------------------------------- forward
-// h0 = relu(W_in x + b_in); the features also go to X0 (FP32 [N][FIN]) for the backward pass
-__global__ void k_nn_input(int N, const double *__restrict__ r, const double *__restrict__ z,
-                           const double *__restrict__ sc, Geom G, const float *__restrict__ prm,
-                           __nv_bfloat16 *__restrict__ H0, float *__restrict__ X0) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N) return;
-    const double s = sc[0] > 0. ? sc[0] : 1.;
-    float x[FIN];
-    x[0] = (float)(r[n] / s);
-    x[1] = (float)(z[n] * (double)G.bdiag[n] / s);
-    x[2] = G.feat2[n];
-    x[3] = G.bnd[n];
-    if (X0) {
-#pragma unroll
-        for (int i = 0; i < FIN; ++i) X0[(size_t)n * FIN + i] = x[i];
-    }
-    __align__(16) __nv_bfloat16 o[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) {
-        float u = prm[OFF_BIN + c];
-#pragma unroll
-        for (int i = 0; i < FIN; ++i) u += prm[OFF_WIN + c * FIN + i] * x[i];
-        o[c] = __float2bfloat16(u > 0.f ? u : 0.f);
-    }
-    const uint4 *src = reinterpret_cast<const uint4 *>(o);
-    uint4 *dst = reinterpret_cast<uint4 *>(H0 + (size_t)n * C);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) dst[i] = src[i];
-}
-
-// The 96-wide layer input of node n, quarter q (channels 8q..8q+7) of each 32-channel block:
-// [h_n ; A_h(h)_n ; A_v(h)_n]
-__device__ __forceinline__ void layer_row(const ColMesh &M, const Geom &G, const __nv_bfloat16 *__restrict__ H,
-                                          int n, int q, float *self, float *ah, float *av) {
-    const int c = n / M.L, k = n - c * M.L;
-    B8 sb = *reinterpret_cast<const B8 *>(H + (size_t)n * C + 8 * q);
-    b8_to_f(sb, self);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) { ah[i] = 0.f; av[i] = 0.f; }
-    const float ih = G.iDh[n], iv = G.iDv[n];
-    for_faces(M, c, k, n,
-        [&](const Face &f) {
-            RowB p;
-            p.h = *reinterpret_cast<const B8 *>(H + (size_t)f.j * C + 8 * q);
-            p.t = face_T(M, G, f);
-            return p;
-        },
-        [&](const Face &f, const auto &p) {
-            float hj[8];
-            b8_to_f(p.h, hj);
-            const float w = p.t * (f.vert ? iv : ih);
-            if (f.vert) {
-#pragma unroll
-                for (int i = 0; i < 8; ++i) av[i] += w * (hj[i] - self[i]);
-            } else {
-#pragma unroll
-                for (int i = 0; i < 8; ++i) ah[i] += w * (hj[i] - self[i]);
-            }
-        });
-}
-
-// One message-passing layer.  Each warp builds a 32 x 96 BF16 input tile in shared memory
-// (4 lanes per node, 8 channels per lane), multiplies it by W^T (96 x 32) on the tensor cores
-// and applies bias + ReLU.  With Xs != null the input rows are also kept for the backward pass.
-__global__ void __launch_bounds__(32 * WARPS)
-k_nn_layer(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __nv_bfloat16 *__restrict__ Wbf,
-           const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Hout, __nv_bfloat16 *__restrict__ Xs) {
-    using namespace nvcuda;
-    __shared__ __align__(32) __nv_bfloat16 sW[K3 * C];             // W^T: [k][n]
-    __shared__ __align__(32) __nv_bfloat16 sX[WARPS][TILE * K3];
-    __shared__ __align__(32) float sC[WARPS][TILE * C];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = threadIdx.x; i < K3 * C; i += blockDim.x) {
-        const int kk = i / C, nn = i - kk * C;
-        sW[i] = Wbf[nn * K3 + kk];
-    }
-    __syncthreads();
-    const int N = M.N;
-    const int ntiles = (N + TILE - 1) / TILE;
-    for (int t = blockIdx.x * WARPS + w; t < ntiles; t += gridDim.x * WARPS) {
-        const int base = t * TILE;
-        __nv_bfloat16 *X = sX[w];
-        for (int pass = 0; pass < TILE / 8; ++pass) {
-            const int m = pass * 8 + (lane >> 2), q = lane & 3;
-            const int n = base + m;
-            float self[8], ah[8], av[8];
-            if (n < N) {
-                layer_row(M, G, Hin, n, q, self, ah, av);
-            } else {
-#pragma unroll
-                for (int i = 0; i < 8; ++i) { self[i] = 0.f; ah[i] = 0.f; av[i] = 0.f; }
-            }
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                X[m * K3 + 8 * q + i] = __float2bfloat16(self[i]);
-                X[m * K3 + C + 8 * q + i] = __float2bfloat16(ah[i]);
-                X[m * K3 + 2 * C + 8 * q + i] = __float2bfloat16(av[i]);
-            }
-        }
-        __syncwarp();
-        for (int rt = 0; rt < TILE / 16; ++rt) {
-            for (int ct = 0; ct < C / 16; ++ct) {
-                wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
-                wmma::fill_fragment(acc, 0.f);
-#pragma unroll
-                for (int kc = 0; kc < K3 / 16; ++kc) {
-                    wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
-                    wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b;
-                    wmma::load_matrix_sync(a, X + rt * 16 * K3 + kc * 16, K3);
-                    wmma::load_matrix_sync(b, sW + kc * 16 * C + ct * 16, C);
-                    wmma::mma_sync(acc, a, b, acc);
-                }
-                wmma::store_matrix_sync(sC[w] + rt * 16 * C + ct * 16, acc, C, wmma::mem_row_major);
-            }
-        }
-        __syncwarp();
-        // epilogue: row m = lane, 32 channels
-        {
-            const int n = base + lane;
-            if (n < N) {
-                __align__(16) __nv_bfloat16 o[C];
-#pragma unroll
-                for (int c = 0; c < C; ++c) {
-                    const float u = sC[w][lane * C + c] + bias[c];
-                    o[c] = __float2bfloat16(u > 0.f ? u : 0.f);
-                }
-                const uint4 *src = reinterpret_cast<const uint4 *>(o);
-                uint4 *dst = reinterpret_cast<uint4 *>(Hout + (size_t)n * C);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) dst[i] = src[i];
-                if (Xs) {
-                    const uint4 *xs = reinterpret_cast<const uint4 *>(X + lane * K3);
-                    uint4 *xd = reinterpret_cast<uint4 *>(Xs + (size_t)n * K3);
-#pragma unroll
-                    for (int i = 0; i < K3 / 8; ++i) xd[i] = xs[i];
-                }
-            }
-        }
-        __syncwarp();
-    }
-}
-
-// ------------------------------------------------------------------ tcgen05 layer (forward)
-// One CTA of 256 threads takes tiles of 128 consecutive nodes.  Thread (warp w, lane l) owns node
-// row m = 32*(w%4) + l of the tile and channel half hf = w/4 (16 channels): it gathers its half of
-// the 96-wide layer input [h_n; A_h(h)_n; A_v(h)_n] and stores it to shared memory in the
-// canonical K-major layout of the tensor-core operands (8x8 BF16 core matrices of 128 contiguous
-// bytes; core (row group g, K chunk kc) at (kc*16 + g)*128 bytes), so the 32 lanes of a warp
-// write 512 contiguous bytes.  One thread then issues the 128x32x96 product X W^T as six
-// tcgen05.mma (kind::f16, BF16 operands, FP32 accumulator in tensor memory, 32 columns) and
-// commits it to an mbarrier; every thread waits, reads its row half back with tcgen05.ld
-// (warp w reads TMEM lanes 32*(w%4)..+31, columns 16*hf..+15), adds the bias, applies ReLU and
-// stores 32 bytes of BF16.
-constexpr int TCM = 128;                    // nodes per tile = TMEM lanes = UMMA M
-constexpr int TC_THREADS = 256;
+// ------------------------------------------------------------------ tensor-core operands
+// The layer transform X W^T (X: 128 rows x 96 BF16, W: 32 x 96 BF16) runs as six tcgen05.mma
+// (kind::f16, K = 16 each) with the FP32 accumulator in tensor memory (32 columns).  Both operands
+// sit in shared memory in the canonical K-major layout without swizzle: 8x8 BF16 core matrices of
+// 128 contiguous bytes, core (row group g, K chunk kc) at (kc*groups + g)*128 bytes.
+constexpr int TCM = 128;                    // rows per tile = TMEM lanes = UMMA M
 constexpr int TC_KC = K3 / 8;               // 12 K chunks of 8 channels
 constexpr uint32_t TC_A_LBO = 16 * 128;     // A: next K chunk (16 row groups of 128 B)
 constexpr uint32_t TC_B_LBO = 4 * 128;      // B: next K chunk (4 row groups)
@@ -249,24 +100,55 @@ __device__ __forceinline__ uint32_t tc_core_off(int row, int kc, int groups) {
     return (uint32_t)((kc * groups + (row >> 3)) * 128 + (row & 7) * 16);
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 3)
-k_nn_layer_tc(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __nv_bfloat16 *__restrict__ Wbf,
-              const float *__restrict__ bias, __nv_bfloat16 *__restrict__ Hout, __nv_bfloat16 *__restrict__ Xs,
-              int *__restrict__ err) {
-    __shared__ __align__(1024) uint8_t sA[TCM * K3 * 2];      // 24 KB
-    __shared__ __align__(1024) uint8_t sB[C * K3 * 2];        // 6 KB
-    __shared__ float sBias[C];
+// ------------------------------------------------------------------ column layer (forward)
+// One CTA of 4 warps per column (L <= 128 levels = one UMMA tile of M = 128 rows; rows L..127
+// stay zero).  Warp w owns channel octet w (8 channels) of rows k = lane, lane+32, ... (NS
+// slots), so for every horizontal face of the column (uniform for the CTA) a warp reads 16 bytes
+// of 32 consecutive neighbour rows — one contiguous block of the neighbour column — and keeps
+// NS such loads per face in flight.  The column's own rows are staged in shared memory, which
+// also serves the vertical aggregation (its two faces join adjacent rows).  The 96-wide inputs
+// go to shared memory in the canonical K-major operand layout, one thread issues the
+// 128x32x96 BF16 product (tcgen05.mma, FP32 accumulator in tensor memory), and in the epilogue
+// warp w reads TMEM lanes 32w..32w+31 (rows 32w + lane), all 32 columns: each thread holds a
+// whole output row.
+//   FIRST: the layer input h0 = relu(W_in x + b_in) is computed on the fly from the node
+//          features x (X0, FP32 [N][4]) of the column and of each neighbour;
+//   LAST:  the epilogue applies the output layer, y = w_out . h3 + b_out, q = z + y s / |b|,
+//          instead of storing h3 (kept only when training).
+// Training keeps H (h0 with FIRST, the layer output), Xs (the layer input rows) and Y.
+constexpr int COL_THREADS = 128;
+constexpr int COL_MAXL = 128;
+
+template <int NS, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(COL_THREADS)
+k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const float *__restrict__ X0,
+         const __nv_bfloat16 *__restrict__ Wbf, const float *__restrict__ prm, int layer,
+         const double *__restrict__ z, const double *__restrict__ sc,
+         __nv_bfloat16 *__restrict__ Hout, double *__restrict__ qd, float *__restrict__ qf,
+         __nv_bfloat16 *__restrict__ Hkeep0, __nv_bfloat16 *__restrict__ Xs, float *__restrict__ Y,
+         int *__restrict__ err) {
+    __shared__ __align__(1024) uint8_t sA[TCM * K3 * 2];          // 24 KB operand tile
+    __shared__ __align__(1024) uint8_t sB[C * K3 * 2];            // 6 KB weights
+    __shared__ __align__(16) __nv_bfloat16 sH[COL_MAXL * C];      // own rows (8 KB)
+    __shared__ float sBias[C], sWin[C * FIN + C], sWout[C + 1];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-    const int m = 32 * (w & 3) + lane, hf = w >> 2;
-    // weights W [C][K3] (row n = output channel, K contiguous) -> canonical layout, 16 B per thread
-    for (int i = tid; i < C * TC_KC; i += TC_THREADS) {
+    const int L = M.L;
+    const float *bias = prm + OFF_L0 + layer * LSTRIDE + C * K3;
+    for (int i = tid; i < C * TC_KC; i += COL_THREADS) {
         const int n = i / TC_KC, kc = i - n * TC_KC;
         *reinterpret_cast<uint4 *>(sB + tc_core_off(n, kc, C / 8)) =
             *reinterpret_cast<const uint4 *>(Wbf + (size_t)n * K3 + kc * 8);
     }
+    // rows L..127 of the operand tile are zero for every column
+    for (int i = tid; i < TCM * TC_KC; i += COL_THREADS) {
+        const int row = i / TC_KC, kc = i - row * TC_KC;
+        if (row >= L) *reinterpret_cast<uint4 *>(sA + tc_core_off(row, kc, TCM / 8)) = make_uint4(0, 0, 0, 0);
+    }
     if (tid < C) sBias[tid] = bias[tid];
+    if (FIRST) for (int i = tid; i < C * FIN + C; i += COL_THREADS) sWin[i] = prm[OFF_WIN + i];
+    if (LAST && tid <= C) sWout[tid] = prm[OFF_WOUT + tid];
     if (w == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      :: "r"(smem_u32(&tmem_base)), "r"(TC_TMEM_COLS));
@@ -282,77 +164,119 @@ k_nn_layer_tc(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base;
     const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
-    const int N = M.N;
-    const int ntiles = (N + TCM - 1) / TCM;
     uint32_t phase = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const int n = t * TCM + m;
-        // ---- gather: [h ; sum w (h_j - h)] for this thread's 16 channels
-        float ah[16], av[16];
-        B8 s0, s1;                                  // own row half, kept packed during the gather
+    // the first layer's input rows: h0 = bf16(relu(W_in x + b_in)), channels 8w..8w+7
+    auto h0_row = [&](const float4 x, float *o) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) { ah[i] = 0.f; av[i] = 0.f; }
+        for (int i = 0; i < 8; ++i) {
+            const int c = 8 * w + i;
+            float u = sWin[C * FIN + c] + sWin[c * FIN + 0] * x.x + sWin[c * FIN + 1] * x.y +
+                      sWin[c * FIN + 2] * x.z + sWin[c * FIN + 3] * x.w;
+            o[i] = __bfloat162float(__float2bfloat16(u > 0.f ? u : 0.f));
+        }
+    };
+    for (int c = blockIdx.x; c < M.NC && ok; c += gridDim.x) {
+        const int base = c * L;
+        // ---- own rows (octet w) into sH
 #pragma unroll
-        for (int i = 0; i < 4; ++i) { s0.v[i] = __floats2bfloat162_rn(0.f, 0.f); s1.v[i] = s0.v[i]; }
-        if (n < N) {
-            const int c = n / M.L, k = n - c * M.L;
-            const B8 *sp = reinterpret_cast<const B8 *>(Hin + (size_t)n * C + 16 * hf);
-            s0 = sp[0];
-            s1 = sp[1];
-            float wh = 0.f, wv = 0.f;
-            const float ih = G.iDh[n], iv = G.iDv[n];
-            for_faces(M, c, k, n,
-                [&](const Face &f) {
-                    RowB2 p;
-                    const B8 *src = reinterpret_cast<const B8 *>(Hin + (size_t)f.j * C + 16 * hf);
-                    p.a = src[0];
-                    p.b = src[1];
-                    p.t = face_T(M, G, f);
-                    return p;
-                },
-                [&](const Face &f, const RowB2 &p) {
-                    float hj[16];
-                    b8_to_f(p.a, hj);
-                    b8_to_f(p.b, hj + 8);
-                    if (f.vert) {
-                        const float wt = p.t * iv;
-                        wv += wt;
+        for (int s = 0; s < NS; ++s) {
+            const int k = lane + 32 * s;
+            if (k < L) {
+                B8 v;
+                if (FIRST) {
+                    float o[8];
+                    h0_row(*reinterpret_cast<const float4 *>(X0 + (size_t)(base + k) * FIN), o);
 #pragma unroll
-                        for (int i = 0; i < 16; ++i) av[i] += wt * hj[i];
-                    } else {
-                        const float wt = p.t * ih;
-                        wh += wt;
-#pragma unroll
-                        for (int i = 0; i < 16; ++i) ah[i] += wt * hj[i];
-                    }
-                });
-            float self[16];
-            b8_to_f(s0, self);
-            b8_to_f(s1, self + 8);
-#pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                ah[i] -= wh * self[i];
-                av[i] -= wv * self[i];
+                    for (int i = 0; i < 4; ++i) v.v[i] = __floats2bfloat162_rn(o[2 * i], o[2 * i + 1]);
+                    if (Hkeep0) *reinterpret_cast<B8 *>(Hkeep0 + (size_t)(base + k) * C + 8 * w) = v;
+                } else {
+                    v = *reinterpret_cast<const B8 *>(Hin + (size_t)(base + k) * C + 8 * w);
+                }
+                *reinterpret_cast<B8 *>(sH + k * C + 8 * w) = v;
             }
         }
-        // ---- operand tile: chunks (self: 2hf, 2hf+1), (A_h: 4+..), (A_v: 8+..)
+        // ---- horizontal aggregation: ah = sum_f w_f h_j, wsum = sum_f w_f
+        float ah[NS][8], wsum[NS], ih[NS];
 #pragma unroll
-        for (int part = 0; part < 3; ++part) {
+        for (int s = 0; s < NS; ++s) {
+            const int k = lane + 32 * s;
+            ih[s] = k < L ? G.iDh[base + k] : 0.f;
+            wsum[s] = 0.f;
 #pragma unroll
-            for (int h2 = 0; h2 < 2; ++h2) {
-                B8 o;
-                if (part == 0) {
-                    o = h2 ? s1 : s0;
-                } else {
-                    const float *src = part == 1 ? ah : av;
+            for (int i = 0; i < 8; ++i) ah[s][i] = 0.f;
+        }
+        const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
+        for (int j = beg; j < end; ++j) {
+            const int2 en = __ldg(&M.cadj[j]);
+            if (en.x < 0) continue;                      // vertical faces: below, from sH
+            const int e = en.x >> 1, nb = en.y * L;
+            uint4 v[NS];
+            float t[NS];
 #pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        o.v[i] = __floats2bfloat162_rn(src[8 * h2 + 2 * i], src[8 * h2 + 2 * i + 1]);
+            for (int s = 0; s < NS; ++s) {
+                const int k = lane + 32 * s;
+                if (k < L) {
+                    if (FIRST) v[s] = *reinterpret_cast<const uint4 *>(X0 + (size_t)(nb + k) * FIN);
+                    else v[s] = *reinterpret_cast<const uint4 *>(Hin + (size_t)(nb + k) * C + 8 * w);
+                    t[s] = G.Th[(size_t)e * L + k];
                 }
-                const int kc = 4 * part + 2 * hf + h2;
-                *reinterpret_cast<B8 *>(sA + tc_core_off(m, kc, TCM / 8)) = o;
-                if (Xs && n < N) *reinterpret_cast<B8 *>(Xs + (size_t)n * K3 + 8 * kc) = o;
+            }
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const int k = lane + 32 * s;
+                if (k >= L) continue;
+                float hj[8];
+                if (FIRST) h0_row(*reinterpret_cast<const float4 *>(&v[s]), hj);
+                else b8_to_f(*reinterpret_cast<const B8 *>(&v[s]), hj);
+                const float wt = t[s] * ih[s];
+                wsum[s] += wt;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) ah[s][i] += wt * hj[i];
+            }
+        }
+        __syncwarp();
+        // ---- operand rows: [h ; ah - wsum h ; av] for octet w
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int k = lane + 32 * s;
+            if (k >= L) continue;
+            const int n = base + k;
+            float hs[8], av[8];
+            b8_to_f(*reinterpret_cast<const B8 *>(sH + k * C + 8 * w), hs);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) av[i] = 0.f;
+            const float iv = G.iDv[n];
+            float wv = 0.f;
+            if (k > 0) {
+                float hb[8];
+                b8_to_f(*reinterpret_cast<const B8 *>(sH + (k - 1) * C + 8 * w), hb);
+                const float wt = G.Tv[n - 1] * iv;
+                wv += wt;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) av[i] += wt * hb[i];
+            }
+            if (k + 1 < L) {
+                float ha[8];
+                b8_to_f(*reinterpret_cast<const B8 *>(sH + (k + 1) * C + 8 * w), ha);
+                const float wt = G.Tv[n] * iv;
+                wv += wt;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) av[i] += wt * ha[i];
+            }
+            B8 o[3];
+            o[0] = *reinterpret_cast<const B8 *>(sH + k * C + 8 * w);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                o[1].v[i] = __floats2bfloat162_rn(ah[s][2 * i] - wsum[s] * hs[2 * i],
+                                                  ah[s][2 * i + 1] - wsum[s] * hs[2 * i + 1]);
+                o[2].v[i] = __floats2bfloat162_rn(av[2 * i] - wv * hs[2 * i], av[2 * i + 1] - wv * hs[2 * i + 1]);
+            }
+#pragma unroll
+            for (int part = 0; part < 3; ++part) {
+                const int kc = 4 * part + w;
+                *reinterpret_cast<B8 *>(sA + tc_core_off(k, kc, TCM / 8)) = o[part];
+                if (Xs) *reinterpret_cast<B8 *>(Xs + (size_t)n * K3 + 8 * kc) = o[part];
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -361,10 +285,10 @@ k_nn_layer_tc(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-            for (int s = 0; s < K3 / 16; ++s) {
-                const uint64_t ad = umma_desc(aBase + 2 * s * TC_A_LBO, TC_A_LBO, TC_SBO);
-                const uint64_t bd = umma_desc(bBase + 2 * s * TC_B_LBO, TC_B_LBO, TC_SBO);
-                const uint32_t acc = s > 0 ? 1u : 0u;
+            for (int st = 0; st < K3 / 16; ++st) {
+                const uint64_t ad = umma_desc(aBase + 2 * st * TC_A_LBO, TC_A_LBO, TC_SBO);
+                const uint64_t bd = umma_desc(bBase + 2 * st * TC_B_LBO, TC_B_LBO, TC_SBO);
+                const uint32_t acc = st > 0 ? 1u : 0u;
                 asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
                              :: "r"(tmem), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc));
@@ -372,7 +296,6 @@ k_nn_layer_tc(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          :: "r"(smem_u32(&bar)) : "memory");
         }
-        // ---- wait for the product (bounded)
         {
             uint32_t done = 0;
             long long spins = 0;
@@ -382,7 +305,6 @@ k_nn_layer_tc(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __
                              : "=r"(done) : "r"(smem_u32(&bar)), "r"(phase) : "memory");
                 if (!done && ++spins > TC_SPIN_MAX) break;
             }
-            // the whole CTA leaves together if any thread gave up
             if (__syncthreads_or(!done)) {
                 ok = false;
                 if (tid == 0) atomicExch(err, 1);
@@ -390,33 +312,57 @@ k_nn_layer_tc(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __
         }
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // ---- epilogue: TMEM lanes 32*(w%4).., columns 16*hf..
-        uint32_t r[16];
+        // ---- epilogue: row k = 32w + lane, 32 channels
+        uint32_t r[32];
         {
-            const uint32_t taddr = tmem + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)(16 * hf);
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-                         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            const uint32_t taddr = tmem + ((uint32_t)(32 * w) << 16);
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
                          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
                            "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-                           "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                           "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+                           "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+                           "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+                           "=r"(r[31])
                          : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         }
-        if (n < N) {
-            B8 o[2];
+        const int k = 32 * w + lane;
+        if (k < L) {
+            const int n = base + k;
+            B8 o[4];
+            float hv[C];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                float u0 = ok ? __uint_as_float(r[2 * i]) + sBias[16 * hf + 2 * i] : __int_as_float(0x7fc00000);
-                float u1 = ok ? __uint_as_float(r[2 * i + 1]) + sBias[16 * hf + 2 * i + 1] : __int_as_float(0x7fc00000);
+            for (int i = 0; i < C / 2; ++i) {
+                float u0 = ok ? __uint_as_float(r[2 * i]) + sBias[2 * i] : __int_as_float(0x7fc00000);
+                float u1 = ok ? __uint_as_float(r[2 * i + 1]) + sBias[2 * i + 1] : __int_as_float(0x7fc00000);
                 u0 = u0 > 0.f ? u0 : (u0 == u0 ? 0.f : u0);
                 u1 = u1 > 0.f ? u1 : (u1 == u1 ? 0.f : u1);
-                o[i >> 2].v[i & 3] = __floats2bfloat162_rn(u0, u1);
+                const __nv_bfloat162 b2 = __floats2bfloat162_rn(u0, u1);
+                o[i >> 2].v[i & 3] = b2;
+                const float2 f2 = __bfloat1622float2(b2);
+                hv[2 * i] = f2.x;
+                hv[2 * i + 1] = f2.y;
             }
-            B8 *dst = reinterpret_cast<B8 *>(Hout + (size_t)n * C + 16 * hf);
-            dst[0] = o[0];
-            dst[1] = o[1];
+            if (!LAST || Hout) {
+                B8 *dst = reinterpret_cast<B8 *>(Hout + (size_t)n * C);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) dst[i] = o[i];
+            }
+            if (LAST) {
+                float y = sWout[C];
+#pragma unroll
+                for (int i = 0; i < C; ++i) y += sWout[i] * hv[i];
+                if (Y) Y[n] = y;
+                const double sg = sc[0] > 0. ? sc[0] : 1.;
+                const double q = z[n] + (double)y * sg / (double)G.bdiag[n];
+                if (qd) qd[n] = q;
+                if (qf) qf[n] = (float)q;
+            }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();                                  // sH and sA are rewritten next
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -424,24 +370,18 @@ k_nn_layer_tc(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const __
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_TMEM_COLS));
 }
 
-// y = w_out . h3 + b_out;  q = z + y s / |b|;  with Y != null also keeps y
-__global__ void k_nn_output(int N, const __nv_bfloat16 *__restrict__ H3, const float *__restrict__ prm,
-                            const double *__restrict__ z, const double *__restrict__ sc, Geom G,
-                            float *__restrict__ Y, double *__restrict__ qd, float *__restrict__ qf) {
+// node features x = [r/s, z|b|/s, ln(Dv/Dh)/8, bnd] (FP32 [N][4])
+__global__ void k_nn_features(int N, const double *__restrict__ r, const double *__restrict__ z,
+                              const double *__restrict__ sc, Geom G, float *__restrict__ X0) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
-    float h[C];
-    const B8 *src = reinterpret_cast<const B8 *>(H3 + (size_t)n * C);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) b8_to_f(src[i], h + 8 * i);
-    float y = prm[OFF_BOUT];
-#pragma unroll
-    for (int c = 0; c < C; ++c) y += prm[OFF_WOUT + c] * h[c];
-    if (Y) Y[n] = y;
     const double s = sc[0] > 0. ? sc[0] : 1.;
-    const double q = z[n] + (double)y * s / (double)G.bdiag[n];
-    if (qd) qd[n] = q;
-    if (qf) qf[n] = (float)q;
+    float4 x;
+    x.x = (float)(r[n] / s);
+    x.y = (float)(z[n] * (double)G.bdiag[n] / s);
+    x.z = G.feat2[n];
+    x.w = G.bnd[n];
+    *reinterpret_cast<float4 *>(X0 + (size_t)n * FIN) = x;
 }
 
 // ---------------------------------------------------------------------------------- backward

@@ -45,14 +45,17 @@ __global__ void k_aun(ColMesh M, MpScratchT<T> S, U3 U) {
     if (t < nh) {
         const int e = t / M.L, k = t - e * M.L;
         const int a = S.e2a[e] * M.L + k, b = S.e2b[e] * M.L + k;
-        S.aunh[t] = face_aun<T>(U.u, a, b, SPick<T>::get(M, 0, false)[t], SPick<T>::get(M, 1, false)[t],
-                                SPick<T>::get(M, 2, false)[t]);
+        T sx, sy, sz;
+        FaceVec<T>::load(M, false, t, sx, sy, sz);
+        S.aunh[t] = face_aun<T>(U.u, a, b, sx, sy, sz);
     } else if (t < nh + M.N) {
         const int n = t - nh;
         const int k = n % M.L;
-        if (k + 1 < M.L)
-            S.aunv[n] = face_aun<T>(U.u, n, n + 1, SPick<T>::get(M, 0, true)[n], SPick<T>::get(M, 1, true)[n],
-                                    SPick<T>::get(M, 2, true)[n]);
+        if (k + 1 < M.L) {
+            T sx, sy, sz;
+            FaceVec<T>::load(M, true, n, sx, sy, sz);
+            S.aunv[n] = face_aun<T>(U.u, n, n + 1, sx, sy, sz);
+        }
     }
 }
 
@@ -97,8 +100,10 @@ __global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, T *__res
     T ax = 0., ay = 0., az = 0., hi = T(-1.e15), lo = T(1.e15);
     for_faces(M, c, k, n,
         [&](const Face &f) {
-            return V4T<T>{__ldg(SPick<T>::get(M, 0, f.vert) + f.si), __ldg(SPick<T>::get(M, 1, f.vert) + f.si),
-                          __ldg(SPick<T>::get(M, 2, f.vert) + f.si), psi1[f.j]};
+            V4T<T> v;
+            FaceVec<T>::load(M, f.vert, f.si, v.a, v.b, v.c);
+            v.d = psi1[f.j];
+            return v;
         },
         [&](const Face &f, const V4T<T> &v) {
             const T pj = v.d;

@@ -41,8 +41,8 @@ struct ColMesh {
     const int2 *cadj;        // [cptr[NC]]
     const double *Sh[3];     // [NE2*L]
     const double *Sv[3];     // [N]
-    const float *Shf[3];     // FP32 copies (mixed precision), may be null
-    const float *Svf[3];
+    const float4 *Shf4;      // FP32 copies (mixed precision) packed (x, y, z, 0): one 16-byte
+    const float4 *Svf4;      // load per face; may be null
     const int32_t *bptr;     // [NC+1] boundary entries per column
     const BEntry *bent;
     int32_t iper;            // 2: no boundary closure in derivative; 0: sbb closure

@@ -16,6 +16,7 @@ The network, its forward and backward passes and the Adam update live in the CUD
 """
 from __future__ import annotations
 
+import os
 import time
 
 import numpy as np
@@ -82,3 +83,62 @@ def compare(refmesh, params: RunParams, weights, steps: int = 5, warm: int = 2, 
             out[name] = {"iters_per_step": float(np.mean(its)), "ms_per_step": 1000 * dt / steps,
                          "fallbacks": fb, "u": s.get(F_UNK)}
     return out
+
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "learned_weights.npz")
+
+
+def train_seeds(nx: int = 256, levels: int = 81, seeds=range(8), steps: int = 8, every: int = 4,
+                max_records: int = 48, epochs: int = 2, lr: float = 2e-3, dt: float = 6.0, device: int = 0,
+                log=print):
+    """Training run of the learned preconditioner on the 256x256x81 workload family: one mesh per
+    seed (jittered columns, Agnesi hill with h0 drawn uniformly from 200-600 m), plain solves
+    harvested for `steps` steps each, weights carried from seed to seed.  Returns
+    (weights, plain_rate, history)."""
+    from . import mesh
+    rng = np.random.default_rng(1234)
+    w, hist, rates = None, [], []
+    for sd in seeds:
+        h0 = float(rng.uniform(200.0, 600.0))
+        cm = mesh.generate(nx, L=levels, seed=int(sd), h0=h0)
+        rm = cm.to_reference()
+        P = RunParams(delt=dt, lord=3, eps0=1e-8, itr=200, iprc=2, itrp1=1, lipps=1,
+                      strat=0.01 ** 2 / 9.80616)
+        w, h, rate = train(rm, P, steps=steps, every=every, max_records=max_records, epochs=epochs, lr=lr,
+                           seed=int(sd), device=device, init=w,
+                           log=(lambda e, sd=sd, h0=h0: log({"seed": sd, "h0": round(h0, 1), **e})) if log else None)
+        hist += h
+        rates.append(rate)
+    plain_rate = float(np.exp(np.mean(np.log(rates))))
+    return w, plain_rate, hist
+
+
+def save_weights(path, weights, plain_rate, meta):
+    np.savez(path, params=np.asarray(weights, np.float32), plain_rate=plain_rate, meta=str(meta))
+
+
+def load_weights(path=WEIGHTS):
+    """(params, plain_rate) of a saved training run."""
+    d = np.load(path)
+    return d["params"], float(d["plain_rate"])
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the learned preconditioner and save its weights")
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--levels", type=int, default=81)
+    ap.add_argument("--seeds", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=2)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--out", default=WEIGHTS)
+    a = ap.parse_args()
+    t0 = time.time()
+    w, rate, hist = train_seeds(a.nx, a.levels, range(a.seeds), a.steps, epochs=a.epochs, lr=a.lr,
+                                log=lambda e: print(json.dumps(e), flush=True))
+    meta = {"nx": a.nx, "levels": a.levels, "seeds": a.seeds, "steps": a.steps, "epochs": a.epochs, "lr": a.lr,
+            "pairs": int(sum(h["pairs"] for h in hist)), "train_s": round(time.time() - t0, 1)}
+    save_weights(a.out, w, rate, meta)
+    print(json.dumps({"saved": a.out, "plain_rate": rate, **meta}), flush=True)
