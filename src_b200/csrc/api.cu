@@ -480,7 +480,15 @@ int nn_alloc_train(mpg_handle h) {
 template <int NS>
 void nn_layers(mpg_handle h, const nn::Geom &G, double *qd, float *qf, bool train) {
     auto &S = h->nn;
-    const int nb = std::min(h->NC, 148 * 5);
+    // persistent grid: as many CTAs as fit on the device at once (tensor memory included)
+    static int per_sm = 0, sms = 0;
+    if (!per_sm) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nn::k_nn_col<NS, false, false>, nn::COL_THREADS, 0);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
+        per_sm = std::max(1, std::min(per_sm, 512 / (int)nn::TC_TMEM_COLS));
+        sms = std::max(1, sms);
+    }
+    const int nb = std::min(h->NC, sms * per_sm);
     const size_t W = (size_t)nn::C * nn::K3;
     nn::k_nn_col<NS, true, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
         h->M, G, nullptr, S.X0, S.Wbf, S.prm, 0, nullptr, nullptr, S.H[1], nullptr, nullptr,
