@@ -72,16 +72,17 @@ def compare(refmesh, params: RunParams, weights, steps: int = 5, warm: int = 2, 
             for _ in range(warm):
                 s.step(diag=False)
             s.synchronize()
-            its, fb = [], 0
+            its, first, fb = [], [], 0
             t0 = time.perf_counter()
             for _ in range(steps):
                 d = s.step()
                 its.append(d.niter1 + d.niter)
+                first.append(d.niter1)
                 fb += d.fallbacks
             s.synchronize()
             dt = time.perf_counter() - t0
-            out[name] = {"iters_per_step": float(np.mean(its)), "ms_per_step": 1000 * dt / steps,
-                         "fallbacks": fb, "u": s.get(F_UNK)}
+            out[name] = {"iters_per_step": float(np.mean(its)), "first_solve_iters": first,
+                         "ms_per_step": 1000 * dt / steps, "fallbacks": fb, "u": s.get(F_UNK)}
     return out
 
 
@@ -134,7 +135,20 @@ if __name__ == "__main__":
     ap.add_argument("--epochs", type=int, default=2)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--compare", action="store_true",
+                    help="instead of training: plain vs learned (saved weights) on one seeded mesh of this size")
     a = ap.parse_args()
+    if a.compare:
+        from . import mesh
+        w, rate = load_weights(a.out)
+        rm = mesh.generate(a.nx, L=a.levels, seed=0, h0=400.0).to_reference()
+        P = RunParams(delt=6.0, lord=3, eps0=1e-8, itr=200, itrp1=1, lipps=1, strat=0.01 ** 2 / 9.80616,
+                      nn_rate=rate)
+        res = compare(rm, P, w, steps=3, warm=1)
+        du = float(np.abs(res["learned"]["u"] - res["plain"]["u"]).max())
+        print(json.dumps({k: {kk: vv for kk, vv in v.items() if kk != "u"} for k, v in res.items()} |
+                         {"max_abs_du": du, "nn_rate": rate}), flush=True)
+        raise SystemExit(0)
     t0 = time.time()
     w, rate, hist = train_seeds(a.nx, a.levels, range(a.seeds), a.steps, epochs=a.epochs, lr=a.lr,
                                 log=lambda e: print(json.dumps(e), flush=True))
