@@ -78,6 +78,9 @@ typedef struct mpg_params {
                                   * iterations (m >= lord) is at most nn_rate^m times its initial
                                   * value; otherwise the plain line preconditioner takes over for
                                   * the rest of the solve.  <= 0 selects 0.98.                      */
+    int32_t itraj;               /* 1: velprd trajectory prediction of the advective velocity
+                                  * (ref.f:4448-4528) in set-up and every step; the reference
+                                  * hard-codes 0 (ref.f:111)                                       */
 } mpg_params;
 
 #define MPG_PREC_FP64  0
@@ -156,6 +159,7 @@ enum {
     MPG_F_THE    = 40,
     MPG_F_DTHEDZ = 41,
     MPG_F_D1     = 42,   /* /doperator/ d1 (compute_d_unstr)                                   */
+    MPG_F_UUU1   = 43,   /* uuu1(:,1..3) velprd's predicted velocity (itraj = 1)               */
     MPG_F_WORK   = 48,   /* 8 caller-usable work arrays MPG_F_WORK + 0..7                       */
     MPG_F_COUNT  = 56
 };
@@ -219,6 +223,8 @@ int mpg_half_forcing(mpg_handle h);                 /* ref.f:290-301 */
 int mpg_explicit_forcing(mpg_handle h, int mtri);   /* ref.f:323-359 */
 int mpg_post_solve(mpg_handle h, int mtri);         /* ref.f:367-383 */
 int mpg_extrapolate(mpg_handle h);                  /* ref.f:387-439 */
+/* velprd(unk, frc, uuu, uuu1, unkdash)                  ref.f:4448-4528 (itraj = 1 driver path) */
+int mpg_velprd(mpg_handle h);
 /* Last GCR statistics of the handle (/itero/). */
 int mpg_get_gcr_stats(mpg_handle h, mpg_gcr_stats *stats);
 /* Wait for all work of the handle. */
@@ -263,6 +269,22 @@ int mpg_learned_train_pair(mpg_handle h, int r, int t, float lr, double *loss);
 int mpg_learned_harvest(mpg_handle h, int every, int max_records);
 /* `epochs` passes of Adam steps over the recorded pairs (then the records are cleared) */
 int mpg_learned_train_records(mpg_handle h, int epochs, float lr, double *mean_loss, int *npairs);
+
+/* ---------------------------------------------------------------- restart files */
+/* MPG_RESTART_TEXT: the layout of Restart_Out_old / Restart_In_old (ref.f:4779-4890), one node per
+ * line in reference node order, F14.6 fields (lossy, as in the reference): uuu(:,1:3), uuu1(:,1:3)
+ * (velprd's array, zero: itraj = 0), unkdash(:,1:3), unk(:,1:4), frc(:,1:4), then
+ * prpot/rhs/cour/coefw, a list-directed line "nitsm icount" and one with ntime.  Reading restores
+ * those fields (uuu1 is skipped) and nitsm/icount, as Restart_In_old does (ref.f:277-278).
+ * MPG_RESTART_BINARY: every field the time step carries (unk incl. passive scalars, unk1, uuu,
+ * uuu0, frc, unkdash, prpot, rhs, cour) in FP64 with the counters, so a run continued from it is
+ * bit-identical to the uninterrupted one.  Either replaces mpg_setup for a restarted run.  `path`
+ * is a NUL-terminated file name; `ntime` is the step number written (read back into *ntime when
+ * the file holds it; may be NULL). */
+#define MPG_RESTART_TEXT   0
+#define MPG_RESTART_BINARY 1
+int mpg_restart_write(mpg_handle h, const char *path, int format, int ntime);
+int mpg_restart_read(mpg_handle h, const char *path, int format, int *ntime);
 
 /* ---------------------------------------------------------------- allocation-free laplc */
 /* laplc(press, alap, impfl) for callers that must not allocate device memory at call time: a

@@ -942,6 +942,52 @@ static void compute_d(orc *o) {
     free(dix); free(diy); free(diz);
 }
 
+/* ------------------------------------------------------------------ velprd ref.f:4448-4528 */
+void orc_velprd(orc *o) {
+    int n = o->npoin;
+    double **f = o->f;
+    double *rh0 = f[MPG_F_RH0], *ts = o->timestp, *vol = o->vol;
+    double *unk[3] = {f[MPG_F_UNK], f[MPG_F_UNK + 1], f[MPG_F_UNK + 2]};
+    double *frc[3] = {f[MPG_F_FRC], f[MPG_F_FRC + 1], f[MPG_F_FRC + 2]};
+    double *uuu[3] = {f[MPG_F_UUU], f[MPG_F_UUU + 1], f[MPG_F_UUU + 2]};
+    double *ud[3] = {f[MPG_F_UNKDASH], f[MPG_F_UNKDASH + 1], f[MPG_F_UNKDASH + 2]};
+    double *u1[3] = {f[MPG_F_UUU1], f[MPG_F_UUU1 + 1], f[MPG_F_UUU1 + 2]};
+    double *ff1 = dz(n), *ff2 = dz(n), *ff3 = dz(n), *pp = dz(n);
+    for (int ip = 0; ip < n; ++ip)
+        for (int k = 0; k < 3; ++k) ud[k][ip] = unk[k][ip] + ts[ip] * frc[k][ip];
+    for (int k = 0; k < 3; ++k) {                              /* ref.f:4466-4505, isfera = 0 */
+        orc_derivative(o, ud[k], ff1, 1);
+        orc_derivative(o, ud[k], ff2, 2);
+        orc_derivative(o, ud[k], ff3, 3);
+        for (int ip = 0; ip < n; ++ip) {
+            ff1[ip] = ff1[ip] / vol[ip];
+            ff2[ip] = ff2[ip] / vol[ip];
+            ff3[ip] = ff3[ip] / vol[ip];
+        }
+        for (int ip = 0; ip < n; ++ip)
+            u1[k][ip] = ud[k][ip] - ts[ip] * (uuu[0][ip] * ff1[ip] + uuu[1][ip] * ff2[ip] + uuu[2][ip] * ff3[ip]);
+    }
+    for (int ip = 0; ip < n; ++ip) {
+        u1[0][ip] = u1[0][ip] / (o->gmm[ip] * o->cosa[ip]);
+        u1[1][ip] = u1[1][ip] / o->gmm[ip];
+        pp[ip] = 0.;
+        ff1[ip] = 0.;
+        ff2[ip] = 0.;
+        ff3[ip] = 0.;
+    }
+    orc_gcrk(o, pp, u1[0], u1[1], u1[2], ff1, ff2, ff3, 0, NULL);
+    orc_prfr(o, pp, u1[0], u1[1], u1[2], ff1, ff2, ff3, 0);
+    for (int ip = 0; ip < n; ++ip) {                           /* ref.f:4517-4526 */
+        uuu[0][ip] = (uuu[0][ip] + ff1[ip]) * 0.5 * rh0[ip];
+        uuu[1][ip] = (uuu[1][ip] + ff2[ip]) * 0.5 * rh0[ip];
+        uuu[2][ip] = (uuu[2][ip] + ff3[ip]) * 0.5 * rh0[ip];
+        ud[0][ip] = ff1[ip] * o->gmm[ip] * o->cosa[ip];
+        ud[1][ip] = ff2[ip] * o->gmm[ip];
+        ud[2][ip] = ff3[ip];
+    }
+    free(ff1); free(ff2); free(ff3); free(pp);
+}
+
 /* ------------------------------------------------------------------ mpsolver set-up ref.f:99-273 */
 void orc_setup(orc *o, mpg_diag *diag) {
     int n = o->npoin;
@@ -999,11 +1045,15 @@ void orc_setup(orc *o, mpg_diag *diag) {
         coefw[ip] = 1. + 0.25 * (o->timestp[0] * o->timestp[0]) * gth0 * dthedz[ip];
         coefw[ip] = 1. / coefw[ip];
     }
-    for (int ip = 0; ip < n; ++ip) {                           /* itraj = 0, ref.f:258-266 */
-        for (int k = 0; k < 3; ++k) {
-            f[MPG_F_UUU + k][ip] = f[MPG_F_UUU + k][ip] * rh0[ip];
-            f[MPG_F_UNKDASH + k][ip] = f[MPG_F_UNK + k][ip];
+    if (P->itraj == 0) {
+        for (int ip = 0; ip < n; ++ip) {                       /* ref.f:258-266 */
+            for (int k = 0; k < 3; ++k) {
+                f[MPG_F_UUU + k][ip] = f[MPG_F_UUU + k][ip] * rh0[ip];
+                f[MPG_F_UNKDASH + k][ip] = f[MPG_F_UNK + k][ip];
+            }
         }
+    } else {
+        orc_velprd(o);                                         /* ref.f:267-268 */
     }
     mpg_diag dd;
     memset(&dd, 0, sizeof dd);
@@ -1091,6 +1141,7 @@ void orc_step(orc *o, mpg_diag *diag) {
         frc[1][ip] = frc[1][ip] + frm2;
         frc[2][ip] = frc[2][ip] + frm3;
         frc[3][ip] = frc[3][ip] + frm4;
+        if (P->itraj != 0) continue;
         for (int k = 0; k < 3; ++k) uuu[k][ip] = 1.5 * uuu[k][ip] * rh0[ip] - 0.5 * uuu0[k][ip];
         double rhoi = 1. / rh0[ip];
         uuu0[0][ip] = uuu0[0][ip] * rhoi * o->gmm[ip] * o->cosa[ip];
@@ -1098,6 +1149,7 @@ void orc_step(orc *o, mpg_diag *diag) {
         uuu0[2][ip] = uuu0[2][ip] * rhoi;
         for (int k = 0; k < 3; ++k) ud[k][ip] = 2. * unk[k][ip] - uuu0[k][ip];
     }
+    if (P->itraj != 0) orc_velprd(o);                          /* ref.f:441-442 */
     mpg_diag dd;                                               /* ref.f:456-459 */
     memset(&dd, 0, sizeof dd);
     orc_div(o, uuu[0], uuu[1], uuu[2], f[MPG_F_RHS], 1, &dd);

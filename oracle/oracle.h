@@ -49,6 +49,7 @@ void orc_courant(orc *o, int iflag, mpg_diag *diag);
 void orc_stats(orc *o, mpg_diag *diag);
 void orc_setup(orc *o, mpg_diag *diag);
 void orc_step(orc *o, mpg_diag *diag);
+void orc_velprd(orc *o);                          /* velprd, ref.f:4448-4528 */
 void orc_get_gcr_stats(orc *o, mpg_gcr_stats *st);
 double orc_beta(orc *o);            /* betaunstr1 */
 /* vertical-line preconditioner alone: z = M^{-1} rhs (coefficients for impfl) */

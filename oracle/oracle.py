@@ -49,6 +49,7 @@ def lib():
         L.orc_stats.argtypes = [vp, vp]
         L.orc_setup.argtypes = [vp, vp]
         L.orc_step.argtypes = [vp, vp]
+        L.orc_velprd.argtypes = [vp]
         L.orc_get_gcr_stats.argtypes = [vp, vp]
         L.orc_beta.restype = C.c_double
         L.orc_beta.argtypes = [vp]
@@ -151,6 +152,9 @@ class Oracle:
         return u
 
     # ---- driver
+    def velprd(self) -> None:
+        self.L.orc_velprd(self.h)
+
     def setup(self) -> MpgDiag:
         d = MpgDiag()
         self.L.orc_setup(self.h, C.byref(d))

@@ -31,7 +31,8 @@ EXPORTS = [
     "mpg_synchronize", "mpg_analyze_mesh", "mpg_get_stream", "mpg_kernel_timing", "mpg_kernel_times",
     "mpg_laplc_noalloc", "mpg_learned_init", "mpg_learned_set_params", "mpg_learned_get_params",
     "mpg_learned_forward", "mpg_learned_grad", "mpg_learned_train_pair", "mpg_learned_harvest",
-    "mpg_learned_train_records", "mpg_learned_loss", "mpg_laplc_adjoint",
+    "mpg_learned_train_records", "mpg_learned_loss", "mpg_laplc_adjoint", "mpg_restart_write",
+    "mpg_restart_read", "mpg_velprd",
 ]
 NPARAM = 9505
 
@@ -89,6 +90,9 @@ def lib():
         L.mpg_learned_harvest.argtypes = [vp, ip, ip]
         L.mpg_learned_train_records.argtypes = [vp, ip, C.c_float, C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.mpg_learned_loss.argtypes = [vp, ip]
+        L.mpg_restart_write.argtypes = [vp, C.c_char_p, ip, ip]
+        L.mpg_velprd.argtypes = [vp]
+        L.mpg_restart_read.argtypes = [vp, C.c_char_p, ip, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -96,6 +100,11 @@ def lib():
 def _check(rc):
     if rc != 0:
         raise MpgError(rc, lib().mpg_last_error().decode())
+
+
+def reference_restart_name(ntime: int) -> str:
+    """File name Restart_Out_old gives step `ntime`: 'Rstart_Out' // i9 // '.d' (ref.f:4794-4796)."""
+    return "Rstart_Out%9d.d" % ntime
 
 
 def analyze_mesh(refmesh) -> dict:
@@ -211,8 +220,23 @@ class Solver:
         _check(self.L.mpg_step(self.h, C.byref(d) if diag else None))
         return d
 
+    def velprd(self) -> None:
+        """velprd (ref.f:4448): trajectory prediction of the advective velocity (itraj = 1 path)."""
+        _check(self.L.mpg_velprd(self.h))
+
     def synchronize(self) -> None:
         _check(self.L.mpg_synchronize(self.h))
+
+    # ---------------------------------------------------------------- restart files
+    def restart_write(self, path: str, fmt: int = 0, ntime: int = 0) -> None:
+        """Restart_Out_old (fmt 0: the reference's F14.6 text layout) or the lossless binary form (1)."""
+        _check(self.L.mpg_restart_write(self.h, os.fsencode(path), fmt, ntime))
+
+    def restart_read(self, path: str, fmt: int = 0) -> int:
+        """Restart_In_old (fmt 0) or the binary form (1); returns the step number stored in the file."""
+        nt = C.c_int()
+        _check(self.L.mpg_restart_read(self.h, os.fsencode(path), fmt, C.byref(nt)))
+        return nt.value
 
     # ---------------------------------------------------------------- learned preconditioner
     def learned_init(self, seed: int = 0) -> None:

@@ -31,7 +31,7 @@ class MpgParams(C.Structure):
         ("implgw", C.c_int32), ("lipps", C.c_int32),
         ("strat", C.c_double), ("tetbar", C.c_double), ("g", C.c_double),
         ("iprc", C.c_int32), ("nscal", C.c_int32), ("precision", C.c_int32), ("itmn", C.c_int32),
-        ("nn_rate", C.c_double),
+        ("nn_rate", C.c_double), ("itraj", C.c_int32),
     ]
 
 
@@ -96,6 +96,7 @@ class MpgInfo(C.Structure):
 # field ids (include/mpgcr.h)
 F_UNK, F_UNK1, F_UUU, F_UUU0, F_FRC, F_UNKDASH = 0, 16, 20, 23, 26, 30
 F_PRPOT, F_RHS, F_COUR, F_ALPHA, F_COEFW, F_RH0, F_TH0, F_THE, F_DTHEDZ, F_D1 = range(33, 43)
+F_UUU1 = 43
 F_WORK = 48
 F_COUNT = 56
 
@@ -148,6 +149,7 @@ class RunParams:
     precision: int = 0
     itmn: int = 3
     nn_rate: float = 0.0
+    itraj: int = 0
 
     def to_c(self) -> MpgParams:
         p = MpgParams()

@@ -49,7 +49,7 @@ struct mpg_solver {
     mpg_params P{};
     int dev = 0;
     cudaStream_t st = nullptr;
-    int32_t NC = 0, L = 0, N = 0, NE2 = 0, kch = 1;
+    int32_t NC = 0, L = 0, N = 0, NE2 = 0;
     bool bitwise = true;
     ColMesh M{};
     std::vector<void *> allocs;
@@ -70,6 +70,7 @@ struct mpg_solver {
     // line preconditioner
     double *la[2] = {}, *lm[2] = {}, *lcp[2] = {};   // a, 1/m, c' (interleaved)
     double *dbuf = nullptr;                          // forward-sweep values (interleaved)
+    double *vp[4] = {};                              // velprd: its potential and velocity
     // MPDATA scratch
     MpScratch S{};
     double *psi1 = nullptr, *g3[3] = {}, *mx = nullptr, *mn = nullptr;
@@ -237,9 +238,25 @@ template <> struct Buf<float> {
     static const float *coefw(mpg_handle h) { return h->coefwf; }
 };
 
+#ifndef MPG_LAP_PAIRS
+#define MPG_LAP_PAIRS 0
+#endif
 template <class T>
 int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
     using B = Buf<T>;
+    if (MPG_LAP_PAIRS) {
+        const int PL = (h->L + 1) / 2, nt = h->NC * PL;
+        {
+            KTIME(KT_LAP_GRAD);
+            k_lap_grad2<T><<<grid(nt), kThreads, 0, h->st>>>(h->M, PL, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
+                                                            (T)h->P.delt, impfl, B::F(h));
+        }
+        {
+            KTIME(KT_LAP_DIV);
+            k_lap_div2<T><<<grid(nt), kThreads, 0, h->st>>>(h->M, PL, B::F(h), B::vol(h), B::rh0(h), alap);
+        }
+        return check_launch("laplc");
+    }
     {
         KTIME(KT_LAP_GRAD);
         k_lap_grad<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
@@ -1051,6 +1068,39 @@ Fields make_fields(mpg_handle h) {
     return F;
 }
 
+// ------------------------------------------------------------------------------ velprd
+// velprd(unk, frc, uuu, uuu1, unkdash) (ref.f:4448-4528): a first-order prediction of the velocity,
+// made divergence-free by its own potential solve (gcrk + prfr with impfl = 0, from p = 0)
+int op_velprd(mpg_handle h) {
+    const int N = h->N;
+    Fields F = make_fields(h);
+    double *u1[3];
+    for (int q = 0; q < 3; ++q)
+        if (!(u1[q] = fld(h, MPG_F_UUU1 + q))) return mpg_fail(MPG_ERR_NOMEM, "uuu1");
+    int rc;
+    if (!h->vp[0])
+        for (int q = 0; q < 4; ++q)
+            if ((rc = dalloc(h, &h->vp[q], (size_t)N))) return rc;
+    double *pp = h->vp[0], *ff[3] = {h->vp[1], h->vp[2], h->vp[3]};
+    {
+        KTIME(KT_NODE);
+        k_velprd_pre<<<grid(N), kThreads, 0, h->st>>>(N, F, h->P.delt);
+        const U3 U{{F.uuu[0], F.uuu[1], F.uuu[2]}};
+        for (int q = 0; q < 3; ++q)
+            k_velprd_grad<<<grid(N), kThreads, 0, h->st>>>(h->M, F.ud[q], h->vol, U, h->P.delt, u1[q]);
+        k_fill<<<grid(N), kThreads, 0, h->st>>>(N, pp, 0.0);
+        for (int q = 0; q < 3; ++q) k_fill<<<grid(N), kThreads, 0, h->st>>>(N, ff[q], 0.0);
+    }
+    if ((rc = check_launch("velprd"))) return rc;
+    if ((rc = op_gcrk(h, pp, u1[0], u1[1], u1[2], ff[0], ff[1], ff[2], 0))) return rc;
+    if ((rc = op_prfr(h, pp, u1[0], u1[1], u1[2], ff[0], ff[1], ff[2], 0))) return rc;
+    {
+        KTIME(KT_NODE);
+        k_velprd_post<<<grid(N), kThreads, 0, h->st>>>(N, F, ff[0], ff[1], ff[2]);
+    }
+    return check_launch("velprd post");
+}
+
 // ------------------------------------------------------------------------------ diagnostics
 struct ProdDivStats {
     const double *rhs;
@@ -1232,7 +1282,6 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     if (e != cudaSuccess) { delete h; return mpg_fail(MPG_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e)); }
     h->NC = hm.NC; h->L = hm.L; h->N = hm.N; h->NE2 = hm.NE2;
     if (hm.L > 128) { delete h; return mpg_fail(MPG_ERR_MESH, "more than 128 levels per column"); }
-    h->kch = (hm.L + 31) / 32;
     h->bitwise = hm.bitwise_order;
     h->betaunstr1 = h->hs.betaunstr1;
     h->iperm = hm.iperm;
@@ -1545,9 +1594,10 @@ extern "C" int mpg_setup(mpg_handle h, mpg_diag *diag) {
     if ((rc = op_prfr(h, prpot, F.unk1[0], F.unk1[1], F.unk1[2], F.unk[0], F.unk[1], F.unk[2], 0))) return rc;
     {
         KTIME(KT_NODE);
-        k_setup_post<<<grid(N), kThreads, 0, h->st>>>(N, F, prpot);
+        k_setup_post<<<grid(N), kThreads, 0, h->st>>>(N, F, prpot, h->P.itraj);
     }
     if ((rc = check_launch("setup post"))) return rc;
+    if (h->P.itraj != 0 && (rc = op_velprd(h))) return rc;
     if ((rc = step_diag(h, diag))) return rc;
     MPG_CUDA(cudaStreamSynchronize(h->st));
     if (h->gstatus == MPG_GCR_NAN) return mpg_fail(MPG_ERR_NUMERIC, "setup: NaN in the potential-flow solve");
@@ -1594,9 +1644,16 @@ extern "C" int mpg_extrapolate(mpg_handle h) {
     Fields F = make_fields(h);
     {
         KTIME(KT_NODE);
-        k_extrapolate<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, fcr2_of(), fcr3_of(), 1.0);
+        k_extrapolate<<<grid(h->N), kThreads, 0, h->st>>>(h->N, F, fcr2_of(), fcr3_of(), 1.0, h->P.itraj);
     }
-    return check_launch("extrapolate");
+    int rc = check_launch("extrapolate");
+    if (!rc && h->P.itraj != 0) rc = op_velprd(h);
+    return rc;
+}
+
+extern "C" int mpg_velprd(mpg_handle h) {
+    if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
+    return op_velprd(h);
 }
 
 // One pass of DO ITIME (ref.f:285-463), driving the entry points above in mpsolver's order.
@@ -1742,6 +1799,161 @@ extern "C" int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap
     k_lap_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, F, h->vol, h->f[MPG_F_RH0], aout);
     k_gather_perm<<<grid(N), kThreads, 0, h->st>>>(N, h->d_perm, aout, alap);
     return check_launch("laplc_noalloc");
+}
+
+// ------------------------------------------------------------------------------ restart files
+#include <fstream>
+
+namespace {
+
+// Fortran's F14.6 edit: right-justified in 14 characters with 6 decimals; a value that does not
+// fit (or is not finite) prints as 14 asterisks
+void put_f14_6(std::string &out, double v) {
+    char b[64];
+    const int n = std::snprintf(b, sizeof b, "%14.6f", v);
+    if (n != 14 || !std::isfinite(v)) out.append(14, '*');
+    else out.append(b, 14);
+}
+bool get_f14_6(const std::string &line, int i, double &v) {
+    if (line.size() < (size_t)(14 * (i + 1))) return false;
+    const std::string f = line.substr((size_t)14 * i, 14);
+    if (f.find('*') != std::string::npos) return false;
+    char *end = nullptr;
+    v = std::strtod(f.c_str(), &end);
+    return end != f.c_str();
+}
+
+// the blocks of Restart_Out_old (ref.f:4797-4816): field ids per column, -1 = uuu1 (zero)
+const int kRestartText[6][4] = {
+    {MPG_F_UUU, MPG_F_UUU + 1, MPG_F_UUU + 2, -2},
+    {-1, -1, -1, -2},
+    {MPG_F_UNKDASH, MPG_F_UNKDASH + 1, MPG_F_UNKDASH + 2, -2},
+    {MPG_F_UNK, MPG_F_UNK + 1, MPG_F_UNK + 2, MPG_F_UNK + 3},
+    {MPG_F_FRC, MPG_F_FRC + 1, MPG_F_FRC + 2, MPG_F_FRC + 3},
+    {MPG_F_PRPOT, MPG_F_RHS, MPG_F_COUR, MPG_F_COEFW}};
+
+struct RestartHeader {
+    char magic[8];
+    int32_t npoin, nscal, nitsm, icount, ntime, nfields;
+};
+
+std::vector<int> restart_binary_fields(mpg_handle h) {
+    std::vector<int> f;
+    for (int q = 0; q < 4 + h->P.nscal; ++q) f.push_back(MPG_F_UNK + q);
+    for (int q = 0; q < 4; ++q) f.push_back(MPG_F_UNK1 + q);
+    for (int q = 0; q < 3; ++q) { f.push_back(MPG_F_UUU + q); f.push_back(MPG_F_UUU0 + q); f.push_back(MPG_F_UNKDASH + q); }
+    for (int q = 0; q < 4; ++q) f.push_back(MPG_F_FRC + q);
+    f.push_back(MPG_F_PRPOT);
+    f.push_back(MPG_F_RHS);
+    f.push_back(MPG_F_COUR);
+    return f;
+}
+
+}  // namespace
+
+extern "C" int mpg_restart_write(mpg_handle h, const char *path, int format, int ntime) {
+    if (!h || !path) return mpg_fail(MPG_ERR_ARG, "null argument");
+    const size_t N = (size_t)h->N;
+    int rc;
+    if (format == MPG_RESTART_BINARY) {
+        std::FILE *fp = std::fopen(path, "wb");
+        if (!fp) return mpg_fail(MPG_ERR_ARG, std::string("restart: cannot open ") + path);
+        const std::vector<int> fids = restart_binary_fields(h);
+        RestartHeader hd{};
+        std::memcpy(hd.magic, "MPGRST01", 8);
+        hd.npoin = h->N; hd.nscal = h->P.nscal; hd.nitsm = h->nitsm; hd.icount = h->icount; hd.ntime = ntime;
+        hd.nfields = (int32_t)fids.size();
+        bool ok = std::fwrite(&hd, sizeof hd, 1, fp) == 1;
+        std::vector<double> v(N);
+        for (int fid : fids) {
+            if ((rc = mpg_get_field(h, fid, v.data()))) { std::fclose(fp); return rc; }
+            const int32_t id = fid;
+            ok = ok && std::fwrite(&id, sizeof id, 1, fp) == 1 && std::fwrite(v.data(), sizeof(double), N, fp) == N;
+        }
+        ok = (std::fclose(fp) == 0) && ok;
+        return ok ? MPG_OK : mpg_fail(MPG_ERR_ARG, std::string("restart: write failed on ") + path);
+    }
+    if (format != MPG_RESTART_TEXT) return mpg_fail(MPG_ERR_ARG, "restart: unknown format");
+    std::vector<std::vector<double>> col(4, std::vector<double>(N));
+    std::FILE *fp = std::fopen(path, "w");
+    if (!fp) return mpg_fail(MPG_ERR_ARG, std::string("restart: cannot open ") + path);
+    bool ok = true;
+    std::string line;
+    for (int b = 0; b < 6 && ok; ++b) {
+        const int ncol = kRestartText[b][3] == -2 ? 3 : 4;
+        for (int j = 0; j < ncol; ++j) {
+            const int fid = kRestartText[b][j];
+            if (fid < 0) std::fill(col[j].begin(), col[j].end(), 0.);
+            else if ((rc = mpg_get_field(h, fid, col[j].data()))) { std::fclose(fp); return rc; }
+        }
+        for (size_t ip = 0; ip < N && ok; ++ip) {        // ref.f:4797-4816, formats 198/199
+            line.clear();
+            for (int j = 0; j < ncol; ++j) put_f14_6(line, col[j][ip]);
+            line.push_back('\n');
+            ok = std::fwrite(line.data(), 1, line.size(), fp) == line.size();
+        }
+    }
+    ok = ok && std::fprintf(fp, " %11d %11d\n", h->nitsm, h->icount) > 0;   // write(nfid,*) n1, n2
+    ok = ok && std::fprintf(fp, " %11d\n", ntime) > 0;                        // write(nfid,*) ntime8+ntimet
+    ok = (std::fclose(fp) == 0) && ok;
+    return ok ? MPG_OK : mpg_fail(MPG_ERR_ARG, std::string("restart: write failed on ") + path);
+}
+
+extern "C" int mpg_restart_read(mpg_handle h, const char *path, int format, int *ntime) {
+    if (!h || !path) return mpg_fail(MPG_ERR_ARG, "null argument");
+    const size_t N = (size_t)h->N;
+    int rc;
+    if (format == MPG_RESTART_BINARY) {
+        std::FILE *fp = std::fopen(path, "rb");
+        if (!fp) return mpg_fail(MPG_ERR_ARG, std::string("restart: cannot open ") + path);
+        RestartHeader hd{};
+        if (std::fread(&hd, sizeof hd, 1, fp) != 1 || std::memcmp(hd.magic, "MPGRST01", 8) != 0) {
+            std::fclose(fp);
+            return mpg_fail(MPG_ERR_ARG, std::string("restart: not a binary restart file: ") + path);
+        }
+        if (hd.npoin != h->N || hd.nscal != h->P.nscal) {
+            std::fclose(fp);
+            return mpg_fail(MPG_ERR_ARG, "restart: file written for another mesh or scalar count");
+        }
+        std::vector<double> v(N);
+        for (int i = 0; i < hd.nfields; ++i) {
+            int32_t fid = -1;
+            if (std::fread(&fid, sizeof fid, 1, fp) != 1 || std::fread(v.data(), sizeof(double), N, fp) != N) {
+                std::fclose(fp);
+                return mpg_fail(MPG_ERR_ARG, std::string("restart: truncated file ") + path);
+            }
+            if ((rc = mpg_set_field(h, fid, v.data()))) { std::fclose(fp); return rc; }
+        }
+        std::fclose(fp);
+        h->nitsm = hd.nitsm;
+        h->icount = hd.icount;
+        if (ntime) *ntime = hd.ntime;
+        return MPG_OK;
+    }
+    if (format != MPG_RESTART_TEXT) return mpg_fail(MPG_ERR_ARG, "restart: unknown format");
+    std::ifstream in(path);
+    if (!in) return mpg_fail(MPG_ERR_ARG, std::string("restart: cannot open ") + path);
+    std::vector<std::vector<double>> col(4, std::vector<double>(N));
+    std::string line;
+    for (int b = 0; b < 6; ++b) {                        // ref.f:4855-4873
+        const int ncol = kRestartText[b][3] == -2 ? 3 : 4;
+        for (size_t ip = 0; ip < N; ++ip) {
+            bool ok = (bool)std::getline(in, line);
+            for (int j = 0; j < ncol && ok; ++j) ok = get_f14_6(line, j, col[j][ip]);
+            if (!ok)
+                return mpg_fail(MPG_ERR_ARG, "restart: unreadable line " + std::to_string((size_t)b * N + ip + 1) +
+                                             " of " + path);
+        }
+        for (int j = 0; j < ncol; ++j)
+            if (kRestartText[b][j] >= 0 && (rc = mpg_set_field(h, kRestartText[b][j], col[j].data()))) return rc;
+    }
+    int n1 = 0, n2 = 0, nt = 0;
+    if (!std::getline(in, line) || std::sscanf(line.c_str(), "%d %d", &n1, &n2) != 2)   // read(nfid,*) n1, n2
+        return mpg_fail(MPG_ERR_ARG, std::string("restart: missing nitsm/icount in ") + path);
+    h->nitsm = n1;
+    h->icount = n2;
+    if (ntime) *ntime = (std::getline(in, line) && std::sscanf(line.c_str(), "%d", &nt) == 1) ? nt : 0;
+    return MPG_OK;
 }
 
 // ------------------------------------------------------------------------------ learned preconditioner API

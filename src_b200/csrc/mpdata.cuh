@@ -259,7 +259,7 @@ __global__ void k_post_solve(int N, Fields F, double dt, double g, int last) {
 }
 
 // ref.f:387-439 (iblatt = 0, itraj = 0)
-__global__ void k_extrapolate(int N, Fields F, double fcr2, double fcr3, double ideep) {
+__global__ void k_extrapolate(int N, Fields F, double fcr2, double fcr3, double ideep, int itraj) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
     const double u0 = F.unk[0][n], u1 = F.unk[1][n], u2 = F.unk[2][n], u3 = F.unk[3][n];
@@ -273,6 +273,7 @@ __global__ void k_extrapolate(int N, Fields F, double fcr2, double fcr3, double 
     F.frc[1][n] = F.frc[1][n] + frm2;
     F.frc[2][n] = F.frc[2][n] + frm3;
     F.frc[3][n] = F.frc[3][n] + frm4;
+    if (itraj != 0) return;                       // velprd follows (ref.f:441-442)
     const double r = F.rh0[n];
     double o[3];
     for (int q = 0; q < 3; ++q) {
@@ -304,7 +305,7 @@ __global__ void k_setup_ambient(int N, Fields F, double *prpot, double *unk1_3) 
     prpot[n] = 0.;
 }
 
-__global__ void k_setup_post(int N, Fields F, double *prpot) {
+__global__ void k_setup_post(int N, Fields F, double *prpot, int itraj) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
     for (int q = 0; q < 3; ++q) F.uuu[q][n] = F.unk[q][n];
@@ -312,10 +313,40 @@ __global__ void k_setup_post(int N, Fields F, double *prpot) {
     F.unk[1][n] = F.unk[1][n] * 1.0;
     prpot[n] = 0.;
     for (int q = 0; q < 4; ++q) F.frc[q][n] = 0.;
+    if (itraj != 0) return;                       // velprd follows (ref.f:267-268)
     const double r = F.rh0[n];
     for (int q = 0; q < 3; ++q) {
         F.uuu[q][n] = F.uuu[q][n] * r;
         F.ud[q][n] = F.unk[q][n];
+    }
+}
+
+// velprd (ref.f:4448-4528), isfera = 0 (gmm = cosa = 1):
+// unkdash = unk + dt frc (ref.f:4461-4465)
+__global__ void k_velprd_pre(int N, Fields F, double dt) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    for (int q = 0; q < 3; ++q) F.ud[q][n] = F.unk[q][n] + dt * F.frc[q][n];
+}
+// uuu1(:,q) = unkdash(:,q) - dt (uuu . grad unkdash(:,q)) with the gradient / vol (ref.f:4466-4505)
+__global__ void GATHER_BOUNDS k_velprd_grad(ColMesh M, const double *__restrict__ ud, const double *__restrict__ vol,
+                                            U3 U, double dt, double *__restrict__ u1) {
+    NODE_BEGIN
+    double gx, gy, gz;
+    grad3<double>(M, ud, c, k, n, gx, gy, gz);
+    const double v = vol[n];
+    const double f1 = gx / v, f2 = gy / v, f3 = gz / v;
+    u1[n] = ud[n] - dt * (U.u[0][n] * f1 + U.u[1][n] * f2 + U.u[2][n] * f3);
+}
+// advective velocity at n+1/2 and the low-order solution at n+1 (ref.f:4517-4526)
+__global__ void k_velprd_post(int N, Fields F, const double *__restrict__ f1, const double *__restrict__ f2,
+                              const double *__restrict__ f3) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const double r = F.rh0[n], ff[3] = {f1[n], f2[n], f3[n]};
+    for (int q = 0; q < 3; ++q) {
+        F.uuu[q][n] = (F.uuu[q][n] + ff[q]) * 0.5 * r;
+        F.ud[q][n] = ff[q];
     }
 }
 

@@ -328,6 +328,26 @@ def test_100_steps_c1_bitwise(c1_mesh):
     s.close()
 
 
+def test_velprd_steps_bitwise(small_mesh):
+    """itraj = 1: set-up and steps with velprd's trajectory prediction (ref.f:267-268, 441-442),
+    bit-identical to the oracle replaying the GPU reduction order."""
+    from src_b200.cabi import F_UNKDASH, F_UUU1
+    _, rm = small_mesh
+    P = RunParams(delt=10.0, itraj=1)
+    o = Oracle(P, rm, gpu_order=True)
+    with Solver(P, rm) as s:
+        assert_diag_equal(s.setup(), o.setup())
+        for _ in range(3):
+            assert_diag_equal(s.step(), o.step())
+        for fid in ([F_UNK + k for k in range(4)] + [F_UUU + k for k in range(3)] +
+                    [F_UUU1 + k for k in range(3)] + [F_UNKDASH + k for k in range(3)]):
+            assert np.array_equal(s.get(fid), o.get(fid)), fid
+        s.velprd()
+        o.velprd()
+        for fid in [F_UUU + k for k in range(3)] + [F_UNKDASH + k for k in range(3)]:
+            assert np.array_equal(s.get(fid), o.get(fid)), fid
+
+
 def test_deterministic(small_mesh):
     cm, rm = small_mesh
     out = []

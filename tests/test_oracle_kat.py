@@ -144,3 +144,24 @@ def test_steps_conserve_theta_mass(small_mesh):
     assert abs(d.mass[4] - m0) <= 1e-12 * m0
     assert d.smin[0] >= 0.0
     assert o.gcr_stats().status == 0
+
+
+def test_velprd_prediction_is_divergence_free(small_mesh):
+    """velprd (itraj = 1) ends with a potential solve: its low-order velocity (unkdash) meets the
+    solver's stopping test, max|D(rh0 u)/(vol rh0)| <= eps0/dt, and the advective momentum is
+    the average of the old and predicted velocities times rh0."""
+    from src_b200.cabi import F_UNKDASH, F_UUU1
+    _, rm = small_mesh
+    P = RunParams(delt=10.0, itraj=1)
+    o = Oracle(P, rm)
+    o.setup()
+    o.step()
+    uuu_before = [o.get(F_UUU + k) for k in range(3)]
+    o.velprd()
+    ud = [o.get(F_UNKDASH + k) for k in range(3)]
+    rhs, _ = o.div(ud[0], ud[1], ud[2], -1)
+    assert np.abs(rhs).max() <= P.eps0 / P.delt
+    rh0 = o.get(F_RH0)
+    for k in range(3):
+        assert np.array_equal(o.get(F_UUU + k), (uuu_before[k] + ud[k]) * 0.5 * rh0)
+    assert np.abs(o.get(F_UUU1)).max() > 0
