@@ -238,25 +238,9 @@ template <> struct Buf<float> {
     static const float *coefw(mpg_handle h) { return h->coefwf; }
 };
 
-#ifndef MPG_LAP_PAIRS
-#define MPG_LAP_PAIRS 0
-#endif
 template <class T>
 int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
     using B = Buf<T>;
-    if (MPG_LAP_PAIRS) {
-        const int PL = (h->L + 1) / 2, nt = h->NC * PL;
-        {
-            KTIME(KT_LAP_GRAD);
-            k_lap_grad2<T><<<grid(nt), kThreads, 0, h->st>>>(h->M, PL, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
-                                                            (T)h->P.delt, impfl, B::F(h));
-        }
-        {
-            KTIME(KT_LAP_DIV);
-            k_lap_div2<T><<<grid(nt), kThreads, 0, h->st>>>(h->M, PL, B::F(h), B::vol(h), B::rh0(h), alap);
-        }
-        return check_launch("laplc");
-    }
     {
         KTIME(KT_LAP_GRAD);
         k_lap_grad<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
@@ -264,8 +248,8 @@ int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
     }
     {
         KTIME(KT_LAP_DIV);
-        k_lap_div<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, B::F(h), B::vol(h),
-                                                         B::rh0(h), alap);
+        const int PL = (h->L + 1) / 2;
+        k_lap_div2<T><<<grid(h->NC * PL), kThreads, 0, h->st>>>(h->M, PL, B::F(h), B::vol(h), B::rh0(h), alap);
     }
     return check_launch("laplc");
 }

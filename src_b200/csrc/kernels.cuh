@@ -300,12 +300,14 @@ __global__ void DIV_BOUNDS k_lap_div(ColMesh M, const Flux<T> F, const T *__rest
     alap[n] = (dx + dy + dz) / (vol[n] * rh0[n]);
 }
 
-// ------------------------------------------------------------------------------ level-pair laplc
-// The two halves of laplc with one thread per pair of adjacent levels (k0 = 2p, k1 = 2p + 1) of a
+// ------------------------------------------------------------------------------ level-pair divergence
+// laplc's second half with one thread per pair of adjacent levels (k0 = 2p, k1 = 2p + 1) of a
 // column: the adjacency entry, its decode and the face addressing serve both nodes (a horizontal
 // face of level k1 is the next element of every array), and the vertical face between the two is
-// loaded once.  Each node still adds its terms in the reference's edge order, so the results are
-// bit-identical to k_lap_grad / k_lap_div.
+// loaded once.  Each node still adds its terms in the reference's edge order, so the result is
+// bit-identical to k_lap_div.  Measured on the 512x512x81 workload it is 5% faster than k_lap_div
+// (823 against 869 us in FP64); the same structure for the gradient half was 9% slower, which is
+// why that half keeps one thread per node.
 struct Face2 {
     int j0, j1, s0, s1;
     bool sub, vert, v0, v1;
@@ -327,70 +329,11 @@ __device__ __forceinline__ Face2 decode_face2(int2 en, int n0, int k0, int L, bo
     return f;
 }
 
-#ifndef MPG_LAP_PAIR_MINB
-#define MPG_LAP_PAIR_MINB 4
-#endif
-template <class T>
-__global__ void __launch_bounds__(kThreads, MPG_LAP_PAIR_MINB)
-k_lap_grad2(ColMesh M, int PL, const T *__restrict__ p, const T *__restrict__ vol, const T *__restrict__ rh0,
-            const T *__restrict__ coefw, const double *__restrict__ ue, T dt, int impfl, Flux<T> F) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= M.NC * PL) return;
-    const int c = t / PL, L = M.L, k0 = 2 * (t - c * PL), n0 = c * L + k0;
-    const bool two = k0 + 1 < L;
-    const T p0 = p[n0], p1 = two ? p[n0 + 1] : T(0);
-    T a0x = 0., a0y = 0., a0z = 0., a1x = 0., a1y = 0., a1z = 0.;
-    const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
-    for (int j = beg; j < end; ++j) {
-        const Face2 f = decode_face2(__ldg(&M.cadj[j]), n0, k0, L, two);
-        T sx0, sy0, sz0, sx1 = 0., sy1 = 0., sz1 = 0.;
-        FaceVec<T>::load(M, f.vert, f.s0, sx0, sy0, sz0);
-        const T q0 = p[f.j0];
-        T q1 = 0.;
-        if (two) {
-            FaceVec<T>::load(M, f.vert, f.s1, sx1, sy1, sz1);
-            q1 = p[f.j1];
-        }
-        if (f.v0) {
-            const T u = (p0 + q0) * T(0.5);
-            const T tx = sx0 * u, ty = sy0 * u, tz = sz0 * u;
-            if (f.sub) { a0x = a0x - tx; a0y = a0y - ty; a0z = a0z - tz; }
-            else       { a0x = a0x + tx; a0y = a0y + ty; a0z = a0z + tz; }
-        }
-        if (f.v1) {
-            const T u = (p1 + q1) * T(0.5);
-            const T tx = sx1 * u, ty = sy1 * u, tz = sz1 * u;
-            if (f.sub) { a1x = a1x - tx; a1y = a1y - ty; a1z = a1z - tz; }
-            else       { a1x = a1x + tx; a1y = a1y + ty; a1z = a1z + tz; }
-        }
-    }
-    const T pn[2] = {p0, p1};
-    T ax[2] = {a0x, a1x}, ay[2] = {a0y, a1y}, az[2] = {a0z, a1z};
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        if (h == 1 && !two) break;
-        const int k = k0 + h, n = n0 + h;
-        T gx = ax[h], gy = ay[h], gz = az[h];
-        if (M.iper == 0) {
-            for_boundary(M, c, k, [&](const BEntry &be) {
-                gx = gx + T(be.sbb[0]) * pn[h];
-                gy = gy + T(be.sbb[1]) * pn[h];
-                gz = gz + T(be.sbb[2]) * pn[h];
-            });
-        }
-        const T v = vol[n];
-        T dx = dt * gx / v, dy = dt * gy / v, dz = dt * gz / v;
-        dx = T(0.5) * dx / T(1.0);
-        dy = T(0.5) * dy / T(1.0);
-        dz = T(0.5) * dz * (coefw[n] * (T)impfl + (T)(1 - impfl));
-        bcv_node<T>(M, c, k, n, ue, 0.0, dx, dy, dz);
-        const T r = rh0[n];
-        F.store(n, dx * r, dy * r, dz * r);
-    }
-}
+// 64 registers: the two nodes' operands of a face in flight together
+constexpr int kLapPairMinBlocks = 4;
 
 template <class T>
-__global__ void __launch_bounds__(kThreads, MPG_LAP_PAIR_MINB)
+__global__ void __launch_bounds__(kThreads, kLapPairMinBlocks)
 k_lap_div2(ColMesh M, int PL, const Flux<T> F, const T *__restrict__ vol, const T *__restrict__ rh0,
            T *__restrict__ alap) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
