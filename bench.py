@@ -45,6 +45,23 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+def max_over_ranks(x, device="cuda"):
+    """The largest of a per-rank value over all ranks (the value itself on one rank).  The N-GPU
+    run is N independent replicas, so this maximum of the device times is the only exchange."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, steps, seconds):
+    """Steps per second of the whole job: every replica runs `steps` steps in at most `seconds`."""
+    return world * steps / seconds
+
+
 def build_params(name, precision=0):
     from src_b200.cabi import RunParams
     nx, L, dt, h0, lord, nscal = WORKLOADS[name]
@@ -291,12 +308,8 @@ def main():
     ref_fields = {k: s.get(F_UNK + k) for k in range(4)} if not args.no_variants else None
     rates = [d.rate1 for d in diags if d.rate1 > 0]
     plain_rate = float(np.exp(np.mean(np.log(rates)))) if rates else 0.0
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = world * args.steps / (ms_max / 1000.0)
+    ms_max = max_over_ranks(ms)
+    value = whole_job_rate(world, args.steps, ms_max / 1000.0)
 
     # ---------------- per-kernel roofline
     N, L, NC, NE2 = info["npoin"], info["nlev"], info["ncol"], info["nedge2d"]
@@ -352,14 +365,10 @@ def main():
         for f in fids:
             host[f][:] = s.get(f)
         t1 = time.perf_counter()
-        sec = t1 - t0
-        if world > 1:
-            t = torch.tensor([sec], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            sec = float(t.item())
+        sec = max_over_ranks(t1 - t0)
         state = len(fids) * 8 * rm.npoin
         import ctypes
-        e2e = {"value": world * args.steps / sec, "unit": "steps/s",
+        e2e = {"value": whole_job_rate(world, args.steps, sec), "unit": "steps/s",
                "h2d_bytes_per_step": state // args.steps,
                "d2h_bytes_per_step": (state + args.steps * ctypes.sizeof(MpgDiag)) // args.steps,
                "path": "mpg_set_field x%d from pinned host arrays, %d x mpg_step (per-step diagnostics "
@@ -410,11 +419,7 @@ def main():
             a1.record(stream_v)
             a1.synchronize()
             barrier()
-            vms = a0.elapsed_time(a1)
-            if world > 1:
-                t = torch.tensor([vms], device="cuda")
-                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-                vms = float(t.item())
+            vms = max_over_ranks(a0.elapsed_time(a1))
             vkt = sv.kernel_times()
             vsolve = vkt.get("pressure_solve", (1, 0.0))
             err = {}
@@ -422,13 +427,13 @@ def main():
                 a, b = sv.get(F_UNK + k), ref_fields[k]
                 err[nm] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
             variants[vname] = {
-                "value": world * args.steps / (vms / 1000.0), "unit": "steps/s",
+                "value": whole_job_rate(world, args.steps, vms / 1000.0), "unit": "steps/s",
                 "ms_per_step": vms / args.steps,
                 "ms_per_pressure_solve": round(vsolve[1] / max(vsolve[0], 1), 3),
                 "gcr_iters_per_solve": round(float(np.mean([a for p in vit for a in p])), 2),
                 "gcr_iters_first_solve": round(float(np.mean([p[0] for p in vit])), 2),
                 "gcr_rate_first_solve": round(float(np.exp(np.mean(np.log([x for x in vrate if x > 0] or [1.0])))), 5),
-                "speedup_vs_fp64": round((world * args.steps / (vms / 1000.0)) / value, 3),
+                "speedup_vs_fp64": round(whole_job_rate(world, args.steps, vms / 1000.0) / value, 3),
                 "rel_l2_vs_fp64": err,
                 "kernels_ms": {k: round(v[1], 2) for k, v in vkt.items()},
                 "precision": "FP32 face vectors, MPDATA fluxes, GCR directions and operator; "

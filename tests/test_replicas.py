@@ -1,0 +1,64 @@
+"""The N-GPU path of bench.py is N independent replicas: the only exchange is the maximum of the
+per-rank device times.  Checked with two gloo ranks on the CPU (127.0.0.1 rendezvous)."""
+import os
+import socket
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, q):
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        import bench
+        ms = [120.0, 150.0][rank]
+        m = bench.max_over_ranks(ms, device="cpu")
+        # each replica advances its own state: the oracle on its own copy of the mesh
+        import numpy as np
+        from oracle.oracle import Oracle
+        from src_b200 import mesh
+        from src_b200.cabi import F_UNK, RunParams
+        rm = mesh.generate(6, L=5, seed=1).to_reference()
+        o = Oracle(RunParams(delt=10.0), rm)
+        o.setup()
+        o.step()
+        u = o.get(F_UNK)
+        q.put((rank, m, bench.whole_job_rate(world, 10, m / 1000.0), float(np.sum(u * u))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_replicas_take_the_max_time():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(2))
+    assert [r[1] for r in res] == [150.0, 150.0]                 # both ranks see the slowest time
+    assert res[0][2] == res[1][2] == pytest.approx(2 * 10 / 0.150)
+    assert res[0][3] == res[1][3]                                 # identical independent replicas
+
+
+def test_single_rank_is_identity():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.max_over_ranks(42.0) == 42.0
+    assert bench.whole_job_rate(1, 10, 2.0) == 5.0
