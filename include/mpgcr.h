@@ -260,6 +260,13 @@ int mpg_learned_forward(mpg_handle h, int r, int q);
 #define MPG_NN_LOSS_RESIDUAL 0
 #define MPG_NN_LOSS_ERROR    1
 int mpg_learned_loss(mpg_handle h, int mode);
+/* Failure-detection self-test of the bounded waits in the library's tensor-core kernels (no
+ * counterpart in the reference): one CTA arms an mbarrier for one arrival and waits on it with
+ * the same bounded loop the network layers use, giving up after `spins` polls (1..2^22).  With
+ * arrive != 0 a thread arrives and *completed = 1; with arrive == 0 nothing arrives, the wait runs
+ * out, the kernel returns normally and *completed = 0 — the device stays usable.  In the network
+ * layers the same give-up writes NaN outputs, which gcrk's finite check turns into a fallback. */
+int mpg_selftest_wait(mpg_handle h, int arrive, int spins, int *completed);
 int mpg_learned_grad(mpg_handle h, int r, int t, float *grad, double *loss);
 /* one Adam step on the pair (r, t) */
 int mpg_learned_train_pair(mpg_handle h, int r, int t, float lr, double *loss);

@@ -32,7 +32,7 @@ EXPORTS = [
     "mpg_laplc_noalloc", "mpg_learned_init", "mpg_learned_set_params", "mpg_learned_get_params",
     "mpg_learned_forward", "mpg_learned_grad", "mpg_learned_train_pair", "mpg_learned_harvest",
     "mpg_learned_train_records", "mpg_learned_loss", "mpg_laplc_adjoint", "mpg_restart_write",
-    "mpg_restart_read", "mpg_velprd",
+    "mpg_restart_read", "mpg_velprd", "mpg_selftest_wait",
 ]
 NPARAM = 9505
 
@@ -92,6 +92,7 @@ def lib():
         L.mpg_learned_loss.argtypes = [vp, ip]
         L.mpg_restart_write.argtypes = [vp, C.c_char_p, ip, ip]
         L.mpg_velprd.argtypes = [vp]
+        L.mpg_selftest_wait.argtypes = [vp, ip, ip, C.POINTER(C.c_int)]
         L.mpg_restart_read.argtypes = [vp, C.c_char_p, ip, C.POINTER(C.c_int)]
         _lib = L
     return _lib
@@ -264,6 +265,12 @@ class Solver:
         loss = C.c_double()
         _check(self.L.mpg_learned_train_pair(self.h, r, t, lr, C.byref(loss)))
         return loss.value
+
+    def selftest_wait(self, arrive: bool, spins: int) -> bool:
+        """Run the bounded-wait self-test; True when the wait completed, False when it gave up."""
+        done = C.c_int()
+        _check(self.L.mpg_selftest_wait(self.h, 1 if arrive else 0, spins, C.byref(done)))
+        return bool(done.value)
 
     def learned_loss(self, mode: int) -> None:
         """0: residual norm ||A q - r||_W (default), 1: regression on the scaled error."""

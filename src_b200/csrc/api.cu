@@ -103,6 +103,8 @@ struct mpg_solver {
         int loss_mode = MPG_NN_LOSS_RESIDUAL;
         double *qd = nullptr, *ed = nullptr, *dq = nullptr;
         int *err = nullptr;          // set by the tensor-core layer when its wait gave up
+        int *selftest = nullptr;     // status of mpg_selftest_wait
+        int col_ctas = 0;            // persistent grid of the column layers (CTAs resident at once)
     } nn;
 };
 
@@ -482,14 +484,14 @@ template <int NS>
 void nn_layers(mpg_handle h, const nn::Geom &G, double *qd, float *qf, bool train) {
     auto &S = h->nn;
     // persistent grid: as many CTAs as fit on the device at once (tensor memory included)
-    static int per_sm = 0, sms = 0;
-    if (!per_sm) {
+    if (!S.col_ctas) {
+        int per_sm = 0, sms = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nn::k_nn_col<NS, false, false>, nn::COL_THREADS, 0);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
         per_sm = std::max(1, std::min(per_sm, 512 / (int)nn::TC_TMEM_COLS));
-        sms = std::max(1, sms);
+        S.col_ctas = std::max(1, sms) * per_sm;
     }
-    const int nb = std::min(h->NC, sms * per_sm);
+    const int nb = std::min(h->NC, S.col_ctas);
     const size_t W = (size_t)nn::C * nn::K3;
     nn::k_nn_col<NS, true, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
         h->M, G, nullptr, S.X0, S.Wbf, S.prm, 0, nullptr, nullptr, S.H[1], nullptr, nullptr,
@@ -2007,6 +2009,18 @@ extern "C" int mpg_learned_grad(mpg_handle h, int r, int t, float *grad, double 
         MPG_CUDA(cudaMemcpyAsync(grad, h->nn.grad, sizeof(float) * nn::NPARAM, cudaMemcpyDeviceToHost, h->st));
         MPG_CUDA(cudaStreamSynchronize(h->st));
     }
+    return MPG_OK;
+}
+
+extern "C" int mpg_selftest_wait(mpg_handle h, int arrive, int spins, int *completed) {
+    if (!h || !completed) return mpg_fail(MPG_ERR_ARG, "null argument");
+    if (spins < 1 || spins > (1 << 22)) return mpg_fail(MPG_ERR_ARG, "spins must be in 1..4194304");
+    int rc;
+    if (!h->nn.selftest && (rc = dalloc(h, &h->nn.selftest, 1))) return rc;
+    nn::k_mbar_selftest<<<1, 128, 0, h->st>>>(arrive ? 1 : 0, (long long)spins, h->nn.selftest);
+    if ((rc = check_launch("selftest wait"))) return rc;
+    MPG_CUDA(cudaMemcpyAsync(completed, h->nn.selftest, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    MPG_CUDA(cudaStreamSynchronize(h->st));
     return MPG_OK;
 }
 

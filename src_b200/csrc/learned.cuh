@@ -87,6 +87,39 @@ constexpr long long TC_SPIN_MAX = 1ll << 22;  // bound on the mbarrier wait (the
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+// Bounded wait for phase `phase` of an mbarrier: true once the phase completed, false after
+// `limit` polls (mbarrier.try_wait may itself suspend the thread for a while between polls).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, long long limit) {
+    uint32_t done = 0;
+    long long spins = 0;
+    while (!done) {
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+        if (!done && ++spins > limit) break;
+    }
+    return done != 0;
+}
+
+// Self-test of the bounded wait: one CTA arms an mbarrier for a single arrival.  With `arrive`,
+// thread 0 arrives and the wait completes; without, nothing arrives and every thread gives up
+// after `limit` polls.  status[0] = 1 when all threads saw the phase complete, 0 when they gave up.
+__global__ void k_mbar_selftest(int arrive, long long limit, int *status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (arrive && threadIdx.x == 0) {
+        uint64_t state;
+        asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(state) : "r"(smem_u32(&bar)) : "memory");
+    }
+    const bool done = mbar_wait_bounded(&bar, 0u, limit);
+    const int all = __syncthreads_and(done);
+    if (threadIdx.x == 0) status[0] = all;
+}
+
 // shared-memory matrix descriptor: canonical K-major layout without swizzle
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
@@ -311,14 +344,7 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const float *
                          :: "r"(smem_u32(&bar)) : "memory");
         }
         {
-            uint32_t done = 0;
-            long long spins = 0;
-            while (!done) {
-                asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                             "selp.u32 %0, 1, 0, p;\n\t}\n"
-                             : "=r"(done) : "r"(smem_u32(&bar)), "r"(phase) : "memory");
-                if (!done && ++spins > TC_SPIN_MAX) break;
-            }
+            const bool done = mbar_wait_bounded(&bar, phase, TC_SPIN_MAX);
             if (__syncthreads_or(!done)) {
                 ok = false;
                 if (tid == 0) atomicExch(err, 1);

@@ -239,6 +239,27 @@ def test_slow_network_falls_back_and_converges(small_mesh):
             assert np.abs(ga - gb).max() < 1e-3 * 10.0
 
 
+def test_bounded_wait_gives_up_and_device_stays_usable(small_mesh):
+    """The tensor-core kernels' mbarrier waits are bounded: a wait whose arrival never comes (a
+    flag nothing sets) gives up after its poll limit and reports it, and the device keeps working."""
+    import time
+    from src_b200.cabi import F_WORK
+    _, rm = small_mesh
+    with _solver(rm) as s:
+        s.setup()
+        assert s.selftest_wait(True, 1000) is True
+        t0 = time.time()
+        assert s.selftest_wait(False, 2000) is False
+        assert time.time() - t0 < 30.0
+        s.set(F_WORK, np.ones(rm.npoin))
+        s.laplc(F_WORK, F_WORK + 1, 1)                # the context is still usable
+        assert np.all(np.isfinite(s.get(F_WORK + 1)))
+        s.step()
+        from src_b200.api import MpgError
+        with pytest.raises(MpgError):
+            s.selftest_wait(False, 0)
+
+
 def test_learned_requires_parameters(small_mesh):
     from src_b200.api import MpgError
     _, rm = small_mesh
