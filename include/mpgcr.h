@@ -288,6 +288,13 @@ int mpg_learned_train_records(mpg_handle h, int epochs, float lr, double *mean_l
  * bit-identical to the uninterrupted one.  Either replaces mpg_setup for a restarted run.  `path`
  * is a NUL-terminated file name; `ntime` is the step number written (read back into *ntime when
  * the file holds it; may be NULL). */
+/* output(unk) (ref.f:2771-2806): the flow field file the reference writes at the end of a run
+ * (unit 11, r.d, ref.f:40, called at ref.f:477): a list-directed "1." and npoin, the header line
+ * 'point X Y Z u v w temp Velocity', then per node in reference order format (1x,i7,8e12.4): the
+ * 1-based node number, coord/1000 (caller's COMMON array coord(npoinx,3)), u, v, w, theta' and
+ * sqrt(u^2+v^2+w^2) of unk(:,1:4). */
+int mpg_write_output(mpg_handle h, const char *path, const double *coord, int npoinx);
+
 #define MPG_RESTART_TEXT   0
 #define MPG_RESTART_BINARY 1
 int mpg_restart_write(mpg_handle h, const char *path, int format, int ntime);

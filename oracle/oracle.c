@@ -8,9 +8,9 @@
  * -O2 -ffp-contract=off (no FMA contraction, no fast-math).
  *
  * Reference options restated: isfera=0 only (the spherical variant is out of scope),
- * iper=0 or 2, mg_flag=0, ielast=0, itraj=0.  Extensions beyond the reference are marked
- * NEW: the vertical-line preconditioner (iprc=2), runtime lord/itmn, passive scalars and
- * the FP64 mass sums.
+ * iper=0 or 2, mg_flag=0, ielast=0, itraj=0 or 1 (velprd).  Extensions beyond the reference
+ * are marked NEW: the vertical-line preconditioner (iprc=2), runtime lord/itmn, passive
+ * scalars, the FP64 mass sums and the per-solve residual contraction.
  */
 #include "oracle.h"
 

@@ -32,7 +32,7 @@ EXPORTS = [
     "mpg_laplc_noalloc", "mpg_learned_init", "mpg_learned_set_params", "mpg_learned_get_params",
     "mpg_learned_forward", "mpg_learned_grad", "mpg_learned_train_pair", "mpg_learned_harvest",
     "mpg_learned_train_records", "mpg_learned_loss", "mpg_laplc_adjoint", "mpg_restart_write",
-    "mpg_restart_read", "mpg_velprd", "mpg_selftest_wait",
+    "mpg_restart_read", "mpg_velprd", "mpg_selftest_wait", "mpg_write_output",
 ]
 NPARAM = 9505
 
@@ -92,6 +92,7 @@ def lib():
         L.mpg_learned_loss.argtypes = [vp, ip]
         L.mpg_restart_write.argtypes = [vp, C.c_char_p, ip, ip]
         L.mpg_velprd.argtypes = [vp]
+        L.mpg_write_output.argtypes = [vp, C.c_char_p, vp, ip]
         L.mpg_selftest_wait.argtypes = [vp, ip, ip, C.POINTER(C.c_int)]
         L.mpg_restart_read.argtypes = [vp, C.c_char_p, ip, C.POINTER(C.c_int)]
         _lib = L
@@ -238,6 +239,11 @@ class Solver:
         nt = C.c_int()
         _check(self.L.mpg_restart_read(self.h, os.fsencode(path), fmt, C.byref(nt)))
         return nt.value
+
+    def write_output(self, path: str, coord) -> None:
+        """output(unk) (ref.f:2771): the r.d field file; coord is the mesh's (npoin, 3) coordinates."""
+        cf = np.ascontiguousarray(np.asarray(coord, np.float64).T)     # coord(npoinx, 3), column-major
+        _check(self.L.mpg_write_output(self.h, os.fsencode(path), cf.ctypes.data, cf.shape[1]))
 
     # ---------------------------------------------------------------- learned preconditioner
     def learned_init(self, seed: int = 0) -> None:

@@ -485,9 +485,26 @@ void nn_layers(mpg_handle h, const nn::Geom &G, double *qd, float *qf, bool trai
     auto &S = h->nn;
     // persistent grid: as many CTAs as fit on the device at once (tensor memory included)
     if (!S.col_ctas) {
-        int per_sm = 0, sms = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, nn::k_nn_col<NS, false, false>, nn::COL_THREADS, 0);
+        // CTAs resident per SM from the kernel's own footprint: registers, static shared memory
+        // (with the largest carveout requested) and the 512 tensor-memory columns of an SM.  The
+        // occupancy API reported 1 for these kernels, which measured 2.8x slower than 4.
+        cudaFuncSetAttribute(nn::k_nn_col<NS, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(nn::k_nn_col<NS, false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(nn::k_nn_col<NS, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        int per_sm = 1 << 30, sms = 0, regs_sm = 65536, smem_sm = 228 * 1024;
+        const void *fns[3] = {(const void *)nn::k_nn_col<NS, true, false>, (const void *)nn::k_nn_col<NS, false, false>,
+                              (const void *)nn::k_nn_col<NS, false, true>};
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, h->dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->dev);
+        for (const void *fn : fns) {
+            cudaFuncAttributes fa{};
+            if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) { per_sm = 1; break; }
+            const int regs_cta = ((fa.numRegs + 7) / 8 * 8) * nn::COL_THREADS;
+            const int smem_cta = (int)fa.sharedSizeBytes + 1024;       // plus the per-CTA reserve
+            per_sm = std::min(per_sm, std::min(regs_sm / std::max(regs_cta, 1), smem_sm / std::max(smem_cta, 1)));
+        }
+        cudaGetLastError();
         per_sm = std::max(1, std::min(per_sm, 512 / (int)nn::TC_TMEM_COLS));
         S.col_ctas = std::max(1, sms) * per_sm;
     }
@@ -720,10 +737,12 @@ struct ProdAxpy {   // p += beta x, r += beta ax; returns |r|, r^2
     const double *scal;
     const T *x, *a;
     double *p, *r;
-    __device__ void operator()(int n, double *v) const {
+    struct Loaded { double p, r, x, a; };
+    __device__ Loaded load(int n) const { return Loaded{p[n], r[n], (double)x[n], (double)a[n]}; }
+    __device__ void finish(int n, const Loaded &l, double *v) const {
         const double beta = scal[S_BETA];
-        p[n] = p[n] + beta * (double)x[n];
-        const double rn = r[n] + beta * (double)a[n];
+        p[n] = l.p + beta * l.x;
+        const double rn = l.r + beta * l.a;
         r[n] = rn;
         v[0] = fabs(rn);
         v[1] = rn * rn;
@@ -734,10 +753,17 @@ struct ProdDots {
     const T *ar;
     const T *ax[MPG_MAX_LORD];
     int i;
-    __device__ void operator()(int n, double *v) const {
-        const double a = (double)ar[n];
+    struct Loaded { double a, x[NQ]; };
+    __device__ Loaded load(int n) const {
+        Loaded l;
+        l.a = (double)ar[n];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) v[q] = q < i ? (double)ax[q][n] * a : 0.0;
+        for (int q = 0; q < NQ; ++q) l.x[q] = q < i ? (double)ax[q][n] : 0.0;
+        return l;
+    }
+    __device__ void finish(int, const Loaded &l, double *v) const {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) v[q] = q < i ? l.x[q] * l.a : 0.0;
     }
 };
 template <class T>
@@ -783,32 +809,45 @@ struct ProdUpdate {
     const double *r;
     VecListT<T> x, ax;
     T *xo, *axo;
-    __device__ void operator()(int n, double *v) const {
+    struct Loaded { double q, a, r, x[I], ax[I]; };
+    __device__ Loaded load(int n) const {
+        Loaded l;
+        l.q = (double)qr[n];
+        l.a = (double)ar[n];
+        l.r = r[n];
+#pragma unroll
+        for (int ii = 0; ii < I; ++ii) {
+            l.x[ii] = (double)x.v[ii][n];
+            l.ax[ii] = (double)ax.v[ii][n];
+        }
+        return l;
+    }
+    __device__ void finish(int n, const Loaded &l, double *v) const {
         double a, b;
         if (RESTART) {
-            a = (double)qr[n] + scal[S_DEL] * (double)x.v[0][n];
-            b = (double)ar[n] + scal[S_DEL] * (double)ax.v[0][n];
+            a = l.q + scal[S_DEL] * l.x[0];
+            b = l.a + scal[S_DEL] * l.ax[0];
 #pragma unroll
             for (int ii = 1; ii < I; ++ii) {
                 const double d = scal[S_DEL + ii];
-                a = a + d * (double)x.v[ii][n];
-                b = b + d * (double)ax.v[ii][n];
+                a = a + d * l.x[ii];
+                b = b + d * l.ax[ii];
             }
         } else {
-            a = (double)qr[n];
-            b = (double)ar[n];
+            a = l.q;
+            b = l.a;
 #pragma unroll
             for (int ii = 0; ii < I; ++ii) {
                 const double d = scal[S_DEL + ii];
-                a = a + d * (double)x.v[ii][n];
-                b = b + d * (double)ax.v[ii][n];
+                a = a + d * l.x[ii];
+                b = b + d * l.ax[ii];
             }
         }
         const T at = (T)a, bt = (T)b;
         xo[n] = at;
         axo[n] = bt;
         const double bs = (double)bt;        // the stored direction, as the next iteration reads it
-        v[0] = r[n] * bs;
+        v[0] = l.r * bs;
         v[1] = bs * bs;
     }
 };
@@ -1835,7 +1874,56 @@ std::vector<int> restart_binary_fields(mpg_handle h) {
     return f;
 }
 
+// Fortran's Ew.d edit with d = 4, w = 12: 0.dddd mantissa, E and a signed 2-digit exponent
+// ("0.dddd+eee" when the exponent needs three digits), right-justified; 12 asterisks when the
+// value is not finite
+void put_e12_4(std::string &out, double v) {
+    char m[32], b[32];
+    if (!std::isfinite(v)) { out.append(12, '*'); return; }
+    if (v == 0.) { std::snprintf(b, sizeof b, "%12s", "0.0000E+00"); out.append(b, 12); return; }
+    std::snprintf(m, sizeof m, "%.3E", std::fabs(v));             // d.dddE+xx, 4 significant digits
+    const int e = std::atoi(m + 6) + 1;                           // exponent of the 0.dddd form
+    char digits[5] = {m[0], m[2], m[3], m[4], 0};
+    char ex[8];
+    if (e >= -99 && e <= 99) std::snprintf(ex, sizeof ex, "E%c%02d", e < 0 ? '-' : '+', e < 0 ? -e : e);
+    else std::snprintf(ex, sizeof ex, "%c%03d", e < 0 ? '-' : '+', e < 0 ? -e : e);
+    std::snprintf(b, sizeof b, "%s0.%s%s", v < 0 ? "-" : "", digits, ex);
+    char r[32];
+    std::snprintf(r, sizeof r, "%12s", b);
+    out.append(r, 12);
+}
+
 }  // namespace
+
+extern "C" int mpg_write_output(mpg_handle h, const char *path, const double *coord, int npoinx) {
+    if (!h || !path || !coord) return mpg_fail(MPG_ERR_ARG, "null argument");
+    if (npoinx < h->N) return mpg_fail(MPG_ERR_ARG, "npoinx smaller than npoin");
+    const size_t N = (size_t)h->N;
+    std::vector<std::vector<double>> u(4, std::vector<double>(N));
+    int rc;
+    for (int q = 0; q < 4; ++q)
+        if ((rc = mpg_get_field(h, MPG_F_UNK + q, u[q].data()))) return rc;
+    std::FILE *fp = std::fopen(path, "w");
+    if (!fp) return mpg_fail(MPG_ERR_ARG, std::string("output: cannot open ") + path);
+    bool ok = std::fprintf(fp, "   1.0000000000000000     \n %11d\npoint X Y Z u v w temp Velocity\n", h->N) > 0;
+    std::string line;
+    for (size_t ip = 0; ip < N && ok; ++ip) {                     // ref.f:2793-2803, format 100
+        char head[16];
+        std::snprintf(head, sizeof head, " %7d", (int)(ip + 1));
+        line.assign(head);
+        for (int i = 0; i < 3; ++i) put_e12_4(line, coord[(size_t)i * npoinx + ip] / 1.e+03);
+        const double a = u[0][ip], b = u[1][ip], w = u[2][ip];
+        put_e12_4(line, a);
+        put_e12_4(line, b);
+        put_e12_4(line, w);
+        put_e12_4(line, u[3][ip]);
+        put_e12_4(line, std::sqrt(a * a + b * b + w * w));
+        line.push_back('\n');
+        ok = std::fwrite(line.data(), 1, line.size(), fp) == line.size();
+    }
+    ok = (std::fclose(fp) == 0) && ok;
+    return ok ? MPG_OK : mpg_fail(MPG_ERR_ARG, std::string("output: write failed on ") + path);
+}
 
 extern "C" int mpg_restart_write(mpg_handle h, const char *path, int format, int ntime) {
     if (!h || !path) return mpg_fail(MPG_ERR_ARG, "null argument");

@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "mpgcr_internal.h"
 
 namespace mpgk {
@@ -542,6 +544,14 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
 // ------------------------------------------------------------------------------ reductions
 enum RedKind { RSUM = 0, RMAX = 1 };
 
+// A reduction functor may split its work per node into load(n) -> Loaded and finish(n, Loaded,
+// vals) (it then defines a nested type Loaded).  k_reduce then loads two nodes of its
+// grid-stride sequence before finishing either, which the compiler cannot arrange by itself
+// when finish stores to arrays that might alias the next node's operands.  The order in which a
+// thread accumulates its nodes is the same, so the results are bit-identical.
+template <class P, class = void> struct SplitProd { static constexpr bool value = false; };
+template <class P> struct SplitProd<P, std::void_t<typename P::Loaded>> { static constexpr bool value = true; };
+
 // Deterministic reduction of NQ quantities produced per node by `prod(n, vals)`.  `kinds` is a
 // bitmask: bit q set -> quantity q is a max, else a sum.  The last block to finish reduces the
 // block partials in fixed order and calls fin(results) with one thread.
@@ -553,12 +563,32 @@ k_reduce(int N, unsigned kinds, Prod prod, Fin fin, double *__restrict__ part,
 #pragma unroll
     for (int q = 0; q < NQ; ++q) acc[q] = ((kinds >> q) & 1u) ? -INFINITY : 0.0;
     const int stride = gridDim.x * blockDim.x;
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += stride) {
-        double v[NQ];
-        prod(n, v);
+    auto add = [&](const double *v) {
 #pragma unroll
         for (int q = 0; q < NQ; ++q)
             acc[q] = ((kinds >> q) & 1u) ? amax(acc[q], v[q]) : acc[q] + v[q];
+    };
+    int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if constexpr (SplitProd<Prod>::value) {
+        for (; n + stride < N; n += 2 * stride) {
+            const typename Prod::Loaded a = prod.load(n), b = prod.load(n + stride);
+            double v[NQ];
+            prod.finish(n, a, v);
+            add(v);
+            prod.finish(n + stride, b, v);
+            add(v);
+        }
+        for (; n < N; n += stride) {
+            double v[NQ];
+            prod.finish(n, prod.load(n), v);
+            add(v);
+        }
+    } else {
+        for (; n < N; n += stride) {
+            double v[NQ];
+            prod(n, v);
+            add(v);
+        }
     }
     __shared__ double sred[NQ][kRedThreads / 32];
     __shared__ bool last;

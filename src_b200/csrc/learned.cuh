@@ -240,15 +240,12 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const float *
             for (int i = 0; i < 8; ++i) ah[s][i] = 0.f;
         }
         const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
-        // horizontal faces in a two-deep pipeline: the next face's rows are requested before the
-        // current face is accumulated (vertical entries are skipped; they come from sH below)
-        auto next_h = [&](int j) {
-            while (j < end && __ldg(&M.cadj[j]).x < 0) ++j;
-            return j;
-        };
-        auto fetch = [&](int j, uint4 *v, float *t) {
+        for (int j = beg; j < end; ++j) {
             const int2 en = __ldg(&M.cadj[j]);
+            if (en.x < 0) continue;                      // vertical faces: below, from sH
             const int e = en.x >> 1, nb = en.y * L;
+            uint4 v[NS];
+            float t[NS];
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 const int k = lane + 32 * s;
@@ -258,14 +255,6 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const float *
                     t[s] = G.Th[(size_t)e * L + k];
                 }
             }
-        };
-        uint4 v[NS], vn[NS];
-        float t[NS], tn[NS];
-        int j = next_h(beg);
-        if (j < end) fetch(j, v, t);
-        while (j < end) {
-            const int jn = next_h(j + 1);
-            if (jn < end) fetch(jn, vn, tn);
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 const int k = lane + 32 * s;
@@ -278,9 +267,6 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const float *
 #pragma unroll
                 for (int i = 0; i < 8; ++i) ah[s][i] += wt * hj[i];
             }
-#pragma unroll
-            for (int s = 0; s < NS; ++s) { v[s] = vn[s]; t[s] = tn[s]; }
-            j = jn;
         }
         __syncwarp();
         // ---- operand rows: [h ; ah - wsum h ; av] for octet w

@@ -102,3 +102,30 @@ def test_restart_errors(small_mesh, tmp_path):
             s.restart_read(str(short), 0)
         with pytest.raises(MpgError):
             s.restart_write(str(tmp_path / "x"), 7)
+
+
+def test_output_file_reference_layout(small_mesh, tmp_path):
+    """output(unk) (ref.f:2771-2806): header, then one line per node in format (1x,i7,8e12.4)."""
+    _, rm = small_mesh
+    path = str(tmp_path / "r.d")
+    with _started(rm, 2) as s:
+        s.write_output(path, rm.coord)
+        u = [s.get(F_UNK + k) for k in range(4)]
+    lines = open(path).read().split("\n")[:-1]
+    n = rm.npoin
+    assert float(lines[0]) == 1.0 and int(lines[1]) == n
+    assert lines[2] == "point X Y Z u v w temp Velocity"
+    assert len(lines) == n + 3 and all(len(l) == 104 for l in lines[3:])
+
+    def e4(x):                                  # the value an E12.4 field denotes
+        return float("%.3E" % x)
+
+    vv = np.sqrt(u[0] ** 2 + u[1] ** 2 + u[2] ** 2)
+    for ip in (0, 1, n // 2, n - 1):
+        l = lines[3 + ip]
+        assert int(l[:8]) == ip + 1
+        f = [l[8 + 12 * i:20 + 12 * i] for i in range(8)]
+        assert all(x.strip()[0] in "-0" and "E" in x for x in f), f
+        want = [rm.coord[ip, 0] / 1e3, rm.coord[ip, 1] / 1e3, rm.coord[ip, 2] / 1e3,
+                u[0][ip], u[1][ip], u[2][ip], u[3][ip], vv[ip]]
+        assert [float(x) for x in f] == [e4(x) for x in want]
