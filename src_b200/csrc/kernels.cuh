@@ -389,6 +389,23 @@ k_lap_div2(ColMesh M, int PL, const Flux<T> F, const T *__restrict__ vol, const 
     }
 }
 
+// ------------------------------------------------------------------------------ mbarrier wait
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Bounded wait for phase `phase` of an mbarrier: true once the phase completed, false after
+// `limit` polls (mbarrier.try_wait may itself suspend the thread for a while between polls).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, long long limit) {
+    uint32_t done = 0;
+    long long spins = 0;
+    while (!done) {
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done) : "r"(smem_addr(bar)), "r"(phase) : "memory");
+        if (!done && ++spins > limit) break;
+    }
+    return done != 0;
+}
+
 // Adjoint of laplc in the inner product weighted by W = vol*rh0.  laplc is
 // A = diag(1/W) sum_d B_d rh0 P S1 B_d (B_d: derivative matrix of component d, S1: the dt/2,
 // coefw and 1/vol scaling, P: bcv's projections), so A^T W y = sum_d B_d^T S1 P^T rh0 B_d^T y.

@@ -87,20 +87,6 @@ constexpr long long TC_SPIN_MAX = 1ll << 22;  // bound on the mbarrier wait (the
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Bounded wait for phase `phase` of an mbarrier: true once the phase completed, false after
-// `limit` polls (mbarrier.try_wait may itself suspend the thread for a while between polls).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, long long limit) {
-    uint32_t done = 0;
-    long long spins = 0;
-    while (!done) {
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}\n"
-                     : "=r"(done) : "r"(smem_u32(bar)), "r"(phase) : "memory");
-        if (!done && ++spins > limit) break;
-    }
-    return done != 0;
-}
-
 // Self-test of the bounded wait: one CTA arms an mbarrier for a single arrival.  With `arrive`,
 // thread 0 arrives and the wait completes; without, nothing arrives and every thread gives up
 // after `limit` polls.  status[0] = 1 when all threads saw the phase complete, 0 when they gave up.
