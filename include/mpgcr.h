@@ -2,7 +2,8 @@
  * mpgcr.h — C ABI of the B200 implementation of the two hot loops of the edge-based
  * anelastic solver `lippsLFroude_implgwopks3D_unstr3.f` (the reference):
  *
- *   * MPDATA advection      : mpdatamper            (ref.f:3617-3941) + derivative (ref.f:3943-4022)
+ *   * MPDATA advection      : mpdatamper            (ref.f:3617-3941), mpdatam (ref.f:3029-3311)
+ *                             + derivative (ref.f:3943-4022)
  *   * GCR(k) pressure solve : gcrk (ref.f:1776-1972), precon (ref.f:482-753), laplc (ref.f:1288-1353),
  *                             prfr (ref.f:1536-1580), div (ref.f:2096-2170), bcv (ref.f:1583-1643)
  *
@@ -206,8 +207,14 @@ int mpg_precon(mpg_handle h, int rhs, int p, int r, int iprc, int impfl);
 /* gcrk(p, u1, v1, w1, u2, v2, w2, impfl)                ref.f:1776-1972 */
 int mpg_gcrk(mpg_handle h, int p, int u1, int v1, int w1, int u2, int v2, int w2,
              int impfl, mpg_gcr_stats *stats);
-/* mpdatamper(uuu, unk(1,iflag), iflag)                  ref.f:3617-3941 (uuu = MPG_F_UUU) */
+/* mpdatamper(uuu, unk(1,iflag), iflag)                  ref.f:3617-3941 (uuu = MPG_F_UUU); iper = 2 */
 int mpg_mpdatamper(mpg_handle h, int unk, int iflag);
+/* mpdatam(uuu, unk(1,iflag), iflag)                     ref.f:3029-3311; iper = 0 (open boundaries).
+ * The first pass closes every boundary point of a type other than 11, 5 or 6 with the flux
+ * that balances the node's face fluxes, upwinded with the free-stream value afree(iflag) on
+ * inflow (ue per node for iflag = 1), ref.f:3143-3169.  iflag > 4 (passive scalars, not in
+ * the reference) flows in with 0. */
+int mpg_mpdatam(mpg_handle h, int unk, int iflag);
 /* courant(uuu, cour, iflag) and stats(unk)              ref.f:1974-2094, ref.f:2847-2912 */
 int mpg_courant(mpg_handle h, int iflag, mpg_diag *diag);
 int mpg_stats(mpg_handle h, mpg_diag *diag);

@@ -571,12 +571,16 @@ void orc_get_gcr_stats(orc *o, mpg_gcr_stats *st) {
     st->dvmx = o->dvmx_last; st->rl2 = o->rl2_last; st->rate = o->rate_last;
 }
 
-/* ------------------------------------------------------------------ mpdatamper ref.f:3617-3941 */
+/* ------------------------------------------------------------------ mpdatamper ref.f:3617-3941,
+ * mpdatam ref.f:3029-3311.  The two differ in the boundary-point loop of the first pass: mpdatam
+ * (open = 1) closes every boundary point that is not of type 11, 5 or 6 with the flux that
+ * balances the node's face fluxes, taking the free-stream value on inflow (ref.f:3143-3169);
+ * mpdatamper adds zero there and sums the periodic duplicates.  With empty periodic lists the
+ * rest of the two subroutines is the same loop for loop. */
 static double partp(double y) { return AMAX(0., y); }
 static double partn(double y) { return -AMIN(0., y); }
 
-void orc_mpdatamper(orc *o, double *unk, int iflag) {
-    (void)iflag;
+static void mpdata_core(orc *o, double *unk, int iflag, int open) {
     int n = o->npoin, ne = o->nedge, nb = o->nbface;
     double *const *uuu = &o->f[MPG_F_UUU];
     const double *rh0 = o->f[MPG_F_RH0];
@@ -628,11 +632,26 @@ void orc_mpdatamper(orc *o, double *unk, int iflag) {
         for (int b = 0; b < o->nboun; ++b) {                        /* ref.f:3732-3738 */
             int i1 = o->ibn[b];
             double fl1 = 0.;
+            if (open) {                                             /* ref.f:3143-3169 */
+                if (ipass == 1) {
+                    double aunbb1 = -divv[i1];
+                    /* afreelc(iflag) = afree(iflag), afreelc(1) = ue(i1); afree = (u0inf, v0inf,
+                     * w0inf, 0, 1) (ref.f:125-129).  Passive scalars (iflag > 4, not in the
+                     * reference) enter with 0. */
+                    double fin = iflag == 1 ? o->ue[i1] : iflag == 2 ? o->P.v0inf
+                               : iflag == 3 ? o->P.w0inf : 0.;
+                    fl1 = fin * AMIN(0., aunbb1) + unk[i1] * AMAX(0., aunbb1);
+                }
+                int t = o->ibt[b];
+                if (t == 11 || t == 5 || t == 6) fl1 = 0.;
+            }
             arh2[i1] = arh2[i1] + fl1 * sw[i1];
         }
-        cyclicr(o, arh2);
-        cyclicr2(o, arh2);
-        cyclicr4(o, arh2);
+        if (!open) {
+            cyclicr(o, arh2);
+            cyclicr2(o, arh2);
+            cyclicr4(o, arh2);
+        }
         for (int ip = 0; ip < n; ++ip)                              /* ref.f:3745-3747 */
             unk[ip] = unk[ip] - arh2[ip] * o->timestp[ip] / o->vol[ip] / rh0[ip];
         if (ipass == iord) break;
@@ -664,7 +683,7 @@ void orc_mpdatamper(orc *o, double *unk, int iflag) {
                 unkmx[i2] = AMAX(AMAX(unkmx[i2], p2), p1);
                 unkmn[i2] = AMIN(AMIN(unkmn[i2], p2), p1);
             }
-            for (int c = 0; c < o->ncoin; ++c) {
+            for (int c = 0; c < (open ? 0 : o->ncoin); ++c) {   /* periodic lists: mpdatamper only */
                 int i1 = o->ic1[c], i2 = o->ic2[c];
                 double p1 = unk[i1], p2 = unk[i2];
                 unkmx[i1] = AMAX(AMAX(AMAX(unkmx[i1], p1), p2), unkmx[i2]);
@@ -672,7 +691,7 @@ void orc_mpdatamper(orc *o, double *unk, int iflag) {
                 unkmx[i2] = AMAX(AMAX(AMAX(unkmx[i2], p1), p2), unkmx[i1]);
                 unkmn[i2] = AMIN(AMIN(AMIN(unkmn[i2], p1), p2), unkmn[i1]);
             }
-            for (int c = 0; c < o->ncoin2; ++c) {
+            for (int c = 0; c < (open ? 0 : o->ncoin2); ++c) {
                 int i1 = o->ic2a[c], i2 = o->ic2b[c];
                 double p1 = unk[i1], p2 = unk[i2];
                 unkmx[i1] = AMAX(AMAX(AMAX(unkmx[i1], p1), p2), unkmx[i2]);
@@ -680,7 +699,7 @@ void orc_mpdatamper(orc *o, double *unk, int iflag) {
                 unkmx[i2] = AMAX(AMAX(AMAX(unkmx[i2], p1), p2), unkmx[i1]);
                 unkmn[i2] = AMIN(AMIN(AMIN(unkmn[i2], p1), p2), unkmn[i1]);
             }
-            for (int c = 0; c < o->ncoin4; ++c) {
+            for (int c = 0; c < (open ? 0 : o->ncoin4); ++c) {
                 /* ref.f:3853-3866: the minima are taken over the maxima unkmx (as written). */
                 int ii[4] = {o->ic4[0][c], o->ic4[1][c], o->ic4[2][c], o->ic4[3][c]};
                 double pp[4] = {unk[ii[0]], unk[ii[1]], unk[ii[2]], unk[ii[3]]};
@@ -705,9 +724,11 @@ void orc_mpdatamper(orc *o, double *unk, int iflag) {
                 rhin[i2] = rhin[i2] + partp(a);
                 rhout[i2] = rhout[i2] + partn(a);
             }
-            cyclicr(o, rhin); cyclicr(o, rhout);
-            cyclicr2(o, rhin); cyclicr2(o, rhout);
-            cyclicr4(o, rhin); cyclicr4(o, rhout);
+            if (!open) {
+                cyclicr(o, rhin); cyclicr(o, rhout);
+                cyclicr2(o, rhin); cyclicr2(o, rhout);
+                cyclicr4(o, rhin); cyclicr4(o, rhout);
+            }
             for (int ip = 0; ip < n; ++ip) {
                 cpp[ip] = (unkmx[ip] - unk[ip]) * o->vol[ip] * rh0[ip] / (rhin[ip] * o->timestp[ip] + tol);
                 cnn[ip] = (unk[ip] - unkmn[ip]) * o->vol[ip] * rh0[ip] / (rhout[ip] * o->timestp[ip] + tol);
@@ -725,6 +746,9 @@ void orc_mpdatamper(orc *o, double *unk, int iflag) {
     free(unkmx); free(unkmn); free(rhin); free(rhout); free(cpp); free(cnn);
     free(sw); free(sw1); free(arh2);
 }
+
+void orc_mpdatamper(orc *o, double *unk, int iflag) { mpdata_core(o, unk, iflag, 0); }
+void orc_mpdatam(orc *o, double *unk, int iflag) { mpdata_core(o, unk, iflag, 1); }
 
 /* ------------------------------------------------------------------ courant ref.f:1974-2094 */
 void orc_courant(orc *o, int iflag, mpg_diag *diag) {
@@ -1084,8 +1108,10 @@ void orc_step(orc *o, mpg_diag *diag) {
         for (int k = 0; k < 4; ++k) unk[k][ip] = unk[k][ip] + 0.5 * frc[k][ip] * ts[ip];
         if (implgw == 0) unk[3][ip] = unk[3][ip] + f[MPG_F_THE][ip];
     }
-    for (int k = 0; k < 4 + P->nscal; ++k)                     /* ref.f:314-319 */
-        orc_mpdatamper(o, f[MPG_F_UNK + k], k + 1);
+    for (int k = 0; k < 4 + P->nscal; ++k) {                   /* ref.f:308-319 */
+        if (P->iper == 2) orc_mpdatamper(o, f[MPG_F_UNK + k], k + 1);
+        else orc_mpdatam(o, f[MPG_F_UNK + k], k + 1);
+    }
     int mtrimx = 2, niter1 = 0;
     double rate1 = 0.;
     for (int mtri = 1; mtri <= mtrimx; ++mtri) {

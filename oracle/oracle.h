@@ -45,6 +45,7 @@ void orc_precon(orc *o, const double *rhs, double *p, double *r, int iprc, int i
 void orc_gcrk(orc *o, double *p, const double *u1, const double *v1, const double *w1,
               double *u2, double *v2, double *w2, int impfl, mpg_gcr_stats *st);
 void orc_mpdatamper(orc *o, double *unk, int iflag);
+void orc_mpdatam(orc *o, double *unk, int iflag);
 void orc_courant(orc *o, int iflag, mpg_diag *diag);
 void orc_stats(orc *o, mpg_diag *diag);
 void orc_setup(orc *o, mpg_diag *diag);

@@ -45,6 +45,7 @@ def lib():
         L.orc_precon.argtypes = [vp, dp, dp, dp, ip, ip]
         L.orc_gcrk.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, ip, vp]
         L.orc_mpdatamper.argtypes = [vp, dp, ip]
+        L.orc_mpdatam.argtypes = [vp, dp, ip]
         L.orc_courant.argtypes = [vp, ip, vp]
         L.orc_stats.argtypes = [vp, vp]
         L.orc_setup.argtypes = [vp, vp]
@@ -149,6 +150,11 @@ class Oracle:
     def mpdatamper(self, unk, iflag):
         u = np.array(unk, np.float64)
         self.L.orc_mpdatamper(self.h, _p(u), iflag)
+        return u
+
+    def mpdatam(self, unk, iflag):
+        u = np.array(unk, np.float64)
+        self.L.orc_mpdatam(self.h, _p(u), iflag)
         return u
 
     # ---- driver

@@ -3,7 +3,7 @@
 Method names and argument meaning follow the reference subroutines of
 lippsLFroude_implgwopks3D_unstr3.f: ``gcrk`` (ref.f:1776), ``prfr`` (ref.f:1536),
 ``laplc`` (ref.f:1288), ``div`` (ref.f:2096), ``derivative`` (ref.f:3943), ``precon``
-(ref.f:482), ``bcv`` (ref.f:1583), ``mpdatamper`` (ref.f:3617), ``courant`` (ref.f:1974),
+(ref.f:482), ``bcv`` (ref.f:1583), ``mpdatamper`` (ref.f:3617), ``mpdatam`` (ref.f:3029), ``courant`` (ref.f:1974),
 ``stats`` (ref.f:2847), and the driver ``mpsolver`` split into ``setup`` (ref.f:99-273) and
 ``step`` (one DO ITIME pass, ref.f:285-463).  Arrays passed in or out are in the reference
 node order.  The CUDA library must be built (``__graft_entry__.build()``); there is no CPU
@@ -26,7 +26,7 @@ _lib = None
 EXPORTS = [
     "mpg_create", "mpg_destroy", "mpg_last_error", "mpg_get_info", "mpg_set_field", "mpg_get_field",
     "mpg_derivative", "mpg_bcv", "mpg_laplc", "mpg_prfr", "mpg_div", "mpg_precon", "mpg_gcrk",
-    "mpg_mpdatamper", "mpg_courant", "mpg_stats", "mpg_setup", "mpg_step", "mpg_half_forcing",
+    "mpg_mpdatamper", "mpg_mpdatam", "mpg_courant", "mpg_stats", "mpg_setup", "mpg_step", "mpg_half_forcing",
     "mpg_explicit_forcing", "mpg_post_solve", "mpg_extrapolate", "mpg_get_gcr_stats",
     "mpg_synchronize", "mpg_analyze_mesh", "mpg_get_stream", "mpg_kernel_timing", "mpg_kernel_times",
     "mpg_laplc_noalloc", "mpg_learned_init", "mpg_learned_set_params", "mpg_learned_get_params",
@@ -66,6 +66,7 @@ def lib():
         L.mpg_precon.argtypes = [vp, ip, ip, ip, ip, ip]
         L.mpg_gcrk.argtypes = [vp] + [ip] * 8 + [vp]
         L.mpg_mpdatamper.argtypes = [vp, ip, ip]
+        L.mpg_mpdatam.argtypes = [vp, ip, ip]
         L.mpg_courant.argtypes = [vp, ip, vp]
         L.mpg_stats.argtypes = [vp, vp]
         L.mpg_setup.argtypes = [vp, vp]
@@ -195,6 +196,10 @@ class Solver:
 
     def mpdatamper(self, unk: int, iflag: int) -> None:
         _check(self.L.mpg_mpdatamper(self.h, unk, iflag))
+
+    def mpdatam(self, unk: int, iflag: int) -> None:
+        """Open-boundary MPDATA (ref.f:3029-3311), for ``iper = 0``."""
+        _check(self.L.mpg_mpdatam(self.h, unk, iflag))
 
     def courant(self, iflag: int = 1) -> MpgDiag:
         d = MpgDiag()

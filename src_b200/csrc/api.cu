@@ -1036,9 +1036,11 @@ int op_aun(mpg_handle h) {
     return h->P.precision == MPG_PREC_MIXED ? op_aun_t<float>(h) : op_aun_t<double>(h);
 }
 
-// one mpdatamper call; T is the type of the face fluxes and the intermediate node fields
+// one mpdatamper call (iper = 2) or mpdatam call (iper = 0); T is the type of the face fluxes
+// and the intermediate node fields; iflag names the field as in the reference (1-4: u, v, w,
+// theta'; passive scalars, not in the reference, follow with inflow value 0)
 template <class T>
-int op_mpdata_field_t(mpg_handle h, double *psi) {
+int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
     using B = MpBuf<T>;
     using G = Buf<T>;
     const T dt = (T)h->P.delt;
@@ -1047,7 +1049,15 @@ int op_mpdata_field_t(mpg_handle h, double *psi) {
     auto &S = B::S(h);
     {
         KTIME(KT_MP_DONOR);
-        k_mp_donor<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h));
+        if (h->P.iper == 2) {
+            k_mp_donor<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h),
+                                                                  MpInflow{nullptr, 0., 0});
+        } else {
+            // afree = (u0inf, v0inf, w0inf, 0, 1) (ref.f:125-129); iflag = 1 takes ue per node
+            const double af = iflag == 2 ? h->P.v0inf : iflag == 3 ? h->P.w0inf : 0.;
+            k_mp_donor<T, true><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h),
+                                                                 MpInflow{h->ue, af, iflag});
+        }
     }
     {
         KTIME(KT_MP_GRADB);
@@ -1074,8 +1084,9 @@ int op_mpdata_field_t(mpg_handle h, double *psi) {
     }
     return check_launch("mpdata");
 }
-int op_mpdata_field(mpg_handle h, double *psi) {
-    return h->P.precision == MPG_PREC_MIXED ? op_mpdata_field_t<float>(h, psi) : op_mpdata_field_t<double>(h, psi);
+int op_mpdata_field(mpg_handle h, double *psi, int iflag) {
+    return h->P.precision == MPG_PREC_MIXED ? op_mpdata_field_t<float>(h, psi, iflag)
+                                            : op_mpdata_field_t<double>(h, psi, iflag);
 }
 
 Fields make_fields(mpg_handle h) {
@@ -1561,17 +1572,23 @@ extern "C" int mpg_get_gcr_stats(mpg_handle h, mpg_gcr_stats *stats) {
     return MPG_OK;
 }
 
-extern "C" int mpg_mpdatamper(mpg_handle h, int unk, int iflag) {
+static int mpdata_entry(mpg_handle h, int unk, int iflag, int iper) {
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
-    (void)iflag;
-    if (h->P.iper != 2) return mpg_fail(MPG_ERR_UNSUPPORTED, "mpdatam (iper=0 inflow closure) is not provided");
+    if (h->P.iper != iper)
+        return mpg_fail(MPG_ERR_ARG, iper == 2 ? "mpdatamper needs iper = 2 (use mpg_mpdatam for iper = 0)"
+                                               : "mpdatam needs iper = 0 (use mpg_mpdatamper for iper = 2)");
+    if (iflag < 1) return mpg_fail(MPG_ERR_ARG, "iflag must be >= 1");
     FLD(psi, unk);
     for (int q = 0; q < 3; ++q)
         if (!fld(h, MPG_F_UUU + q)) return mpg_fail(MPG_ERR_NOMEM, "uuu");
     int rc = op_aun(h);
     if (rc) return rc;
-    return op_mpdata_field(h, psi);
+    return op_mpdata_field(h, psi, iflag);
 }
+
+extern "C" int mpg_mpdatamper(mpg_handle h, int unk, int iflag) { return mpdata_entry(h, unk, iflag, 2); }
+
+extern "C" int mpg_mpdatam(mpg_handle h, int unk, int iflag) { return mpdata_entry(h, unk, iflag, 0); }
 
 extern "C" int mpg_courant(mpg_handle h, int iflag, mpg_diag *diag) {
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
@@ -1684,15 +1701,14 @@ extern "C" int mpg_velprd(mpg_handle h) {
 // One pass of DO ITIME (ref.f:285-463), driving the entry points above in mpsolver's order.
 extern "C" int mpg_step(mpg_handle h, mpg_diag *diag) {
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
-    if (h->P.iper != 2) return mpg_fail(MPG_ERR_UNSUPPORTED, "mpdatam (iper=0 inflow closure) is not provided");
     int rc;
     Fields F = make_fields(h);
     if ((rc = mpg_half_forcing(h))) return rc;
     if ((rc = op_aun(h))) return rc;                          // uuu is fixed over the advection calls
-    for (int q = 0; q < 4 + h->P.nscal; ++q) {
+    for (int q = 0; q < 4 + h->P.nscal; ++q) {                // mpdatamper or mpdatam, ref.f:308-319
         double *psi = fld(h, MPG_F_UNK + q);
         if (!psi) return mpg_fail(MPG_ERR_NOMEM, "unk");
-        if ((rc = op_mpdata_field(h, psi))) return rc;
+        if ((rc = op_mpdata_field(h, psi, q + 1))) return rc;
     }
     double *prpot = fld(h, MPG_F_PRPOT);
     int niter1 = 0, fallbacks = 0;

@@ -1,10 +1,12 @@
-// MPDATA (mpdatamper, lippsLFroude_implgwopks3D_unstr3.f:3617-3941), the node loops of the
+// MPDATA (mpdatamper, lippsLFroude_implgwopks3D_unstr3.f:3617-3941, and its open-boundary twin
+// mpdatam, ref.f:3029-3311), the node loops of the
 // time-step driver mpsolver (ref.f:285-463) and the per-step diagnostics (ref.f:1974-2170,
 // ref.f:2847-2912) as device kernels.
 //
 // MPDATA per field, iord = 2 with the nonoscillatory option (ifct = 1):
 //   k_aun            once per step: advective face flux aun = (U_a+U_b)/2 . S    (ref.f:3690-3693)
-//   k_mp_donor       donor-cell pass and update psi1 = psi - dt*arh2/(vol*rh0)    (ref.f:3687-3747)
+//   k_mp_donor       donor-cell pass and update psi1 = psi - dt*arh2/(vol*rh0)    (ref.f:3687-3747;
+//                    with the open-boundary closure of mpdatam, ref.f:3085-3172)
 //   k_mp_grad_bounds derivative(psi1) x3 and the FCT bounds mx/mn                 (ref.f:3755-3817)
 //   k_mp_anti_{h,v}  antidiffusive face flux A (infinite-gauge form)              (ref.f:3760-3794)
 //   k_mp_cpcn        in/out sums of A and the limiter ratios cp, cn               (ref.f:3871-3909)
@@ -70,14 +72,26 @@ __device__ __forceinline__ bool has_boundary(const ColMesh &M, int c, int k) {
     return any;
 }
 
-// donor-cell pass: fl = psi_a*max(0,aun) + psi_b*min(0,aun); a gets +fl, b gets -fl
-template <class T>
+// inflow data of the open-boundary closure (mpdatam): the field's free-stream value afree(iflag),
+// or the ambient ue per node for iflag = 1 (ref.f:3154-3155)
+struct MpInflow {
+    const double *ue;     // used when iflag == 1
+    double afree;         // used otherwise
+    int iflag;
+};
+
+// donor-cell pass: fl = psi_a*max(0,aun) + psi_b*min(0,aun); a gets +fl, b gets -fl.
+// OPEN selects mpdatam's first-pass boundary closure (ref.f:3143-3169): every boundary point
+// of a type other than 11, 5 or 6 carries the flux aunbb1 = -divv that balances the node's face
+// fluxes, donor-cell upwinded with the free-stream value on inflow.  mpdatamper adds zero there
+// (ref.f:3732-3738).
+template <class T, bool OPEN>
 __global__ void k_mp_donor(ColMesh M, MpScratchT<T> S, const double *__restrict__ psi,
                            const T *__restrict__ vol, const T *__restrict__ rh0, T dt,
-                           T *__restrict__ psi1) {
+                           T *__restrict__ psi1, MpInflow in) {
     NODE_BEGIN
     const T pn = (T)psi[n];
-    T arh2 = 0.;
+    T arh2 = 0., divv = 0.;
     for_faces(M, c, k, n,
         [&](const Face &f) { return V4T<T>{(f.vert ? S.aunv : S.aunh)[f.si], (T)psi[f.j], T(0), T(0)}; },
         [&](const Face &f, const V4T<T> &v) {
@@ -85,8 +99,19 @@ __global__ void k_mp_donor(ColMesh M, MpScratchT<T> S, const double *__restrict_
             const T pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
             const T fl = pa * (T(0) > aun ? T(0) : aun) + pb * (T(0) < aun ? T(0) : aun);
             arh2 = f.sub ? arh2 - fl : arh2 + fl;
+            if (OPEN) divv = f.sub ? divv - aun : divv + aun;
         });
-    if (has_boundary(M, c, k)) arh2 = arh2 + T(0) * T(1);      // zero boundary flux, ref.f:3732-3738
+    if (OPEN) {
+        for_boundary(M, c, k, [&](const BEntry &be) {
+            const T aunbb1 = -divv;
+            const T fin = in.iflag == 1 ? (T)in.ue[n] : (T)in.afree;
+            T fl1 = fin * (T(0) < aunbb1 ? T(0) : aunbb1) + pn * (T(0) > aunbb1 ? T(0) : aunbb1);
+            if (be.type == 11 || be.type == 5 || be.type == 6) fl1 = T(0);
+            arh2 = arh2 + fl1 * T(1);
+        });
+    } else if (has_boundary(M, c, k)) {
+        arh2 = arh2 + T(0) * T(1);
+    }
     psi1[n] = pn - arh2 * dt / vol[n] / rh0[n];
 }
 

@@ -71,6 +71,12 @@ class ColumnMesh:
     W: np.ndarray           # (NC,) volume per unit dzeta
     zeta: np.ndarray        # (L,) computational levels
     zeta_half: np.ndarray   # (L+1,) half levels (0 ... H)
+    periodic: bool = True
+    # open (non-periodic) meshes only: one lateral boundary entry per boundary column and
+    # side, (column, type, Tx, Ty) with T the outward face vector per unit dzeta
+    bcol: Optional[np.ndarray] = None     # (nb,) int64
+    btype: Optional[np.ndarray] = None    # (nb,) int32: 7 inflow x=0, 8 outflow x=Lx, 5 y=0, 6 y=Ly
+    bT: Optional[np.ndarray] = None       # (nb, 2)
 
     @property
     def ncol(self) -> int:
@@ -129,13 +135,48 @@ class RefMesh:
 # ----------------------------------------------------------------------------------
 # generator
 # ----------------------------------------------------------------------------------
-def agnesi(x, y, Lx, Ly, h0, a):
+def agnesi(x, y, Lx, Ly, h0, a, periodic=True):
     """Witch-of-Agnesi hill centred in the domain, periodic via minimum image."""
     dx = np.asarray(x) - 0.5 * Lx
     dy = np.asarray(y) - 0.5 * Ly
-    dx = dx - Lx * np.round(dx / Lx)
-    dy = dy - Ly * np.round(dy / Ly)
+    if periodic:
+        dx = dx - Lx * np.round(dx / Lx)
+        dy = dy - Ly * np.round(dy / Ly)
     return h0 / (1.0 + (dx * dx + dy * dy) / (a * a)) ** 1.5
+
+
+def _open_delaunay(pts: np.ndarray, Lx: float, Ly: float):
+    """Delaunay triangulation of a point set whose hull is the rectangle [0,Lx]x[0,Ly].
+
+    Points on the sides are collinear, which Qhull may drop as coplanar.  The
+    triangulation is therefore computed on a copy whose side points bulge outward by a
+    tiny amount (a strictly convex hull, every point a vertex) and then used with the
+    true positions; triangles are checked for positive area there.
+    """
+    from scipy.spatial import Delaunay
+
+    q = pts.copy()
+    u = q[:, 0] / Lx
+    v = q[:, 1] / Ly
+    eps = 1e-6
+    q[:, 0] += np.where(u <= 0.0, -eps * Lx * np.sin(np.pi * v), 0.0)
+    q[:, 0] += np.where(u >= 1.0, eps * Lx * np.sin(np.pi * v), 0.0)
+    q[:, 1] += np.where(v <= 0.0, -eps * Ly * np.sin(np.pi * u), 0.0)
+    q[:, 1] += np.where(v >= 1.0, eps * Ly * np.sin(np.pi * u), 0.0)
+    simp = Delaunay(q).simplices.astype(np.int64)
+    P = pts[simp]
+    cr = ((P[:, 1, 0] - P[:, 0, 0]) * (P[:, 2, 1] - P[:, 0, 1])
+          - (P[:, 1, 1] - P[:, 0, 1]) * (P[:, 2, 0] - P[:, 0, 0]))
+    flip = cr < 0
+    simp[flip] = simp[flip][:, [0, 2, 1]]
+    P = pts[simp]
+    cr = np.abs(cr)
+    h2 = Lx * Ly / pts.shape[0]
+    if cr.min() < 1e-3 * h2:
+        raise RuntimeError("open Delaunay produced a degenerate triangle")
+    if abs(0.5 * cr.sum() - Lx * Ly) > 1e-9 * Lx * Ly:
+        raise RuntimeError("open Delaunay does not cover the rectangle")
+    return simp, P
 
 
 def _periodic_delaunay(pts: np.ndarray, Lx: float, Ly: float, margin: float):
@@ -191,23 +232,43 @@ def level_set(L: int, H: float, stretch_dz0: Optional[float] = None) -> np.ndarr
 def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
              Ly: Optional[float] = None, H: float = 20e3, h0: float = 400.0,
              half_width: float = 10e3, jitter: float = 0.3, seed: int = 0,
-             stretch_dz0: Optional[float] = None) -> ColumnMesh:
-    """Build the jittered periodic prism-column mesh (see module docstring)."""
+             stretch_dz0: Optional[float] = None, periodic: bool = True) -> ColumnMesh:
+    """Build the jittered prism-column mesh (see module docstring).
+
+    ``periodic=False`` builds the open channel used with ``iper = 0``: ``nx * ny`` nodes
+    from corner to corner of the rectangle, side nodes jittered along their side only,
+    corners fixed, and lateral boundary points on the four sides: inflow (type 7) at
+    ``x = 0``, outflow (type 8) at ``x = Lx``, walls (types 5 and 6) at ``y = 0`` and
+    ``y = Ly``.  A side node's lateral face is the vertical strip over its two half side
+    edges, ``dzeta_k * sum 0.5*(s_A + s_B) * rot(B - A)`` like the interior faces.
+    """
     ny = nx if ny is None else ny
     Ly = Lx if Ly is None else Ly
-    hx, hy = Lx / nx, Ly / ny
     rng = np.random.default_rng(seed)
     I, J = np.meshgrid(np.arange(nx), np.arange(ny), indexing="xy")
-    base = np.stack([(I.ravel() + 0.5) * hx, (J.ravel() + 0.5) * hy], axis=1)
+    if periodic:
+        hx, hy = Lx / nx, Ly / ny
+        base = np.stack([(I.ravel() + 0.5) * hx, (J.ravel() + 0.5) * hy], axis=1)
+    else:
+        hx, hy = Lx / (nx - 1), Ly / (ny - 1)
+        base = np.stack([I.ravel() * hx, J.ravel() * hy], axis=1)
     jit = rng.uniform(-jitter, jitter, size=base.shape) * np.array([hx, hy])
+    if not periodic:
+        iside = (I.ravel() == 0) | (I.ravel() == nx - 1)
+        jside = (J.ravel() == 0) | (J.ravel() == ny - 1)
+        jit[iside, 0] = 0.0
+        jit[jside, 1] = 0.0
     xy = base + jit
     ncol = xy.shape[0]
 
-    tri, P = _periodic_delaunay(xy, Lx, Ly, margin=4.0 * max(hx, hy))
-    hnode = agnesi(xy[:, 0], xy[:, 1], Lx, Ly, h0, half_width)
+    if periodic:
+        tri, P = _periodic_delaunay(xy, Lx, Ly, margin=4.0 * max(hx, hy))
+    else:
+        tri, P = _open_delaunay(xy, Lx, Ly)
+    hnode = agnesi(xy[:, 0], xy[:, 1], Lx, Ly, h0, half_width, periodic)
 
     def hf(p):
-        return agnesi(p[..., 0], p[..., 1], Lx, Ly, h0, half_width)
+        return agnesi(p[..., 0], p[..., 1], Lx, Ly, h0, half_width, periodic)
 
     nt = tri.shape[0]
     g = P.mean(axis=1)                                      # (nt, 2)
@@ -224,11 +285,11 @@ def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
     b = np.maximum(p_idx, q_idx)
     key = (a * ncol + b).ravel()
     ukey, inv, cnt = np.unique(key, return_inverse=True, return_counts=True)
-    if not np.all(cnt == 2):
+    if periodic and not np.all(cnt == 2):
         raise RuntimeError("torus triangulation has an edge not shared by two triangles")
     edges2d = np.stack([ukey // ncol, ukey % ncol], axis=1)
     ne2 = edges2d.shape[0]
-    if ne2 != 3 * ncol:
+    if periodic and ne2 != 3 * ncol:
         raise RuntimeError(f"expected {3 * ncol} edges, got {ne2}")
 
     # lateral face vectors: segment midpoint -> centroid, oriented p -> q, flipped to a -> b
@@ -258,6 +319,40 @@ def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
                 A[:, d] += np.bincount(node, weights=s[:, d], minlength=ncol)
             W += np.bincount(node, weights=s[:, 2] * (1.0 - hbar / H), minlength=ncol)
 
+    bcol = btype = bT = None
+    if not periodic:
+        # side half-edges of the boundary edges (one triangle each), CCW so the domain is on
+        # the left and rot(B - A) = (dy, -dx) is the outward normal
+        bmask = (cnt[inv] == 1).reshape(-1, 3)
+        t_i, e_i = np.nonzero(bmask)
+        Pp_b, Pq_b, M_b = Pp[t_i, e_i], Pq[t_i, e_i], M[t_i, e_i]
+        sp = 1.0 - hnode[p_idx[t_i, e_i]] / H
+        sq = 1.0 - hnode[q_idx[t_i, e_i]] / H
+        sm = smid[t_i, e_i]
+
+        def rot(v):
+            return np.stack([v[:, 1], -v[:, 0]], axis=1)
+
+        tp = (0.5 * (sp + sm))[:, None] * rot(M_b - Pp_b)
+        tq = (0.5 * (sm + sq))[:, None] * rot(Pq_b - M_b)
+        tol = 1e-9 * max(Lx, Ly)
+        side = np.full(t_i.shape[0], -1)
+        side[np.abs(M_b[:, 0]) < tol] = 0                       # x = 0: inflow
+        side[np.abs(M_b[:, 0] - Lx) < tol] = 1                  # x = Lx: outflow
+        side[np.abs(M_b[:, 1]) < tol] = 2                       # y = 0: wall
+        side[np.abs(M_b[:, 1] - Ly) < tol] = 3                  # y = Ly: wall
+        if np.any(side < 0):
+            raise RuntimeError("open mesh has a boundary edge off the rectangle's sides")
+        cols = np.concatenate([p_idx[t_i, e_i], q_idx[t_i, e_i]])
+        sides = np.concatenate([side, side])
+        key2 = sides * ncol + cols
+        uk, inv2 = np.unique(key2, return_inverse=True)
+        tt = np.concatenate([tp, tq])
+        bT = np.stack([np.bincount(inv2, weights=tt[:, 0], minlength=uk.shape[0]),
+                       np.bincount(inv2, weights=tt[:, 1], minlength=uk.shape[0])], axis=1)
+        bcol = (uk % ncol).astype(np.int64)
+        btype = np.array([7, 8, 5, 6], dtype=np.int32)[uk // ncol]
+
     zeta = level_set(L, H, stretch_dz0)
     zh = np.empty(L + 1)
     zh[0] = 0.0
@@ -265,7 +360,8 @@ def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
     zh[L] = H
     return ColumnMesh(nx=nx, ny=ny, L=L, Lx=Lx, Ly=Ly, H=H, h0=h0, half_width=half_width,
                       xy=xy, hnode=hnode, tri=tri, edges2d=edges2d.astype(np.int64), T=T,
-                      A=A, W=W, zeta=zeta, zeta_half=zh)
+                      A=A, W=W, zeta=zeta, zeta_half=zh, periodic=periodic,
+                      bcol=bcol, btype=btype, bT=bT)
 
 
 def expand_reference(cm: ColumnMesh) -> RefMesh:
@@ -273,7 +369,8 @@ def expand_reference(cm: ColumnMesh) -> RefMesh:
 
     Node ``c*L + k`` is column ``c`` at level ``k``.  Horizontal edge ``e*L + k`` joins
     ``(a,k)`` and ``(b,k)``; vertical edge ``NE2*L + c*(L-1) + k`` joins ``(c,k)`` and
-    ``(c,k+1)``.  Boundary points: bottoms of all columns, then tops.
+    ``(c,k+1)``.  Boundary points: bottoms of all columns, then tops, then (open meshes)
+    the lateral side points.
     """
     L, NC, NE2, H = cm.L, cm.ncol, cm.edges2d.shape[0], cm.H
     dz = cm.dzeta
@@ -304,15 +401,27 @@ def expand_reference(cm: ColumnMesh) -> RefMesh:
     sn[nh:, 1] = (cm.A[:, 1:2] * fac[None, :]).ravel()
     sn[nh:, 2] = np.repeat(cm.A[:, 2], L - 1)
 
-    nboun = 2 * NC
+    nlat = 0 if cm.periodic else cm.bcol.shape[0] * L
+    nboun = 2 * NC + nlat
     ibpoin = np.empty((nboun, 2), dtype=np.int32)
     ibpoin[:NC, 0] = cs * L
-    ibpoin[NC:, 0] = cs * L + (L - 1)
-    ibpoin[:, 1] = 11
+    ibpoin[NC:2 * NC, 0] = cs * L + (L - 1)
+    ibpoin[:2 * NC, 1] = 11
     sbb = np.zeros((nboun, 3))
     sbb[:NC] = -cm.A
-    sbb[NC:, 2] = cm.A[:, 2]
-    anp = sbb / np.linalg.norm(sbb, axis=1)[:, None]
+    sbb[NC:2 * NC, 2] = cm.A[:, 2]
+    anp = np.zeros((nboun, 3))
+    anp[:2 * NC] = sbb[:2 * NC] / np.linalg.norm(sbb[:2 * NC], axis=1)[:, None]
+    if nlat:
+        # lateral side points, entry by entry over the levels of each (column, side)
+        ibpoin[2 * NC:, 0] = (cm.bcol[:, None] * L + ks[None, :]).ravel()
+        ibpoin[2 * NC:, 1] = np.repeat(cm.btype, L)
+        sbb[2 * NC:, 0] = (cm.bT[:, 0:1] * dz[None, :]).ravel()
+        sbb[2 * NC:, 1] = (cm.bT[:, 1:2] * dz[None, :]).ravel()
+        unit = {7: (-1.0, 0.0), 8: (1.0, 0.0), 5: (0.0, -1.0), 6: (0.0, 1.0)}
+        nrm = np.array([unit[int(t)] for t in cm.btype])
+        anp[2 * NC:, 0] = np.repeat(nrm[:, 0], L)
+        anp[2 * NC:, 1] = np.repeat(nrm[:, 1], L)
     z2 = np.zeros((0, 2), dtype=np.int32)
     return RefMesh(npoin=npoin, nedge=nedge, nbface=0, nboun=nboun, coord=coord, vol=vol,
                    iedge=iedge, sn=sn, kbface=z2.copy(), sb=np.zeros((0, 3)), ibpoin=ibpoin,

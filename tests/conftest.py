@@ -34,3 +34,12 @@ def c1_mesh():
     from src_b200 import mesh
     cm = mesh.generate(48, L=41, seed=0, h0=400.0)
     return cm, cm.to_reference()
+
+
+@pytest.fixture(scope="session")
+def open_mesh():
+    """Open channel (iper = 0): 12x12 columns from corner to corner of the 120 km square, 9
+    levels, inflow at x = 0 (type 7), outflow at x = Lx (8), walls at y = 0 and y = Ly (5, 6)."""
+    from src_b200 import mesh
+    cm = mesh.generate(12, L=9, seed=5, periodic=False)
+    return cm, cm.to_reference()

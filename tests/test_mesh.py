@@ -85,3 +85,23 @@ def test_reference_input_files(tmp_path, small_mesh):
         assert (tmp_path / name).exists()
     lines = (tmp_path / "inputinc.d").read_text().splitlines()
     assert lines[1].split()[5] == "2"   # iper
+
+
+def test_open_channel_counts_and_closure(open_mesh):
+    """Open channel: a triangulated rectangle has 3V - 3 - V_b edges; every dual cell closes with
+    its lateral side faces, which point along the side's outward normal."""
+    cm, rm = open_mesh
+    nbv = np.unique(cm.bcol).shape[0]
+    assert nbv == 2 * (cm.nx + cm.ny) - 4
+    assert cm.edges2d.shape[0] == 3 * cm.ncol - 3 - nbv
+    assert cm.tri.shape[0] == 2 * cm.ncol - 2 - nbv
+    res = mesh.closure_residual(rm, include_boundary=True)
+    assert np.abs(res).max() <= 1e-12 * np.abs(rm.sn).max()
+    lat = rm.ibpoin[:, 1] != 11
+    assert rm.ibpoin.shape[0] == 2 * cm.ncol + cm.bcol.shape[0] * cm.L
+    n = rm.sbb[lat] / np.linalg.norm(rm.sbb[lat], axis=1)[:, None]
+    assert np.allclose(n, rm.anp[lat], atol=1e-12)
+    assert sorted(np.unique(rm.ibpoin[lat, 1]).tolist()) == [5, 6, 7, 8]
+    # corner columns sit on two sides
+    assert np.bincount(cm.bcol).max() == 2 and np.sum(np.bincount(cm.bcol) == 2) == 4
+    assert np.isclose(cm.W.sum() * cm.H, rm.vol.sum(), rtol=1e-12)
