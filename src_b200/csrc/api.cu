@@ -1061,8 +1061,12 @@ int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
     }
     {
         KTIME(KT_MP_GRADB);
-        k_mp_grad_bounds<T><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), B::g(h, 0), B::g(h, 1), B::g(h, 2),
-                                                             B::mx(h), B::mn(h));
+        if (h->P.iper == 2)
+            k_mp_grad_bounds<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), B::g(h, 0), B::g(h, 1),
+                                                                        B::g(h, 2), B::mx(h), B::mn(h));
+        else
+            k_mp_grad_bounds<T, true><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), B::g(h, 0), B::g(h, 1),
+                                                                       B::g(h, 2), B::mx(h), B::mn(h));
     }
     AntiArgs<T> A{B::psi1(h), B::g(h, 0), B::g(h, 1), B::g(h, 2), vol, rh0,
                   U3{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}}, dt};

@@ -115,8 +115,9 @@ __global__ void k_mp_donor(ColMesh M, MpScratchT<T> S, const double *__restrict_
     psi1[n] = pn - arh2 * dt / vol[n] / rh0[n];
 }
 
-// gradient of psi1 (three derivative calls) and the neighbourhood max/min
-template <class T>
+// gradient of psi1 (three derivative calls) and the neighbourhood max/min; OPEN adds the
+// derivative's boundary closure of iper = 0 (mpdatam)
+template <class T, bool OPEN>
 __global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, T *__restrict__ gx,
                                  T *__restrict__ gy, T *__restrict__ gz,
                                  T *__restrict__ mx, T *__restrict__ mn) {
@@ -141,6 +142,13 @@ __global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, T *__res
             lo = lo < pn ? lo : pn;
             lo = lo < pj ? lo : pj;
         });
+    if (OPEN) {                                         // derivative's closure, ref.f:4007-4014
+        for_boundary(M, c, k, [&](const BEntry &be) {
+            ax = ax + T(be.sbb[0]) * pn;
+            ay = ay + T(be.sbb[1]) * pn;
+            az = az + T(be.sbb[2]) * pn;
+        });
+    }
     gx[n] = ax; gy[n] = ay; gz[n] = az;
     mx[n] = hi; mn[n] = lo;
 }
