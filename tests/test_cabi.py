@@ -49,6 +49,15 @@ def test_analyze_column_mesh(small_mesh):
     assert info["bitwise_order"]
 
 
+def test_analyze_open_channel(open_mesh):
+    """The iper = 0 channel (lateral boundary points at every level) is a column mesh too, and
+    its per-node sums keep the reference's edge order."""
+    cm, rm = open_mesh
+    info = api.analyze_mesh(rm)
+    assert info["ncol"] == cm.ncol and info["nlev"] == cm.L
+    assert info["nedge2d"] == cm.edges2d.shape[0] and info["bitwise_order"]
+
+
 def test_analyze_permuted_mesh(small_mesh):
     """Node and edge numbering are free: a shuffled mesh is still recognised."""
     cm, rm = small_mesh

@@ -105,3 +105,17 @@ def test_open_channel_counts_and_closure(open_mesh):
     # corner columns sit on two sides
     assert np.bincount(cm.bcol).max() == 2 and np.sum(np.bincount(cm.bcol) == 2) == 4
     assert np.isclose(cm.W.sum() * cm.H, rm.vol.sum(), rtol=1e-12)
+
+
+def test_open_channel_files(tmp_path, open_mesh):
+    """The channel writes and reads back in the reference's iper = 0 layout (no periodic lists),
+    and the control file carries iper = 0."""
+    from src_b200.cabi import RunParams
+    _, rm = open_mesh
+    mesh.write_reference_inputs(str(tmp_path), rm, RunParams(iper=0))
+    back = mesh.read_mesh3d(str(tmp_path / "mesh3d.d"), iper=0)
+    assert back.nboun == rm.nboun
+    assert np.array_equal(back.ibpoin, rm.ibpoin) and np.array_equal(back.sbb, rm.sbb)
+    assert np.array_equal(back.iedge, rm.iedge) and np.array_equal(back.sn, rm.sn)
+    lines = (tmp_path / "inputinc.d").read_text().splitlines()
+    assert lines[1].split()[5] == "0"
