@@ -62,3 +62,16 @@ def test_single_rank_is_identity():
     import bench
     assert bench.max_over_ranks(42.0) == 42.0
     assert bench.whole_job_rate(1, 10, 2.0) == 5.0
+
+
+def test_reference_arm_sums_replicas():
+    """`bench.py --impl reference` runs one serial oracle replica per requested host thread and
+    reports their summed throughput on the workload's metric, with the core count."""
+    import json
+    import subprocess
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "3", "--ref-replicas", "2"],
+                         capture_output=True, text=True, timeout=600, check=True).stdout
+    line = json.loads(out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["cores"] == 2 and line["e2e"]["value"] == line["value"]
