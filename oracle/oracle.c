@@ -8,7 +8,8 @@
  * -O2 -ffp-contract=off (no FMA contraction, no fast-math).
  *
  * Reference options restated: isfera=0 only (the spherical variant is out of scope),
- * iper=0 or 2, mg_flag=0, ielast=0, itraj=0 or 1 (velprd).  Extensions beyond the reference
+ * iper=0 (open boundaries, mpdatam) or 2 (periodic, mpdatamper), mg_flag=0, ielast=0,
+ * itraj=0 or 1 (velprd).  Extensions beyond the reference
  * are marked NEW: the vertical-line preconditioner (iprc=2), runtime lord/itmn, passive
  * scalars, the FP64 mass sums and the per-solve residual contraction.
  */
