@@ -251,24 +251,53 @@ def _replica_sample(args):
     return (time.perf_counter() - t0) / steps, rm.npoin
 
 
+REF_MAX_REPLICAS = 64          # bounds the reference arm's memory (about 160 MB per replica)
+
+
 def host_threads():
+    """Host threads this process may use: its CPU affinity, lowered to a cgroup CPU quota."""
     try:
-        return len(os.sched_getaffinity(0))
+        n = len(os.sched_getaffinity(0))
     except AttributeError:
-        return os.cpu_count() or 1
+        n = os.cpu_count() or 1
+    for path in ("/sys/fs/cgroup/cpu.max", "/sys/fs/cgroup/cpu/cpu.cfs_quota_us"):
+        try:
+            f = open(path).read().split()
+            if path.endswith("cpu.max") and f[0] != "max":
+                n = min(n, max(1, int(int(f[0]) / int(f[1]))))
+            elif path.endswith("quota_us") and int(f[0]) > 0:
+                period = int(open("/sys/fs/cgroup/cpu/cpu.cfs_period_us").read())
+                n = min(n, max(1, int(f[0]) // period))
+        except (OSError, ValueError, IndexError):
+            pass
+    return n
+
+
+def reference_replicas(requested=0):
+    """Replicas for the reference arm: one per usable host thread (or as requested), at most
+    REF_MAX_REPLICAS and at most what a quarter of the available memory holds at 400 MB each."""
+    n = host_threads() if requested <= 0 else min(requested, host_threads())
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable:"):
+                n = min(n, max(1, int(ln.split()[1]) * 1024 // 4 // (400 << 20)))
+    except OSError:
+        pass
+    return max(1, min(n, REF_MAX_REPLICAS))
 
 
 def run_reference(args):
     """The reference's path on the host cores.  The reference is serial Fortran (no compiler for
-    it here), so its restatement runs as one independent replica per host thread, started
-    together (spawned processes), and the throughput of all replicas is summed."""
+    it here), so its restatement runs as one independent replica per usable host thread (at most
+    REF_MAX_REPLICAS, and as many as memory allows), started together in spawned processes, and
+    the throughput of all replicas is summed."""
     rank, _, world = dist_env()
     if rank != 0:
         return
     import multiprocessing as mp
     nx, L = WORKLOADS[DEFAULT][0], WORKLOADS[DEFAULT][1]
     n_work = nx * nx * L
-    nrep = max(1, min(host_threads(), args.ref_replicas or host_threads()))
+    nrep = reference_replicas(args.ref_replicas)
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(nrep)
     with ctx.Pool(nrep, initializer=_replica_init, initargs=(barrier,)) as pool:
