@@ -49,6 +49,7 @@ struct orc {
     int nvert_e;
     int *vedge;         /* vertical edges: index into the combined edge list */
     int blocked;        /* 1: global sums in the GPU's reduction order (see rsum) */
+    int ref_bugs;       /* 1 (default): reproduce the corner-minimum slip of ref.f:3853-3866 */
 };
 
 /* ------------------------------------------------------------------ helpers */
@@ -117,6 +118,7 @@ static double rsum(const orc *o, const double *v, int n) {
 }
 
 void orc_set_reduction(orc *o, int blocked) { o->blocked = blocked ? 1 : 0; }
+void orc_set_ref_bugs(orc *o, int on) { o->ref_bugs = on ? 1 : 0; }
 
 /* cyclicr, cyclicr2, cyclicr4 — ref.f:4377-4446 */
 static void cyclicr(orc *o, double *u) {
@@ -704,13 +706,15 @@ static void mpdata_core(orc *o, double *unk, int iflag, int open) {
                 /* ref.f:3853-3866: the minima are taken over the maxima unkmx (as written). */
                 int ii[4] = {o->ic4[0][c], o->ic4[1][c], o->ic4[2][c], o->ic4[3][c]};
                 double pp[4] = {unk[ii[0]], unk[ii[1]], unk[ii[2]], unk[ii[3]]};
+                /* With ref_bugs off the minima are taken over unkmn, as the pair lists do. */
+                const double *lo = o->ref_bugs ? unkmx : unkmn;
                 for (int j = 0; j < 4; ++j) {
                     double mx = unkmx[ii[0]];
                     for (int q = 1; q < 4; ++q) mx = AMAX(mx, unkmx[ii[q]]);
                     for (int q = 0; q < 4; ++q) mx = AMAX(mx, pp[q]);
                     unkmx[ii[j]] = mx;
-                    double mn = unkmx[ii[0]];
-                    for (int q = 1; q < 4; ++q) mn = AMIN(mn, unkmx[ii[q]]);
+                    double mn = lo[ii[0]];
+                    for (int q = 1; q < 4; ++q) mn = AMIN(mn, lo[ii[q]]);
                     for (int q = 0; q < 4; ++q) mn = AMIN(mn, pp[q]);
                     unkmn[ii[j]] = mn;
                 }
@@ -1194,6 +1198,7 @@ orc *orc_create(const mpg_params *prm, const mpg_mesh_ref *m) {
         return NULL;
     orc *o = (orc *)calloc(1, sizeof(orc));
     o->P = *prm;
+    o->ref_bugs = 1;
     int n = m->npoin;
     o->npoin = n; o->nedge = m->nedge; o->nbface = m->nbface; o->nboun = m->nboun;
     o->ncoin = m->ncoin; o->ncoin2 = m->ncoin2; o->ncoin4 = m->ncoin4;

@@ -30,6 +30,9 @@ void   orc_destroy(orc *o);
 /* 0 (default): global sums in the reference's sequential order; 1: in the GPU kernels' fixed
  * reduction order, so that CPU and GPU runs can be compared bit for bit */
 void   orc_set_reduction(orc *o, int blocked);
+/* 1 (default): reproduce the corner-minimum slip of mpdatamper (ref.f:3853-3866, minima taken
+ * over unkmx); 0: take them over unkmn like the pair lists. */
+void   orc_set_ref_bugs(orc *o, int on);
 /* pointer to a field (same ids as the product) — n = npoin doubles */
 double *orc_field(orc *o, int fid);
 int    orc_npoin(const orc *o);

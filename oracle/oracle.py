@@ -56,6 +56,7 @@ def lib():
         L.orc_beta.argtypes = [vp]
         L.orc_line_solve.argtypes = [vp, dp, dp, ip]
         L.orc_set_reduction.argtypes = [vp, ip]
+        L.orc_set_ref_bugs.argtypes = [vp, ip]
         _lib = L
     return _lib
 
@@ -68,7 +69,7 @@ def _p(a: np.ndarray):
 class Oracle:
     """The reference restated on the CPU; fields addressed by the product's field ids."""
 
-    def __init__(self, params: RunParams, refmesh, gpu_order: bool = False):
+    def __init__(self, params: RunParams, refmesh, gpu_order: bool = False, ref_bugs: bool = True):
         self.params = params
         self.mm = MeshMarshal(refmesh)
         self._cp = params.to_c()
@@ -79,6 +80,8 @@ class Oracle:
         self.n = refmesh.npoin
         if gpu_order:
             self.L.orc_set_reduction(self.h, 1)
+        if not ref_bugs:
+            self.L.orc_set_ref_bugs(self.h, 0)
 
     def __del__(self):
         h = getattr(self, "h", None)

@@ -34,6 +34,8 @@ at the node, the edge midpoints and the triangle centroids.  With that surface:
 The periodic square is represented as a torus: edges wrap around and there are no
 duplicate nodes, so the reference's periodic duplicate lists (``icoin``, ``icoin2``,
 ``icoin4``) are empty and its ``cyclicr*`` routines are no-ops on this input.
+``generate(..., duplicates=True)`` builds the reference's duplicate-node form of a periodic
+domain instead, and ``merge_duplicates`` converts that form to the torus.
 Semi-edges are not used (``nbface = 0``); the top and bottom of every column are
 boundary points of type 11 (normal velocity removed by ``bcv``) with the outward
 dual face as ``sbb`` and its unit normal as ``anp``.
@@ -77,6 +79,10 @@ class ColumnMesh:
     bcol: Optional[np.ndarray] = None     # (nb,) int64
     btype: Optional[np.ndarray] = None    # (nb,) int32: 7 inflow x=0, 8 outflow x=Lx, 5 y=0, 6 y=Ly
     bT: Optional[np.ndarray] = None       # (nb, 2)
+    # duplicate-node periodic form only: column pairs / quadruples of copies
+    coin: Optional[np.ndarray] = None     # (n, 2) x = 0 ~ x = Lx
+    coin2: Optional[np.ndarray] = None    # (n, 2) y = 0 ~ y = Ly
+    coin4: Optional[np.ndarray] = None    # (1, 4) the corners
 
     @property
     def ncol(self) -> int:
@@ -232,8 +238,16 @@ def level_set(L: int, H: float, stretch_dz0: Optional[float] = None) -> np.ndarr
 def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
              Ly: Optional[float] = None, H: float = 20e3, h0: float = 400.0,
              half_width: float = 10e3, jitter: float = 0.3, seed: int = 0,
-             stretch_dz0: Optional[float] = None, periodic: bool = True) -> ColumnMesh:
+             stretch_dz0: Optional[float] = None, periodic: bool = True,
+             duplicates: bool = False) -> ColumnMesh:
     """Build the jittered prism-column mesh (see module docstring).
+
+    ``duplicates=True`` (periodic only) builds the reference's own periodic form instead of the
+    torus: ``(nx+1) * (ny+1)`` nodes from corner to corner, the nodes of opposite sides
+    duplicates of one another (same tangential jitter), listed in ``icoin`` (x sides),
+    ``icoin2`` (y sides) and ``icoin4`` (the four corners) for the reference's ``cyclicr``
+    routines (ref.f:4377-4446).  Each copy carries its part of the dual cell; the bottom
+    boundary normal ``anp`` of every copy is the normal of the whole cell.
 
     ``periodic=False`` builds the open channel used with ``iper = 0``: ``nx * ny`` nodes
     from corner to corner of the rectangle, side nodes jittered along their side only,
@@ -244,24 +258,38 @@ def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
     """
     ny = nx if ny is None else ny
     Ly = Lx if Ly is None else Ly
+    if duplicates and not periodic:
+        raise ValueError("duplicates=True describes a periodic domain")
+    torus = periodic and not duplicates
     rng = np.random.default_rng(seed)
-    I, J = np.meshgrid(np.arange(nx), np.arange(ny), indexing="xy")
-    if periodic:
+    if torus:
+        I, J = np.meshgrid(np.arange(nx), np.arange(ny), indexing="xy")
         hx, hy = Lx / nx, Ly / ny
         base = np.stack([(I.ravel() + 0.5) * hx, (J.ravel() + 0.5) * hy], axis=1)
+    elif duplicates:
+        nxx, nyy = nx + 1, ny + 1
+        I, J = np.meshgrid(np.arange(nxx), np.arange(nyy), indexing="xy")
+        hx, hy = Lx / nx, Ly / ny
+        base = np.stack([I.ravel() * hx, J.ravel() * hy], axis=1)
     else:
+        nxx, nyy = nx, ny
+        I, J = np.meshgrid(np.arange(nx), np.arange(ny), indexing="xy")
         hx, hy = Lx / (nx - 1), Ly / (ny - 1)
         base = np.stack([I.ravel() * hx, J.ravel() * hy], axis=1)
     jit = rng.uniform(-jitter, jitter, size=base.shape) * np.array([hx, hy])
-    if not periodic:
-        iside = (I.ravel() == 0) | (I.ravel() == nx - 1)
-        jside = (J.ravel() == 0) | (J.ravel() == ny - 1)
+    if not torus:
+        Ir, Jr = I.ravel(), J.ravel()
+        iside = (Ir == 0) | (Ir == nxx - 1)
+        jside = (Jr == 0) | (Jr == nyy - 1)
         jit[iside, 0] = 0.0
         jit[jside, 1] = 0.0
+        if duplicates:       # a copy moves along its side exactly like its partner
+            jit[Ir == nxx - 1, 1] = jit[(Ir == 0), 1]
+            jit[Jr == nyy - 1, 0] = jit[(Jr == 0), 0]
     xy = base + jit
     ncol = xy.shape[0]
 
-    if periodic:
+    if torus:
         tri, P = _periodic_delaunay(xy, Lx, Ly, margin=4.0 * max(hx, hy))
     else:
         tri, P = _open_delaunay(xy, Lx, Ly)
@@ -285,11 +313,11 @@ def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
     b = np.maximum(p_idx, q_idx)
     key = (a * ncol + b).ravel()
     ukey, inv, cnt = np.unique(key, return_inverse=True, return_counts=True)
-    if periodic and not np.all(cnt == 2):
+    if torus and not np.all(cnt == 2):
         raise RuntimeError("torus triangulation has an edge not shared by two triangles")
     edges2d = np.stack([ukey // ncol, ukey % ncol], axis=1)
     ne2 = edges2d.shape[0]
-    if periodic and ne2 != 3 * ncol:
+    if torus and ne2 != 3 * ncol:
         raise RuntimeError(f"expected {3 * ncol} edges, got {ne2}")
 
     # lateral face vectors: segment midpoint -> centroid, oriented p -> q, flipped to a -> b
@@ -353,6 +381,13 @@ def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
         bcol = (uk % ncol).astype(np.int64)
         btype = np.array([7, 8, 5, 6], dtype=np.int32)[uk // ncol]
 
+    coin = coin2 = coin4 = None
+    if duplicates:
+        cidx = np.arange(ncol).reshape(nyy, nxx)
+        coin = np.stack([cidx[1:-1, 0], cidx[1:-1, -1]], axis=1)          # x = 0 ~ x = Lx
+        coin2 = np.stack([cidx[0, 1:-1], cidx[-1, 1:-1]], axis=1)         # y = 0 ~ y = Ly
+        coin4 = np.array([[cidx[0, 0], cidx[0, -1], cidx[-1, 0], cidx[-1, -1]]])
+
     zeta = level_set(L, H, stretch_dz0)
     zh = np.empty(L + 1)
     zh[0] = 0.0
@@ -361,7 +396,7 @@ def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
     return ColumnMesh(nx=nx, ny=ny, L=L, Lx=Lx, Ly=Ly, H=H, h0=h0, half_width=half_width,
                       xy=xy, hnode=hnode, tri=tri, edges2d=edges2d.astype(np.int64), T=T,
                       A=A, W=W, zeta=zeta, zeta_half=zh, periodic=periodic,
-                      bcol=bcol, btype=btype, bT=bT)
+                      bcol=bcol, btype=btype, bT=bT, coin=coin, coin2=coin2, coin4=coin4)
 
 
 def expand_reference(cm: ColumnMesh) -> RefMesh:
@@ -423,10 +458,98 @@ def expand_reference(cm: ColumnMesh) -> RefMesh:
         anp[2 * NC:, 0] = np.repeat(nrm[:, 0], L)
         anp[2 * NC:, 1] = np.repeat(nrm[:, 1], L)
     z2 = np.zeros((0, 2), dtype=np.int32)
+    lists = [z2.copy(), z2.copy(), np.zeros((0, 4), dtype=np.int32)]
+    if cm.coin is not None:
+        # the bottom normal of every copy is that of the whole cell (sum over its copies)
+        Ab = cm.A.copy()
+        for grp in (cm.coin, cm.coin2, cm.coin4):
+            Ab[grp] = cm.A[grp].sum(axis=1, keepdims=True)
+        anp[:NC] = -Ab / np.linalg.norm(Ab, axis=1)[:, None]
+        lists = [(grp[:, None, :] * L + ks[None, :, None]).reshape(-1, grp.shape[1]).astype(np.int32)
+                 for grp in (cm.coin, cm.coin2, cm.coin4)]
     return RefMesh(npoin=npoin, nedge=nedge, nbface=0, nboun=nboun, coord=coord, vol=vol,
                    iedge=iedge, sn=sn, kbface=z2.copy(), sb=np.zeros((0, 3)), ibpoin=ibpoin,
-                   sbb=sbb, anp=anp, icoin=z2.copy(), icoin2=z2.copy(),
-                   icoin4=np.zeros((0, 4), dtype=np.int32))
+                   sbb=sbb, anp=anp, icoin=lists[0], icoin2=lists[1], icoin4=lists[2])
+
+
+def merge_duplicates(rm: RefMesh):
+    """Convert a periodic mesh in the reference's duplicate-node form to the torus form.
+
+    The reference keeps the nodes of opposite periodic sides as separate copies, each with part
+    of the dual cell, and sums their partial results with ``cyclicr``/``cyclicr2``/``cyclicr4``
+    (ref.f:4377-4446) after every edge loop; ``vol`` is summed the same way at set-up
+    (ref.f:99-103).  The library takes a periodic domain as a torus instead (wrap-around edges,
+    one node per physical point, empty lists).  This merges every group of copies into its
+    lowest-numbered node: volumes are summed in ``cyclicr`` order, faces joining the same pair
+    of merged nodes (the two halves of a seam face) are summed, and boundary points of one merged
+    node and type are combined (face vectors summed, unit normal of the sum).  Returns the torus
+    mesh and, for every node of ``rm``, its node in the torus (for moving fields between the two).
+    """
+    n = rm.npoin
+    parent = np.arange(n)
+
+    def find(i):
+        while parent[i] != i:
+            parent[i] = parent[parent[i]]
+            i = parent[i]
+        return i
+
+    for grp in (rm.icoin, rm.icoin2, rm.icoin4):
+        for row in np.asarray(grp):
+            r = [find(int(i)) for i in row]
+            lo = min(r)
+            for x in r:
+                parent[x] = lo
+    root = np.array([find(i) for i in range(n)])
+    reps = np.unique(root)
+    new = np.full(n, -1, dtype=np.int64)
+    new[reps] = np.arange(reps.shape[0])
+    node_of = new[root]
+
+    vol = rm.vol.astype(np.float64).copy()
+    for grp in (rm.icoin, rm.icoin2, rm.icoin4):        # cyclicr, cyclicr2, cyclicr4 in order
+        grp = np.asarray(grp)
+        if grp.shape[0]:
+            tot = vol[grp[:, 0]].copy()
+            for q in range(1, grp.shape[1]):
+                tot = tot + vol[grp[:, q]]
+            for q in range(grp.shape[1]):
+                vol[grp[:, q]] = tot
+
+    faces, S = {}, []
+    for (i1, i2), sv in zip(np.concatenate([rm.iedge, rm.kbface]), np.concatenate([rm.sn, rm.sb])):
+        a, b = int(node_of[i1]), int(node_of[i2])
+        if a == b:
+            raise ValueError("a face joins two copies of one node")
+        key = (min(a, b), max(a, b))
+        sgn = 1.0 if a == key[0] else -1.0
+        if key in faces:
+            S[faces[key]] = S[faces[key]] + sgn * sv
+        else:
+            faces[key] = len(S)
+            S.append(sgn * sv)
+    iedge = np.array(list(faces.keys()), dtype=np.int32).reshape(-1, 2)
+    sn = np.array(S).reshape(-1, 3)
+
+    bkey, sbb = {}, []
+    btype = []
+    for (i, t), sv in zip(rm.ibpoin, rm.sbb):
+        key = (int(node_of[i]), int(t))
+        if key in bkey:
+            sbb[bkey[key]] = sbb[bkey[key]] + sv
+        else:
+            bkey[key] = len(sbb)
+            sbb.append(sv.copy())
+            btype.append(key)
+    ibpoin = np.array(btype, dtype=np.int32).reshape(-1, 2)
+    sbb = np.array(sbb).reshape(-1, 3)
+    anp = sbb / np.linalg.norm(sbb, axis=1)[:, None]
+    z2 = np.zeros((0, 2), dtype=np.int32)
+    torus = RefMesh(npoin=reps.shape[0], nedge=iedge.shape[0], nbface=0, nboun=ibpoin.shape[0],
+                    coord=rm.coord[reps].copy(), vol=vol[reps], iedge=iedge, sn=sn,
+                    kbface=z2.copy(), sb=np.zeros((0, 3)), ibpoin=ibpoin, sbb=sbb, anp=anp,
+                    icoin=z2.copy(), icoin2=z2.copy(), icoin4=np.zeros((0, 4), dtype=np.int32))
+    return torus, node_of
 
 
 # ----------------------------------------------------------------------------------

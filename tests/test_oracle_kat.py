@@ -229,3 +229,93 @@ def test_open_channel_steps(open_orc):
         d = o.step()
         assert o.gcr_stats().status == 0
     assert d.smin[0] >= 0.0
+
+
+# ---- the reference's duplicate-node periodic form against the torus form the library takes
+@pytest.fixture(scope="module")
+def dup_pair():
+    from src_b200 import mesh
+    cm = mesh.generate(6, L=5, seed=2, duplicates=True)
+    rm = cm.to_reference()
+    t, node_of = mesh.merge_duplicates(rm)
+    P = RunParams(delt=10.0)
+    od, ot = Oracle(P, rm, ref_bugs=False), Oracle(P, t)
+    od.setup()
+    ot.setup()
+    return rm, t, node_of, od, ot
+
+
+def _seam(rm, hops):
+    m = np.zeros(rm.npoin, bool)
+    for g in (rm.icoin, rm.icoin2, rm.icoin4):
+        m[g.ravel()] = True
+    for _ in range(hops):
+        nb = m.copy()
+        e = m[rm.iedge[:, 0]] | m[rm.iedge[:, 1]]
+        nb[rm.iedge[e, 0]] = True
+        nb[rm.iedge[e, 1]] = True
+        m = nb
+    return m
+
+
+def test_duplicate_form_merges_to_a_torus(dup_pair):
+    """Merging the copies of the reference's periodic form (icoin/icoin2/icoin4) gives a closed
+    torus mesh with 3 edges per column that the library's host side accepts."""
+    from src_b200 import api, mesh
+    rm, t, node_of, _, _ = dup_pair
+    assert rm.icoin.shape[0] and rm.icoin2.shape[0] and rm.icoin4.shape[0]
+    assert np.abs(mesh.closure_residual(t)).max() <= 1e-14 * np.abs(t.sn).max()
+    info = api.analyze_mesh(t)
+    assert info["ncol"] * info["nlev"] == t.npoin and info["nedge2d"] == 3 * info["ncol"]
+    assert np.array_equal(np.unique(node_of), np.arange(t.npoin))
+
+
+def test_linear_operators_agree_on_both_forms(dup_pair):
+    """derivative with cyclicr (ref.f:4015-4019), laplc, prfr and div on the duplicate form equal
+    the torus form's to rounding on every copy: the forms differ only in how sums are grouped."""
+    rm, t, no, od, ot = dup_pair
+    rng = np.random.default_rng(0)
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
+    phi = rng.standard_normal(t.npoin)
+    for idx in (1, 2, 3):
+        assert rel(od.derivative(phi[no], idx), ot.derivative(phi, idx)[no]) <= 1e-14
+    for impfl in (0, 1):
+        assert rel(od.laplc(phi[no], impfl), ot.laplc(phi, impfl)[no]) <= 1e-14
+    u = [rng.standard_normal(t.npoin) for _ in range(4)]
+    a, b = od.prfr(*[x[no] for x in u], 1), ot.prfr(*u, 1)
+    for k in range(3):
+        assert rel(a[k], b[k][no]) <= 1e-14
+    assert rel(od.div(*[x[no] for x in u[:3]], -1)[0], ot.div(*u[:3], -1)[0][no]) <= 1e-14
+
+
+def test_mpdata_differs_only_at_the_seam(dup_pair):
+    """MPDATA upwinds and limits each half of a seam face separately in the duplicate form
+    (|a| + |b| != |a + b| when the halves' fluxes differ in sign), so its result differs from the
+    torus form's at the copies; two edges away from them only through the limiter's coupling."""
+    rm, t, no, od, ot = dup_pair
+    for k in range(3):
+        od.set(F_UUU + k, ot.get(F_UUU + k)[no])
+    psi = np.random.default_rng(1).uniform(0.5, 1.5, t.npoin)
+    d = np.abs(od.mpdatamper(psi[no], 5) - ot.mpdatamper(psi, 5)[no])
+    assert d[_seam(rm, 0)].max() > 1e-6
+    assert d[~_seam(rm, 1)].max() <= 1e-8
+
+
+def test_corner_minimum_slip_is_local():
+    """ref.f:3853-3866 takes the corner copies' minima over unkmx; switching that off changes
+    MPDATA only at the corner copies and their neighbours."""
+    from src_b200 import mesh
+    rm = mesh.generate(6, L=5, seed=2, duplicates=True).to_reference()
+    on, off = Oracle(RunParams(delt=10.0), rm), Oracle(RunParams(delt=10.0), rm, ref_bugs=False)
+    on.setup()
+    off.setup()
+    for k in range(3):
+        off.set(F_UUU + k, on.get(F_UUU + k))
+    psi = np.random.default_rng(1).uniform(0.5, 1.5, rm.npoin)
+    d = np.abs(on.mpdatamper(psi, 5) - off.mpdatamper(psi, 5))
+    corner = np.zeros(rm.npoin, bool)
+    corner[rm.icoin4.ravel()] = True
+    near = corner.copy()
+    e = corner[rm.iedge[:, 0]] | corner[rm.iedge[:, 1]]
+    near[rm.iedge[e].ravel()] = True
+    assert d[corner].max() > 0 and np.all(d[~near] == 0)
