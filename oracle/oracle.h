@@ -10,7 +10,9 @@
  * golden vectors, and no Fortran compiler exists on either machine, so the restatement cannot
  * be diffed against the Fortran.  It is pinned instead by known-answer properties (dual-cell
  * closure, exact conservation, symmetry of laplc, manufactured GCR solutions, MPDATA
- * constancy/positivity/bounds) checked in tests/.
+ * constancy/positivity/bounds) checked in tests/.  tests/golden/ holds reference-format input
+ * decks with this restatement's results on them, ready to diff against the Fortran wherever a
+ * compiler for it exists.
  *
  * Arrays are 0-based; the mesh is taken from the same mpg_mesh_ref struct the product takes.
  */
