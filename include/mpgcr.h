@@ -71,7 +71,11 @@ typedef struct mpg_params {
     int32_t implgw, lipps;
     double  strat, tetbar, g;
     /* extensions of this implementation */
-    int32_t iprc;                /* 0 identity, 1 reference smoother (ref.f:587-612), 2 vertical line */
+    int32_t iprc;                /* 0 identity, 1 reference smoother (ref.f:587-612), 2 vertical line,
+                                  * 3 learned correction of the line, 4 laplc's own column blocks:
+                                  * laplc couples level k with k and k+-2 in a column, so its column
+                                  * block is tridiagonal on the even and on the odd levels; iprc = 4
+                                  * solves that block exactly (itrp1 relaxations like iprc = 2)     */
     int32_t nscal;               /* passive scalars advected after unk(:,1..4)                      */
     int32_t precision;           /* MPG_PREC_FP64 or MPG_PREC_MIXED                                 */
     int32_t itmn;                /* minimum restart cycles before the convergence test (3, ref.f:1809) */
@@ -178,6 +182,11 @@ int mpg_destroy(mpg_handle h);
  * GPU and fills npoin, nedge, ncol, nedge2d and nlev of `info` (device_bytes = 0; precision =
  * 1 when per-node sums can follow the reference's edge order exactly, else 0). */
 int mpg_analyze_mesh(const mpg_mesh_ref *mesh, mpg_info *info);
+/* Host-only: the factorised column blocks of laplc that the iprc = 4 preconditioner solves
+ * (no counterpart in the reference; see params.iprc), per reference node: sub-diagonal a =
+ * A[k][k-2], inverse pivot 1/m and c' of the Thomas factorisation on the node's parity chain. */
+int mpg_analyze_wide(const mpg_params *prm, const mpg_mesh_ref *mesh, int impfl, double *a,
+                     double *minv, double *cp);
 const char *mpg_last_error(void);
 int mpg_get_info(mpg_handle h, mpg_info *info);
 

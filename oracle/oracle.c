@@ -48,6 +48,7 @@ struct orc {
     int *colnodes;
     int nvert_e;
     int *vedge;         /* vertical edges: index into the combined edge list */
+    int *bst, *blst;    /* boundary points per node (CSR), built on demand */
     int blocked;        /* 1: global sums in the GPU's reduction order (see rsum) */
     int ref_bugs;       /* 1 (default): reproduce the corner-minimum slip of ref.f:3853-3866 */
 };
@@ -399,6 +400,157 @@ static void line_coeffs(orc *o, int impfl, double *a, double *m, double *cp) {
     free(Ta); free(Tc); free(hx); free(hy); free(hz); free(b); free(c);
 }
 
+/* ------------------------------------------------------------------ NEW: the vertical part of laplc
+ * (iprc = 4).  laplc's gradient uses face averages (p_n + p_j)/2, so in a column it couples
+ * level k with k and k+-2 only: the column block of laplc is tridiagonal on the even and on the
+ * odd levels separately.  Its entries, with S the upward face between levels k and k+1,
+ * s_m = (0.5 dt/vol_m) (1/(gc_m^2), 1/gmm_m^2, cw_m), P_m the bcv(.,0) projection at node m:
+ *   A[k][k+2] = ((S_k/2) . rh0_{k+1} P_{k+1}(s_{k+1} (*) S_{k+1}/2)) / (vol_k rh0_k)
+ *   A[k][k-2] = ((S_{k-1}/2) . rh0_{k-1} P_{k-1}(s_{k-1} (*) S_{k-2}/2)) / (vol_k rh0_k)
+ *   A[k][k]   = (sum over faces f of k, neighbour j: -(S_f/2) . rh0_j P_j(s_j (*) S_f/2)
+ *                + e_k . rh0_k P_k(s_k (*) e_k)) / (vol_k rh0_k)
+ * with e_k = (sum of k's outward faces)/2 (+ its boundary faces sbb when iper = 0): the part of
+ * a non-closed cell's gradient that multiplies p_k itself. */
+static void bcv_vec(orc *o, int i, double v[3]) {
+    int per = (o->P.isfera == 1 || o->P.iper == 2);
+    for (int b = o->bst[i]; b < o->bst[i + 1]; ++b) {
+        int q = o->blst[b], t = o->ibt[q];
+        double a1 = o->anx[q], a2 = o->any[q], a3 = o->anz[q];
+        if (t == 11 || (!per && (t == 5 || t == 6))) {
+            double vn = v[0] * a1 + v[1] * a2 + v[2] * a3;
+            v[0] = v[0] - a1 * vn;
+            v[1] = v[1] - a2 * vn;
+            v[2] = v[2] - a3 * vn;
+        }
+        if (!per && (t == 7 || t == 8)) v[0] = 0.;
+    }
+}
+
+static void node_scale(orc *o, int i, int impfl, double sc[3]) {
+    double gc = o->gmm[i] * o->cosa[i], h = 0.5 * (o->timestp[i] / o->vol[i]);
+    sc[0] = h / (gc * gc);
+    sc[1] = h / (o->gmm[i] * o->gmm[i]);
+    sc[2] = h * (o->f[MPG_F_COEFW][i] * (double)impfl + (double)(1 - impfl));
+}
+
+/* (a/2) . rh0_m P_m(s_m (*) b/2) */
+static double path(orc *o, int m, int impfl, const double a[3], const double b[3]) {
+    double sc[3], v[3];
+    node_scale(o, m, impfl, sc);
+    for (int d = 0; d < 3; ++d) v[d] = sc[d] * (0.5 * b[d]);
+    bcv_vec(o, m, v);
+    double r = o->f[MPG_F_RH0][m];
+    return (0.5 * a[0]) * (r * v[0]) + (0.5 * a[1]) * (r * v[1]) + (0.5 * a[2]) * (r * v[2]);
+}
+
+static void boundary_lists(orc *o) {
+    if (o->bst) return;
+    int n = o->npoin;
+    o->bst = iz(n + 1);
+    o->blst = iz(o->nboun);
+    for (int b = 0; b < o->nboun; ++b) o->bst[o->ibn[b] + 1]++;
+    for (int i = 0; i < n; ++i) o->bst[i + 1] += o->bst[i];
+    int *fill = iz(n);
+    for (int b = 0; b < o->nboun; ++b) { int i = o->ibn[b]; o->blst[o->bst[i] + fill[i]++] = b; }
+    free(fill);
+}
+
+/* raw entries of the column blocks of laplc: lo = A[k][k-2], dg = A[k][k], hi = A[k][k+2] */
+void orc_wide_entries(orc *o, int impfl, double *lo, double *dg, double *hi) {
+    int n = o->npoin;
+    line_structure(o);
+    boundary_lists(o);
+    double *ex = dz(n), *ey = dz(n), *ez = dz(n);
+    for (int i = 0; i < n; ++i) { lo[i] = 0.; dg[i] = 0.; hi[i] = 0.; }
+    for (int e = 0; e < o->nedge + o->nbface; ++e) {
+        int in = e < o->nedge;
+        int i1 = in ? o->ie1[e] : o->kb1[e - o->nedge], i2 = in ? o->ie2[e] : o->kb2[e - o->nedge];
+        double S[3] = {in ? o->snx[e] : o->sbx[e - o->nedge], in ? o->sny[e] : o->sby[e - o->nedge],
+                       in ? o->snz[e] : o->sbz[e - o->nedge]};
+        ex[i1] += S[0]; ey[i1] += S[1]; ez[i1] += S[2];
+        ex[i2] -= S[0]; ey[i2] -= S[1]; ez[i2] -= S[2];
+        dg[i1] = dg[i1] - path(o, i2, impfl, S, S);
+        dg[i2] = dg[i2] - path(o, i1, impfl, S, S);
+    }
+    for (int i = 0; i < n; ++i) {
+        double e3[3] = {0.5 * ex[i], 0.5 * ey[i], 0.5 * ez[i]};
+        if (o->P.isfera == 0 && o->P.iper == 0)
+            for (int b = o->bst[i]; b < o->bst[i + 1]; ++b) {
+                int q = o->blst[b];
+                e3[0] += o->sbbx[q]; e3[1] += o->sbby[q]; e3[2] += o->sbbz[q];
+            }
+        double a2[3] = {2. * e3[0], 2. * e3[1], 2. * e3[2]};   /* path() halves both vectors */
+        dg[i] = dg[i] + path(o, i, impfl, a2, a2);
+    }
+    /* upward face vectors along each column */
+    double *sux = dz(n), *suy = dz(n), *suz = dz(n);
+    for (int e = 0; e < o->nedge + o->nbface; ++e) {
+        int in = e < o->nedge;
+        int i1 = in ? o->ie1[e] : o->kb1[e - o->nedge], i2 = in ? o->ie2[e] : o->kb2[e - o->nedge];
+        if (!is_vertical(o, i1, i2)) continue;
+        double sg = o->up[i1] == i2 ? 1. : -1.;
+        int lower = sg > 0 ? i1 : i2;
+        sux[lower] = sg * (in ? o->snx[e] : o->sbx[e - o->nedge]);
+        suy[lower] = sg * (in ? o->sny[e] : o->sby[e - o->nedge]);
+        suz[lower] = sg * (in ? o->snz[e] : o->sbz[e - o->nedge]);
+    }
+    for (int i = 0; i < n; ++i) {
+        double vr = o->vol[i] * o->f[MPG_F_RH0][i];
+        int u1 = o->up[i], d1 = o->dn[i];
+        if (u1 >= 0 && o->up[u1] >= 0) {
+            double a[3] = {sux[i], suy[i], suz[i]}, b[3] = {sux[u1], suy[u1], suz[u1]};
+            hi[i] = path(o, u1, impfl, a, b) / vr;
+        }
+        if (d1 >= 0 && o->dn[d1] >= 0) {
+            int d2 = o->dn[d1];
+            double a[3] = {sux[d1], suy[d1], suz[d1]}, b[3] = {sux[d2], suy[d2], suz[d2]};
+            lo[i] = path(o, d1, impfl, a, b) / vr;
+        }
+        dg[i] = dg[i] / vr;
+    }
+    free(ex); free(ey); free(ez); free(sux); free(suy); free(suz);
+}
+
+/* Thomas factorisation on the even and on the odd levels of each column (bottom to top):
+ * a = A[k][k-2], m = inverse pivot, cp = c' */
+void orc_wide_factors(orc *o, int impfl, double *lo, double *m, double *cp) {
+    int n = o->npoin;
+    double *dg = dz(n), *hi = dz(n);
+    orc_wide_entries(o, impfl, lo, dg, hi);
+    for (int col = 0; col < o->ncol; ++col) {
+        int s = o->colstart[col], t = o->colstart[col + 1];
+        for (int par = 0; par < 2; ++par)
+            for (int k = s + par; k < t; k += 2) {
+                int i = o->colnodes[k];
+                double mm = k < s + 2 ? dg[i] : dg[i] - lo[i] * cp[o->colnodes[k - 2]];
+                cp[i] = hi[i] / mm;
+                m[i] = 1. / mm;
+            }
+    }
+    free(dg); free(hi);
+}
+
+void orc_wide_solve(orc *o, const double *rhs, double *zout, int impfl) {
+    int n = o->npoin;
+    double *lo = dz(n), *m = dz(n), *cp = dz(n), *d = dz(n);
+    orc_wide_factors(o, impfl, lo, m, cp);
+    for (int col = 0; col < o->ncol; ++col) {
+        int s = o->colstart[col], t = o->colstart[col + 1];
+        for (int par = 0; par < 2; ++par) {
+            for (int k = s + par; k < t; k += 2) {
+                int i = o->colnodes[k];
+                d[i] = k < s + 2 ? rhs[i] * m[i] : (rhs[i] - lo[i] * d[o->colnodes[k - 2]]) * m[i];
+            }
+            int top = s + par + ((t - 1 - s - par) / 2) * 2;
+            for (int k = top; k >= s + par; k -= 2) {
+                int i = o->colnodes[k];
+                zout[i] = k == top ? d[i] : d[i] - cp[i] * zout[o->colnodes[k + 2]];
+            }
+        }
+    }
+    free(lo); free(m); free(cp); free(d);
+}
+
 void orc_line_solve(orc *o, const double *rhs, double *zout, int impfl) {
     int n = o->npoin;
     double *a = dz(n), *m = dz(n), *cp = dz(n), *d = dz(n);
@@ -427,15 +579,16 @@ void orc_precon(orc *o, const double *rhs, double *p, double *r, int iprc, int i
         return;
     }
     for (int ip = 0; ip < n; ++ip) { p[ip] = 0.; r[ip] = 0.; }
-    if (iprc == 2) {                                           /* NEW: line relaxation */
+    if (iprc == 2 || iprc == 4) {                              /* NEW: line relaxation */
         double *zz = dz(n), *res = dz(n);
+        void (*solve)(orc *, const double *, double *, int) = iprc == 2 ? orc_line_solve : orc_wide_solve;
         for (int it = 1; it <= o->P.itrp1; ++it) {
             if (it == 1) {
-                orc_line_solve(o, rhs, zz, impfl);
+                solve(o, rhs, zz, impfl);
             } else {
                 orc_laplc(o, p, r, impfl);
                 for (int ip = 0; ip < n; ++ip) res[ip] = rhs[ip] - r[ip];
-                orc_line_solve(o, res, zz, impfl);
+                solve(o, res, zz, impfl);
             }
             for (int ip = 0; ip < n; ++ip) p[ip] = p[ip] + o->P.omega * zz[ip];
         }
@@ -1267,7 +1420,8 @@ void orc_destroy(orc *o) {
     void *ptrs[] = {o->x, o->y, o->z, o->vol, o->ie1, o->ie2, o->snx, o->sny, o->snz, o->kb1, o->kb2,
                     o->sbx, o->sby, o->sbz, o->ibn, o->ibt, o->sbbx, o->sbby, o->sbbz, o->anx, o->any,
                     o->anz, o->ic1, o->ic2, o->ic2a, o->ic2b, o->ic4[0], o->ic4[1], o->ic4[2], o->ic4[3],
-                    o->timestp, o->cosa, o->gmm, o->ue, o->ve, o->up, o->dn, o->colstart, o->colnodes};
+                    o->timestp, o->cosa, o->gmm, o->ue, o->ve, o->up, o->dn, o->colstart, o->colnodes,
+                    o->bst, o->blst};
     for (size_t i = 0; i < sizeof ptrs / sizeof ptrs[0]; ++i) free(ptrs[i]);
     for (int k = 0; k < MPG_F_COUNT; ++k) free(o->f[k]);
     free(o);

@@ -35,6 +35,11 @@ void   orc_set_reduction(orc *o, int blocked);
 /* 1 (default): reproduce the corner-minimum slip of mpdatamper (ref.f:3853-3866, minima taken
  * over unkmx); 0: take them over unkmn like the pair lists. */
 void   orc_set_ref_bugs(orc *o, int on);
+/* NEW (iprc = 4): the column blocks of laplc, lo = A[k][k-2], dg = A[k][k], hi = A[k][k+2] per
+ * node, and the preconditioner that solves them (Thomas on even and odd levels). */
+void   orc_wide_entries(orc *o, int impfl, double *lo, double *dg, double *hi);
+void   orc_wide_factors(orc *o, int impfl, double *lo, double *m, double *cp);
+void   orc_wide_solve(orc *o, const double *rhs, double *zout, int impfl);
 /* pointer to a field (same ids as the product) — n = npoin doubles */
 double *orc_field(orc *o, int fid);
 int    orc_npoin(const orc *o);

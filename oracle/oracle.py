@@ -57,6 +57,9 @@ def lib():
         L.orc_line_solve.argtypes = [vp, dp, dp, ip]
         L.orc_set_reduction.argtypes = [vp, ip]
         L.orc_set_ref_bugs.argtypes = [vp, ip]
+        L.orc_wide_entries.argtypes = [vp, ip, dp, dp, dp]
+        L.orc_wide_solve.argtypes = [vp, dp, dp, ip]
+        L.orc_wide_factors.argtypes = [vp, ip, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -140,6 +143,21 @@ class Oracle:
     def line_solve(self, rhs, impfl):
         z = np.zeros(self.n)
         self.L.orc_line_solve(self.h, _p(np.ascontiguousarray(rhs, np.float64)), _p(z), impfl)
+        return z
+
+    def wide_entries(self, impfl):
+        lo, dg, hi = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        self.L.orc_wide_entries(self.h, impfl, _p(lo), _p(dg), _p(hi))
+        return lo, dg, hi
+
+    def wide_factors(self, impfl):
+        a, m, cp = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        self.L.orc_wide_factors(self.h, impfl, _p(a), _p(m), _p(cp))
+        return a, m, cp
+
+    def wide_solve(self, rhs, impfl):
+        z = np.zeros(self.n)
+        self.L.orc_wide_solve(self.h, _p(np.ascontiguousarray(rhs, np.float64)), _p(z), impfl)
         return z
 
     def gcrk(self, p, u1, v1, w1, impfl):

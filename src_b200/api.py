@@ -28,7 +28,7 @@ EXPORTS = [
     "mpg_derivative", "mpg_bcv", "mpg_laplc", "mpg_prfr", "mpg_div", "mpg_precon", "mpg_gcrk",
     "mpg_mpdatamper", "mpg_mpdatam", "mpg_courant", "mpg_stats", "mpg_setup", "mpg_step", "mpg_half_forcing",
     "mpg_explicit_forcing", "mpg_post_solve", "mpg_extrapolate", "mpg_get_gcr_stats",
-    "mpg_synchronize", "mpg_analyze_mesh", "mpg_get_stream", "mpg_kernel_timing", "mpg_kernel_times",
+    "mpg_synchronize", "mpg_analyze_mesh", "mpg_analyze_wide", "mpg_get_stream", "mpg_kernel_timing", "mpg_kernel_times",
     "mpg_laplc_noalloc", "mpg_learned_init", "mpg_learned_set_params", "mpg_learned_get_params",
     "mpg_learned_forward", "mpg_learned_grad", "mpg_learned_train_pair", "mpg_learned_harvest",
     "mpg_learned_train_records", "mpg_learned_loss", "mpg_laplc_adjoint", "mpg_restart_write",
@@ -77,6 +77,7 @@ def lib():
             getattr(L, nm).argtypes = [vp, ip]
         L.mpg_get_gcr_stats.argtypes = [vp, vp]
         L.mpg_analyze_mesh.argtypes = [vp, vp]
+        L.mpg_analyze_wide.argtypes = [vp, vp, ip, vp, vp, vp]
         L.mpg_get_stream.argtypes = [vp, C.POINTER(vp)]
         L.mpg_kernel_timing.argtypes = [vp, ip]
         L.mpg_kernel_times.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
@@ -119,6 +120,19 @@ def analyze_mesh(refmesh) -> dict:
     d["bitwise_order"] = bool(d.pop("precision"))
     d.pop("device_bytes")
     return d
+
+
+def analyze_wide(params: RunParams, refmesh, impfl: int):
+    """Host-side factorisation of laplc's column blocks used by iprc = 4, per reference node:
+    (a = A[k][k-2], inverse pivot, c') on the node's parity chain (no GPU needed)."""
+    mm = MeshMarshal(refmesh)
+    cp = params.to_c()
+    n = refmesh.npoin
+    a, m, c = np.zeros(n), np.zeros(n), np.zeros(n)
+    dp = C.POINTER(C.c_double)
+    _check(lib().mpg_analyze_wide(C.byref(cp), C.byref(mm.c), impfl, a.ctypes.data_as(dp),
+                                  m.ctypes.data_as(dp), c.ctypes.data_as(dp)))
+    return a, m, c
 
 
 class Solver:

@@ -69,6 +69,7 @@ struct mpg_solver {
     unsigned int *counter = nullptr;
     // line preconditioner
     double *la[2] = {}, *lm[2] = {}, *lcp[2] = {};   // a, 1/m, c' (interleaved)
+    double *wa[2] = {}, *wm[2] = {}, *wcp[2] = {};   // iprc = 4: laplc's column blocks, factorised
     double *dbuf = nullptr;                          // forward-sweep values (interleaved)
     double *vp[4] = {};                              // velprd: its potential and velocity
     // MPDATA scratch
@@ -299,6 +300,20 @@ int op_line(mpg_handle h, const double *rhs, TO *p, int impfl, int acc) {
     return check_launch("line_solve");
 }
 
+// iprc = 4: solve laplc's column blocks (tridiagonal on even and odd levels)
+template <class TO>
+int op_wide(mpg_handle h, const double *rhs, TO *p, int impfl, int acc) {
+    const int q = impfl ? 1 : 0;
+    if (!h->wa[q]) return mpg_fail(MPG_ERR_ARG, "iprc=4 needs a handle created with params.iprc = 4");
+    const int nblk = (h->NC + 32 * kLineWarps - 1) / (32 * kLineWarps);
+    {
+        KTIME(KT_LINE);
+        k_wide_solve<TO><<<nblk, 32 * kLineWarps, 0, h->st>>>(h->NC, h->L, rhs, h->wa[q], h->wm[q], h->wcp[q],
+                                                              h->P.omega, acc, h->dbuf, p);
+    }
+    return check_launch("wide line solve");
+}
+
 // precon(rhs, p, r, iprc, elas, impfl), mg_flag = 0 (ref.f:482-753); `zero_r` restores the
 // reference's clearing of r when a caller may look at it.
 int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, int impfl, bool zero_r) {
@@ -336,7 +351,29 @@ int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, i
         }
         return check_launch("precon line");
     }
-    if (iprc != 1) return mpg_fail(MPG_ERR_UNSUPPORTED, "iprc must be 0, 1 or 2");
+    if (iprc == 4) {                      // the same relaxation with laplc's column blocks
+        for (int it = 1; it <= h->P.itrp1; ++it) {
+            if (it == 1) {
+                int rc = op_wide<double>(h, rhs, p, impfl, 0);
+                if (rc) return rc;
+            } else {
+                int rc = op_laplc(h, p, r, impfl);
+                if (rc) return rc;
+                {
+                    KTIME(KT_MISC);
+                    k_sub<<<grid(N), kThreads, 0, h->st>>>(N, rhs, r, h->tres);
+                }
+                rc = op_wide<double>(h, h->tres, p, impfl, 1);
+                if (rc) return rc;
+            }
+        }
+        if (h->P.itrp1 < 1) {
+            KTIME(KT_MISC);
+            k_fill<<<grid(N), kThreads, 0, h->st>>>(N, p, 0.0);
+        }
+        return check_launch("precon wide line");
+    }
+    if (iprc != 1) return mpg_fail(MPG_ERR_UNSUPPORTED, "iprc must be 0, 1, 2 or 4");
     // reference smoother: the first sweep starts from p = 0, where laplc(0) = 0 exactly
     {
         KTIME(KT_MISC);
@@ -383,6 +420,23 @@ int op_precon_gcr(mpg_handle h, const double *r, int impfl) {
             }
         }
         return check_launch("precon line (mixed)");
+    }
+    if (h->P.iprc == 4) {
+        for (int it = 1; it <= h->P.itrp1; ++it) {
+            int rc;
+            if (it == 1) {
+                if ((rc = op_wide<T>(h, r, qr, impfl, 0))) return rc;
+            } else {
+                T *tmp = Buf<T>::ar(h);
+                if ((rc = op_laplc_t<T>(h, qr, tmp, impfl))) return rc;
+                {
+                    KTIME(KT_MISC);
+                    k_sub_mixed<T><<<grid(N), kThreads, 0, h->st>>>(N, r, tmp, h->tres);
+                }
+                if ((rc = op_wide<T>(h, h->tres, qr, impfl, 1))) return rc;
+            }
+        }
+        return check_launch("precon wide line (mixed)");
     }
     // iprc 0 or 1: the FP64 operator, then rounded to T
     int rc = op_precon(h, r, h->tres, h->ar, h->P.iprc, impfl, false);
@@ -1305,7 +1359,7 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     if (prm->lord < 1 || prm->lord > MPG_MAX_LORD) return mpg_fail(MPG_ERR_ARG, "lord out of range 1..16");
     if (prm->nscal < 0 || 4 + prm->nscal > MPG_MAX_UNK) return mpg_fail(MPG_ERR_ARG, "nscal out of range 0..12");
     if (prm->delt <= 0) return mpg_fail(MPG_ERR_ARG, "delt must be positive");
-    if (prm->iprc < 0 || prm->iprc > 3) return mpg_fail(MPG_ERR_ARG, "iprc must be 0, 1, 2 or 3");
+    if (prm->iprc < 0 || prm->iprc > 4) return mpg_fail(MPG_ERR_ARG, "iprc must be 0, 1, 2, 3 or 4");
     if (prm->precision != MPG_PREC_FP64 && prm->precision != MPG_PREC_MIXED)
         return mpg_fail(MPG_ERR_ARG, "precision must be MPG_PREC_FP64 or MPG_PREC_MIXED");
     HostColumnMesh hm;
@@ -1359,6 +1413,11 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
         if ((rc = upload(h, &h->la[q], h->hs.la[q])) || (rc = upload(h, &h->lm[q], h->hs.lm[q])) ||
             (rc = upload(h, &h->lcp[q], h->hs.lcp[q])))
             return fail(rc);
+    if (prm->iprc == 4)
+        for (int q = 0; q < 2; ++q)
+            if ((rc = upload(h, &h->wa[q], h->hs.wa[q])) || (rc = upload(h, &h->wm[q], h->hs.wm[q])) ||
+                (rc = upload(h, &h->wcp[q], h->hs.wcp[q])))
+                return fail(rc);
     // workspace
     const size_t N = h->N;
     if ((rc = dalloc(h, &h->stage, N)) || (rc = dalloc(h, &h->r, N)) || (rc = dalloc(h, &h->qr, N)) ||
@@ -1760,6 +1819,27 @@ extern "C" int mpg_analyze_mesh(const mpg_mesh_ref *mesh, mpg_info *info) {
     info->nlev = hm.L;
     info->precision = hm.bitwise_order ? 1 : 0;
     info->device_bytes = 0;
+    return MPG_OK;
+}
+
+extern "C" int mpg_analyze_wide(const mpg_params *prm, const mpg_mesh_ref *mesh, int impfl, double *a,
+                                double *minv, double *cp) {
+    if (!prm || !mesh || !a || !minv || !cp) return mpg_fail(MPG_ERR_ARG, "null argument");
+    HostColumnMesh hm;
+    int rc = mpg_build_column_mesh(mesh, &hm);
+    if (rc) return rc;
+    mpg_params P = *prm;
+    P.iprc = 4;
+    HostStatic hs;
+    if ((rc = mpg_host_static(&P, mesh, hm, &hs))) return rc;
+    const int q = impfl ? 1 : 0;
+    for (int n = 0; n < hm.N; ++n) {
+        const int64_t li = line_index(n / hm.L, n % hm.L, hm.L);
+        const int i = hm.iperm[n];
+        a[i] = hs.wa[q][li];
+        minv[i] = hs.wm[q][li];
+        cp[i] = hs.wcp[q][li];
+    }
     return MPG_OK;
 }
 

@@ -558,6 +558,89 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
     }
 }
 
+// The column blocks of laplc (iprc = 4) are tridiagonal on the even and on the odd levels: the
+// same sweeps as k_line_solve with the recurrences reaching two levels back / ahead, both parity
+// chains advanced together level by level.  Staging, prefetch and indexing are k_line_solve's.
+template <class TO>
+__global__ void __launch_bounds__(32 * kLineWarps)
+k_wide_solve(int NC, int L, const double *__restrict__ rhs, const double *__restrict__ la,
+             const double *__restrict__ linv, const double *__restrict__ lcp, double omega, int acc,
+             double *__restrict__ dbuf, TO *__restrict__ p) {
+    __shared__ double tile[kLineWarps][32][kLineChunk + 1];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col0 = (blockIdx.x * kLineWarps + w) * 32;
+    if (col0 >= NC) return;
+    const int ncols = min(32, NC - col0);
+    double(*t)[kLineChunk + 1] = tile[w];
+    const int c = col0 + lane;
+    const bool own = lane < ncols;
+    // forward sweep: d_k = (r_k - a_k d_{k-2}) / m_k
+    double d1 = 0., d2 = 0.;                 // d_{k-1}, d_{k-2}
+    for (int k0 = 0; k0 < L; k0 += kLineChunk) {
+        const int nk = min(kLineChunk, L - k0);
+        for (int i = lane; i < ncols * nk; i += 32) {
+            const int cc = i / nk, kk = i - cc * nk;
+            t[cc][kk] = rhs[(int64_t)(col0 + cc) * L + k0 + kk];
+        }
+        __syncwarp();
+        if (own) {
+            for (int kb = 0; kb < nk; kb += kLinePre) {
+                double A[kLinePre], Mi[kLinePre];
+#pragma unroll
+                for (int i = 0; i < kLinePre; ++i) {
+                    const int64_t li = line_index(c, k0 + kb + i, L);
+                    A[i] = kb + i < nk ? la[li] : 0.;
+                    Mi[i] = kb + i < nk ? linv[li] : 0.;
+                }
+#pragma unroll
+                for (int i = 0; i < kLinePre; ++i) {
+                    if (kb + i >= nk) break;
+                    const int k = k0 + kb + i;
+                    const double d = (k < 2) ? t[lane][kb + i] * Mi[i] : (t[lane][kb + i] - A[i] * d2) * Mi[i];
+                    dbuf[line_index(c, k, L)] = d;
+                    d2 = d1;
+                    d1 = d;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    // backward sweep: z_k = d_k - c'_k z_{k+2}, top chunk first
+    double z1 = 0., z2 = 0.;                 // z_{k+1}, z_{k+2}
+    const int last0 = ((L - 1) / kLineChunk) * kLineChunk;
+    for (int k0 = last0; k0 >= 0; k0 -= kLineChunk) {
+        const int nk = min(kLineChunk, L - k0);
+        if (own) {
+            for (int kb = nk - 1; kb >= 0; kb -= kLinePre) {
+                double D[kLinePre], Cp[kLinePre];
+#pragma unroll
+                for (int i = 0; i < kLinePre; ++i) {
+                    const int64_t li = line_index(c, k0 + kb - i, L);
+                    D[i] = kb - i >= 0 ? dbuf[li] : 0.;
+                    Cp[i] = kb - i >= 0 ? lcp[li] : 0.;
+                }
+#pragma unroll
+                for (int i = 0; i < kLinePre; ++i) {
+                    if (kb - i < 0) break;
+                    const int k = k0 + kb - i;
+                    const double z = (k >= L - 2) ? D[i] : D[i] - Cp[i] * z2;
+                    t[lane][kb - i] = z;
+                    z2 = z1;
+                    z1 = z;
+                }
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < ncols * nk; i += 32) {
+            const int cc = i / nk, kk = i - cc * nk;
+            const int64_t g = (int64_t)(col0 + cc) * L + k0 + kk;
+            const double prev = acc ? (double)p[g] : 0.0;
+            p[g] = (TO)(prev + omega * t[cc][kk]);
+        }
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------------------------ reductions
 enum RedKind { RSUM = 0, RMAX = 1 };
 

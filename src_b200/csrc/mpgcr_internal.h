@@ -88,10 +88,23 @@ struct HostStatic {
     // sub-diagonal a, inverse pivot 1/m and c' of the Thomas factorisation
     std::vector<double> la[2], lm[2], lcp[2];
     std::vector<float> lbabs;       // |diagonal| of the line matrix for impfl = 1 (node order)
+    // iprc = 4: the column blocks of laplc (tridiagonal on even and odd levels), factorised per
+    // parity chain, same interleaved layout; empty unless iprc = 4
+    std::vector<double> wa[2], wm[2], wcp[2];
 };
 
 int mpg_host_static(const mpg_params *P, const mpg_mesh_ref *m, const HostColumnMesh &cm,
                     HostStatic *out);
+
+// iprc = 4: entries A[k][k-2], A[k][k], A[k][k+2] of laplc's column blocks (reference node order,
+// cw = coefw*impfl + (1-impfl) per reference node) and their factorisation into hs->wa/wm/wcp
+void mpg_wide_entries(const mpg_params *P, const mpg_mesh_ref *m, const HostColumnMesh &cm,
+                      const std::vector<double> &rh0r, const std::vector<double> &volr,
+                      const std::vector<double> &cw, std::vector<double> &lo, std::vector<double> &dg,
+                      std::vector<double> &hi);
+void mpg_wide_coeffs(const mpg_params *P, const mpg_mesh_ref *m, const HostColumnMesh &cm,
+                     const std::vector<double> &rh0r, const std::vector<double> &volr,
+                     const std::vector<double> *cwr, HostStatic *hs);
 
 // interleaved coefficient layout for the column solve: column c, level k ->
 // ((c / 32) * L + k) * 32 + (c % 32)

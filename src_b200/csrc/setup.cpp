@@ -481,5 +481,149 @@ int mpg_host_static(const mpg_params *P, const mpg_mesh_ref *m, const HostColumn
             }
         }
     }
+    if (P->iprc == 4) mpg_wide_coeffs(P, m, cm, rh0r, volr, cwr, hs);
     return MPG_OK;
+}
+
+// ---- iprc = 4: the column blocks of laplc itself.  laplc's gradient uses face averages
+// (p_n + p_j)/2, so in a column it couples level k with k and k+-2 only: the block is
+// tridiagonal on the even and on the odd levels.  With S_k the upward face between levels k and
+// k+1, s_m = (0.5 dt/vol_m)(1, 1, cw_m) and P_m the bcv(.,0) projection at node m:
+//   A[k][k+2] = ((S_k/2) . rh0_{k+1} P_{k+1}(s_{k+1} (*) S_{k+1}/2)) / (vol_k rh0_k)
+//   A[k][k-2] = ((S_{k-1}/2) . rh0_{k-1} P_{k-1}(s_{k-1} (*) S_{k-2}/2)) / (vol_k rh0_k)
+//   A[k][k]   = (sum over faces f of k, neighbour j: -(S_f/2) . rh0_j P_j(s_j (*) S_f/2)
+//                + e_k . rh0_k P_k(s_k (*) e_k)) / (vol_k rh0_k),
+// e_k = (sum of k's outward faces)/2, plus its boundary faces sbb when iper = 0.  The entries are
+// accumulated in the reference's edge order, then factorised per parity chain (Thomas from the
+// bottom) into the interleaved layout of the line solve.
+namespace {
+struct WideCtx {
+    const mpg_params *P;
+    const mpg_mesh_ref *m;
+    const std::vector<double> &rh0r, &volr, &cw;
+    std::vector<int32_t> bst, blst;
+    double dt;
+    void bcv_vec(int i, double v[3]) const {
+        const bool per = (P->isfera == 1 || P->iper == 2);
+        for (int b = bst[i]; b < bst[i + 1]; ++b) {
+            const int q = blst[b];
+            const int t = m->ibpoin[(size_t)m->nfacesx + q];
+            const double a1 = m->anp[q], a2 = m->anp[(size_t)m->nfacesx + q], a3 = m->anp[2 * (size_t)m->nfacesx + q];
+            if (t == 11 || (!per && (t == 5 || t == 6))) {
+                double vn = v[0] * a1 + v[1] * a2 + v[2] * a3;
+                v[0] = v[0] - a1 * vn;
+                v[1] = v[1] - a2 * vn;
+                v[2] = v[2] - a3 * vn;
+            }
+            if (!per && (t == 7 || t == 8)) v[0] = 0.;
+        }
+    }
+    // (a/2) . rh0_j P_j(s_j (*) b/2)
+    double path(int j, const double a[3], const double b[3]) const {
+        const double h = 0.5 * (dt / volr[j]);
+        const double sc[3] = {h / (1.0 * 1.0), h / (1.0 * 1.0), h * cw[j]};
+        double v[3];
+        for (int d = 0; d < 3; ++d) v[d] = sc[d] * (0.5 * b[d]);
+        bcv_vec(j, v);
+        const double r = rh0r[j];
+        return (0.5 * a[0]) * (r * v[0]) + (0.5 * a[1]) * (r * v[1]) + (0.5 * a[2]) * (r * v[2]);
+    }
+};
+}  // namespace
+
+void mpg_wide_entries(const mpg_params *P, const mpg_mesh_ref *m, const HostColumnMesh &cm,
+                      const std::vector<double> &rh0r, const std::vector<double> &volr,
+                      const std::vector<double> &cw, std::vector<double> &lo, std::vector<double> &dg,
+                      std::vector<double> &hi) {
+    const int N = cm.N, L = cm.L;
+    WideCtx W{P, m, rh0r, volr, cw, {}, {}, P->delt};
+    W.bst.assign(N + 1, 0);
+    W.blst.assign(m->nboun, 0);
+    for (int b = 0; b < m->nboun; ++b) W.bst[m->ibpoin[b] - 1 + 1]++;
+    for (int i = 0; i < N; ++i) W.bst[i + 1] += W.bst[i];
+    {
+        std::vector<int32_t> fill(N, 0);
+        for (int b = 0; b < m->nboun; ++b) {
+            const int i = m->ibpoin[b] - 1;
+            W.blst[W.bst[i] + fill[i]++] = b;
+        }
+    }
+    EdgeView ev{m};
+    const int64_t nall = ev.n();
+    lo.assign(N, 0.); dg.assign(N, 0.); hi.assign(N, 0.);
+    std::vector<double> ex(N, 0.), ey(N, 0.), ez(N, 0.), sux(N, 0.), suy(N, 0.), suz(N, 0.);
+    for (int64_t j = 0; j < nall; ++j) {
+        const int i1 = ev.i1(j), i2 = ev.i2(j);
+        const double S[3] = {ev.s(j, 0), ev.s(j, 1), ev.s(j, 2)};
+        ex[i1] += S[0]; ey[i1] += S[1]; ez[i1] += S[2];
+        ex[i2] -= S[0]; ey[i2] -= S[1]; ez[i2] -= S[2];
+        dg[i1] = dg[i1] - W.path(i2, S, S);
+        dg[i2] = dg[i2] - W.path(i1, S, S);
+    }
+    for (int i = 0; i < N; ++i) {
+        double e3[3] = {0.5 * ex[i], 0.5 * ey[i], 0.5 * ez[i]};
+        if (P->isfera == 0 && P->iper == 0)
+            for (int b = W.bst[i]; b < W.bst[i + 1]; ++b) {
+                const int q = W.blst[b];
+                e3[0] += m->sbb[q];
+                e3[1] += m->sbb[(size_t)m->nfacesx + q];
+                e3[2] += m->sbb[2 * (size_t)m->nfacesx + q];
+            }
+        const double a2[3] = {2. * e3[0], 2. * e3[1], 2. * e3[2]};
+        dg[i] = dg[i] + W.path(i, a2, a2);
+    }
+    // upward face of each node (reference index of the lower end)
+    auto up = [&](int i) { const int n = cm.perm[i]; return (n % L) + 1 < L ? cm.iperm[n + 1] : -1; };
+    auto dn = [&](int i) { const int n = cm.perm[i]; return (n % L) > 0 ? cm.iperm[n - 1] : -1; };
+    for (int64_t j = 0; j < nall; ++j) {
+        const int i1 = ev.i1(j), i2 = ev.i2(j);
+        if (cm.perm[i1] / L != cm.perm[i2] / L) continue;
+        const double sg = up(i1) == i2 ? 1. : -1.;
+        const int lower = sg > 0 ? i1 : i2;
+        sux[lower] = sg * ev.s(j, 0);
+        suy[lower] = sg * ev.s(j, 1);
+        suz[lower] = sg * ev.s(j, 2);
+    }
+    for (int i = 0; i < N; ++i) {
+        const double vr = volr[i] * rh0r[i];
+        const int u1 = up(i), d1 = dn(i);
+        if (u1 >= 0 && up(u1) >= 0) {
+            const double a[3] = {sux[i], suy[i], suz[i]}, b[3] = {sux[u1], suy[u1], suz[u1]};
+            hi[i] = W.path(u1, a, b) / vr;
+        }
+        if (d1 >= 0 && dn(d1) >= 0) {
+            const int d2 = dn(d1);
+            const double a[3] = {sux[d1], suy[d1], suz[d1]}, b[3] = {sux[d2], suy[d2], suz[d2]};
+            lo[i] = W.path(d1, a, b) / vr;
+        }
+        dg[i] = dg[i] / vr;
+    }
+}
+
+void mpg_wide_coeffs(const mpg_params *P, const mpg_mesh_ref *m, const HostColumnMesh &cm,
+                     const std::vector<double> &rh0r, const std::vector<double> &volr,
+                     const std::vector<double> *cwr, HostStatic *hs) {
+    const int NC = cm.NC, L = cm.L;
+    const size_t nint_sz = (size_t)((NC + 31) / 32) * 32 * L;
+    for (int q = 0; q < 2; ++q) {
+        std::vector<double> lo, dg, hi;
+        mpg_wide_entries(P, m, cm, rh0r, volr, cwr[q], lo, dg, hi);
+        hs->wa[q].assign(nint_sz, 0.);
+        hs->wm[q].assign(nint_sz, 1.);
+        hs->wcp[q].assign(nint_sz, 0.);
+        for (int col = 0; col < NC; ++col)
+            for (int par = 0; par < 2; ++par) {
+                double cpprev = 0.;
+                for (int k = par; k < L; k += 2) {
+                    const int i = cm.iperm[col * L + k];
+                    const double mm = k < 2 ? dg[i] : dg[i] - lo[i] * cpprev;
+                    const double cp = hi[i] / mm;
+                    const int64_t li = line_index(col, k, L);
+                    hs->wa[q][li] = lo[i];
+                    hs->wm[q][li] = 1. / mm;
+                    hs->wcp[q][li] = cp;
+                    cpprev = cp;
+                }
+            }
+    }
 }
