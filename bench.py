@@ -547,6 +547,59 @@ def main():
                                                    "forward, corrects the vertical-line preconditioner"})
             sv.close()
 
+        # laplc's own column blocks as the line preconditioner (iprc = 4), FP64 and mixed.  Run
+        # last and guarded: a failure here is reported in the line instead of ending the run.
+        for vname, prec in (("column_blocks_fp64", 0), ("column_blocks_mixed", 1)):
+            try:
+                Pv = build_params(name, precision=prec)
+                Pv.iprc = 4
+                sv = Solver(Pv, rm, device=local)
+                try:
+                    sv.setup()
+                    if Pv.nscal:
+                        sv.set(F_UNK + 4, gaussian_scalar(rm))
+                    for _ in range(args.warmup):
+                        sv.step()
+                    sv.synchronize()
+                    stream_v = torch.cuda.ExternalStream(sv.stream())
+                    barrier()
+                    torch.cuda.synchronize()
+                    sv.kernel_timing(True)
+                    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a0.record(stream_v)
+                    vit = []
+                    for _ in range(args.steps):
+                        dv = sv.step()
+                        vit.append((dv.niter1, dv.niter))
+                    a1.record(stream_v)
+                    a1.synchronize()
+                    barrier()
+                    vms = max_over_ranks(a0.elapsed_time(a1))
+                    vkt = sv.kernel_times()
+                    vsolve = vkt.get("pressure_solve", (1, 0.0))
+                    err = {}
+                    for k, nm in enumerate(("u", "v", "w", "theta")):
+                        a, b = sv.get(F_UNK + k), ref_fields[k]
+                        err[nm] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+                    vval = whole_job_rate(world, args.steps, vms / 1000.0)
+                    variants[vname] = {
+                        "value": vval, "unit": "steps/s", "ms_per_step": vms / args.steps,
+                        "ms_per_pressure_solve": round(vsolve[1] / max(vsolve[0], 1), 3),
+                        "gcr_iters_per_solve": round(float(np.mean([a for p in vit for a in p])), 2),
+                        "gcr_iters_first_solve": round(float(np.mean([p[0] for p in vit])), 2),
+                        "speedup_vs_fp64": round(vval / value, 3),
+                        "rel_l2_vs_fp64": err,
+                        "kernels_ms": {k: round(v[1], 2) for k, v in vkt.items()},
+                        "preconditioner": "laplc's column blocks (tridiagonal on even and odd levels), "
+                                          "stride-2 Thomas in FP64",
+                        "precision": "FP64" if prec == 0 else
+                                     "FP32 face vectors, MPDATA fluxes, GCR directions and operator; "
+                                     "FP64 p, r, inner products, coefficients, stopping test, Thomas solves"}
+                finally:
+                    sv.close()
+            except Exception as exc:                      # reported, not fatal
+                variants[vname] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sec, n_sample = cpu_sample(3, 1)
