@@ -433,3 +433,22 @@ def test_wide_line_cuts_gcr_iterations():
     assert all(3 * b <= a for a, b in zip(it[2], it[4])), it      # measured 123/32 set-up, 62-92/11-12 steps
     rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
     assert rel(res[4][0], res[2][0]) <= 1e-6
+
+
+def test_column_blocks_converge_where_the_compact_line_stalls():
+    """The stiff case of the workload family (levels stretched to a lowest aspect ratio
+    dx/dz = 1e3, N = 0.02 1/s, h0 = 800 m, GCR(5)), on 16x16x32: with the compact vertical line the
+    solves stall (the residual stops decreasing, status 1); with laplc's column blocks every solve
+    converges within tens of iterations."""
+    from src_b200 import mesh
+    rm = mesh.generate(16, L=32, seed=0, h0=800.0, stretch_dz0=7.5).to_reference()
+    out = {}
+    for iprc in (2, 4):
+        o = Oracle(RunParams(delt=6.0, iprc=iprc, lord=5, strat=0.02 ** 2 / 9.80616, itr=400), rm)
+        o.setup()
+        s0 = o.gcr_stats()
+        d = o.step()
+        out[iprc] = (s0.status, s0.niter, o.gcr_stats().status, d.niter1)
+    assert out[2][0] == 1 and out[2][2] == 1, out          # stalled
+    assert out[4][0] == 0 and out[4][2] == 0, out          # converged
+    assert out[4][1] <= 60 and out[4][3] <= 30, out
