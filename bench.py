@@ -37,6 +37,11 @@ WORKLOADS = {
     "fp64_48x48x41": (48, 41, 10.0, 400.0, 3, 0),
     "fp64_256x256x81": (256, 81, 6.0, 400.0, 3, 1),
 }
+# the stiff large case: levels stretched so the lowest aspect ratio dx/dz is about 1e3 (dx = 117 m,
+# lowest dz = 0.117 m), N = 0.02 1/s, GCR(5).  The compact vertical line stalls on such cells, so
+# its plain method uses laplc's column blocks (iprc = 4).  Run on request only (--workload).
+WORKLOADS["stiff_1024x1024x64"] = (1024, 64, 6.0, 800.0, 5, 0)
+WORKLOAD_EXTRA = {"stiff_1024x1024x64": dict(stretch_dz0=0.117, N=0.02, iprc=4)}
 DEFAULT = "fp64_512x512x81"
 CPU_SAMPLE = "fp64_48x48x41"
 L2_BYTES = 126 * 2 ** 20
@@ -66,14 +71,15 @@ def whole_job_rate(world, steps, seconds):
 def build_params(name, precision=0):
     from src_b200.cabi import RunParams
     nx, L, dt, h0, lord, nscal = WORKLOADS[name]
-    return RunParams(delt=dt, lord=lord, nscal=nscal, eps0=1e-8, itr=200, iprc=2, itrp1=1,
-                     lipps=1, strat=0.01 ** 2 / 9.80616, precision=precision)
+    ex = WORKLOAD_EXTRA.get(name, {})
+    return RunParams(delt=dt, lord=lord, nscal=nscal, eps0=1e-8, itr=200, iprc=ex.get("iprc", 2), itrp1=1,
+                     lipps=1, strat=ex.get("N", 0.01) ** 2 / 9.80616, precision=precision)
 
 
 def build_mesh(name):
     from src_b200 import mesh
     nx, L, dt, h0, lord, nscal = WORKLOADS[name]
-    cm = mesh.generate(nx, L=L, seed=0, h0=h0)
+    cm = mesh.generate(nx, L=L, seed=0, h0=h0, stretch_dz0=WORKLOAD_EXTRA.get(name, {}).get("stretch_dz0"))
     return cm, cm.to_reference()
 
 
@@ -322,7 +328,11 @@ def workload_config(name):
     return {"workload": f"plain FP64 MPDATA+GCR step, {nx}x{nx} jittered periodic columns x {L} levels "
                         f"({nx * nx * L} nodes), Agnesi hill h0={h0:g} m, dt={dt:g} s",
             "nodes": nx * nx * L, "edges": 3 * nx * nx * L + nx * nx * (L - 1), "levels": L, "dt_s": dt,
-            "gcr": f"GCR({lord}) to max|r|*dt<=1e-8, vertical-line preconditioner",
+            "gcr": f"GCR({lord}) to max|r|*dt<=1e-8, " + (
+                "laplc's column blocks as the line preconditioner" if WORKLOAD_EXTRA.get(name, {}).get("iprc") == 4
+                else "vertical-line preconditioner"),
+            **({"levels_stretched_lowest_dz_m": WORKLOAD_EXTRA[name]["stretch_dz0"],
+                "N_per_s": WORKLOAD_EXTRA[name]["N"]} if name in WORKLOAD_EXTRA else {}),
             "mpdata": "iord=2 + nonoscillatory (FCT)", "passive_scalars": nscal,
             "l2": "inputs larger than L2 (each FP64 node field is 8*nodes bytes > 126 MB)"}
 

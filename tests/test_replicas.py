@@ -75,3 +75,17 @@ def test_reference_arm_sums_replicas():
     line = json.loads(out.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["cpu_baseline"]["cores"] == 2 and line["e2e"]["value"] == line["value"]
+
+
+def test_bench_workloads():
+    """The headline workload keeps the compact line (iprc = 2, GCR(3), N = 0.01); the stiff case
+    (1024x1024x64, lowest dx/dz about 1e3, N = 0.02, GCR(5)) uses laplc's column blocks."""
+    sys.path.insert(0, ROOT)
+    import bench
+    P = bench.build_params("fp64_512x512x81")
+    assert (P.iprc, P.lord, P.strat, P.delt) == (2, 3, 0.01 ** 2 / 9.80616, 6.0)
+    S = bench.build_params("stiff_1024x1024x64")
+    assert (S.iprc, S.lord, S.strat) == (4, 5, 0.02 ** 2 / 9.80616)
+    from src_b200 import mesh
+    z = mesh.level_set(64, 20e3, stretch_dz0=bench.WORKLOAD_EXTRA["stiff_1024x1024x64"]["stretch_dz0"])
+    assert 900 < (120e3 / 1024) / (z[1] - z[0]) < 1100
