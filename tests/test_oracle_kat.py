@@ -452,3 +452,16 @@ def test_column_blocks_converge_where_the_compact_line_stalls():
     assert out[2][0] == 1 and out[2][2] == 1, out          # stalled
     assert out[4][0] == 0 and out[4][2] == 0, out          # converged
     assert out[4][1] <= 60 and out[4][3] <= 30, out
+
+
+def test_library_column_block_factors_on_the_channel(open_mesh):
+    """mpg_analyze_wide equals the oracle's factorisation bit for bit on the open channel too
+    (boundary points of types 5-8 at every level, iper = 0 closure in the self term)."""
+    from src_b200 import api
+    _, rm = open_mesh
+    P = RunParams(delt=10.0, iper=0, iprc=4)
+    o = Oracle(P, rm)
+    o.setup()
+    for impfl in (0, 1):
+        for x, y in zip(api.analyze_wide(P, rm, impfl), o.wide_factors(impfl)):
+            assert np.array_equal(x, y)
