@@ -23,6 +23,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -139,8 +140,8 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f".clocks_{os.getpid()}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/.clocks_{os.getpid()}.csv"
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
 
     def start(self):
         try:
@@ -218,8 +219,19 @@ def build_params_copy(P, **kw):
     return RunParams(**{**P.__dict__, **kw})
 
 
+CPU_WORK_SAMPLE = "fp64_256x256x81"
+# GCR iterations per time step (the two pressure solves together) of a workload, as measured by
+# the FP64 GPU path of this bench, which runs the oracle's algorithm step for step (bit for bit
+# with the oracle replaying the GPU's summation order).  The CPU legs use it to turn per-iteration
+# costs into a per-step cost, because a single full-size step of the serial restatement takes
+# about 25 minutes (5 MPDATA fields and ~240 GCR iterations over 21.2M nodes).  The b200 arm's
+# cpu_baseline uses the count its own run measured instead.
+GCR_ITERS_PER_STEP = {"fp64_512x512x81": 239.9, "fp64_256x256x81": 150.0, "fp64_48x48x41": 130.0}
+
+
 def cpu_sample(steps, warmup):
-    """Oracle (CPU restatement, 1 thread) full steps of the 48x48x41 workload."""
+    """Oracle (CPU restatement, 1 thread) full steps of the 48x48x41 workload: seconds per step and
+    the sample's node count (the per-node extrapolation)."""
     from oracle.oracle import Oracle
     cm, rm = build_mesh(CPU_SAMPLE)
     o = Oracle(build_params(CPU_SAMPLE), rm)
@@ -233,6 +245,53 @@ def cpu_sample(steps, warmup):
     return dt, rm.npoin
 
 
+def work_oracle(sample):
+    """An oracle on the sample workload whose GCR solves stop after one restart cycle (itr = 1),
+    set up, for timing the components of a step.  Returns (oracle, reference mesh)."""
+    from oracle.oracle import Oracle
+    from src_b200.cabi import F_UNK
+    cm, rm = build_mesh(sample)
+    P = build_params(sample)
+    P.itr = 1
+    o = Oracle(P, rm)
+    o.setup()
+    if P.nscal:
+        o.set(F_UNK + 4, gaussian_scalar(rm))
+    return o, rm
+
+
+def work_sample(o):
+    """Seconds of one call of each component of a time step, on the oracle's mesh:
+    one MPDATA field, prfr, div(-1), the line preconditioner, laplc, a gcrk capped at one restart
+    cycle (from which the cost of one GCR iteration follows) and the per-step diagnostics."""
+    from src_b200.cabi import F_PRPOT, F_UNK, F_UNK1
+    T = time.perf_counter
+    t = {}
+    a = T(); o.mpdatamper(o.get(F_UNK + 1), 2); t["mpdata_field"] = T() - a
+    p, u = o.get(F_PRPOT), [o.get(F_UNK1 + k) for k in range(3)]
+    a = T(); uo = o.prfr(p, *u, 1); t["prfr"] = T() - a
+    a = T(); r, _ = o.div(*uo, -1); t["div"] = T() - a
+    a = T(); q = o.precon(r, 2, 1); t["precon"] = T() - a
+    a = T(); o.laplc(q, 1); t["laplc"] = T() - a
+    a = T(); _, _, st = o.gcrk(p, *u, 1); t["gcrk_capped"] = T() - a
+    t["gcrk_capped_iterations"] = int(st.niter)
+    t["iteration"] = max(t["gcrk_capped"] - t["prfr"] - t["div"] - t["precon"] - t["laplc"], 0.0) / max(st.niter, 1)
+    a = T(); o.div(*uo, 1); o.courant(1); o.stats(); t["diagnostics"] = T() - a
+    return t
+
+
+def modelled_step_seconds(t, iters_per_step, nfields, scale):
+    """Seconds of one full time step from component times `t` (work_sample) measured on a mesh
+    `scale` times smaller: nfields MPDATA fields; two pressure solves, each prfr + div + precon +
+    laplc before its iterations and the caller's prfr after it; iters_per_step GCR iterations; the
+    diagnostics.  Every component is a fixed number of passes over the nodes, so its cost scales
+    with the node count once the fields exceed the CPU caches (the 256x256x81 sample holds 42 MB
+    per field)."""
+    solve_fixed = t["prfr"] + t["div"] + t["precon"] + t["laplc"] + t["prfr"]
+    return scale * (nfields * t["mpdata_field"] + 2 * solve_fixed + iters_per_step * t["iteration"] +
+                    t["diagnostics"])
+
+
 _BARRIER = None
 
 
@@ -242,22 +301,31 @@ def _replica_init(barrier):
 
 
 def _replica_sample(args):
-    """One serial oracle replica: set-up and warm-up, wait for every replica, then time steps."""
-    steps, warmup = args
+    """One serial oracle replica: real steps of the 48x48x41 mesh (the per-node extrapolation),
+    then component samples of the sample workload (the per-work model); every replica waits for
+    the others before each timed part."""
+    steps, warmup, sample = args
     from oracle.oracle import Oracle
     cm, rm = build_mesh(CPU_SAMPLE)
     o = Oracle(build_params(CPU_SAMPLE), rm)
     o.setup()
-    for _ in range(warmup):
-        o.step()
+    o.step()
     _BARRIER.wait()
     t0 = time.perf_counter()
-    for _ in range(steps):
+    for _ in range(2):
         o.step()
-    return (time.perf_counter() - t0) / steps, rm.npoin
+    per_node = ((time.perf_counter() - t0) / 2, rm.npoin)
+    del o
+    ow, rmw = work_oracle(sample)
+    for _ in range(warmup):
+        work_sample(ow)
+    _BARRIER.wait()
+    samples = [work_sample(ow) for _ in range(steps)]
+    return per_node, samples, rmw.npoin
 
 
-REF_MAX_REPLICAS = 64          # bounds the reference arm's memory (about 160 MB per replica)
+REF_MAX_REPLICAS = 64          # bounds the reference arm's memory
+REF_REPLICA_BYTES = 4 << 30    # one replica: the 256x256x81 sample oracle (~2.8 GB) and its mesh
 
 
 def host_threads():
@@ -281,12 +349,12 @@ def host_threads():
 
 def reference_replicas(requested=0):
     """Replicas for the reference arm: one per usable host thread (or as requested), at most
-    REF_MAX_REPLICAS and at most what a quarter of the available memory holds at 400 MB each."""
+    REF_MAX_REPLICAS and at most what half of the available memory holds at REF_REPLICA_BYTES each."""
     n = host_threads() if requested <= 0 else min(requested, host_threads())
     try:
         for ln in open("/proc/meminfo"):
             if ln.startswith("MemAvailable:"):
-                n = min(n, max(1, int(ln.split()[1]) * 1024 // 4 // (400 << 20)))
+                n = min(n, max(1, int(ln.split()[1]) * 1024 // 2 // REF_REPLICA_BYTES))
     except OSError:
         pass
     return max(1, min(n, REF_MAX_REPLICAS))
@@ -296,29 +364,55 @@ def run_reference(args):
     """The reference's path on the host cores.  The reference is serial Fortran (no compiler for
     it here), so its restatement runs as one independent replica per usable host thread (at most
     REF_MAX_REPLICAS, and as many as memory allows), started together in spawned processes, and
-    the throughput of all replicas is summed."""
+    the throughput of all replicas is summed.
+
+    A full step of the 21.2M-node workload takes the serial restatement about 25 minutes, so each
+    replica times the components of a step on a sample mesh instead (work_sample: one MPDATA field,
+    one GCR iteration, the fixed parts of a solve, the diagnostics) and `value` is the step they
+    add up to at full size (modelled_step_seconds) with the workload's GCR iteration count.  The
+    per-node extrapolation of real 48x48x41 steps, which needs half as many iterations per solve
+    and keeps its fields in cache, is reported beside it."""
     rank, _, world = dist_env()
     if rank != 0:
         return
     import multiprocessing as mp
-    nx, L = WORKLOADS[DEFAULT][0], WORKLOADS[DEFAULT][1]
+    name, sample = DEFAULT, args.ref_sample
+    nx, L = WORKLOADS[name][0], WORKLOADS[name][1]
     n_work = nx * nx * L
+    nfields = 4 + WORKLOADS[name][5]
+    iters = GCR_ITERS_PER_STEP[name]
     nrep = reference_replicas(args.ref_replicas)
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(nrep)
     with ctx.Pool(nrep, initializer=_replica_init, initargs=(barrier,)) as pool:
-        res = pool.map(_replica_sample, [(args.steps, args.warmup)] * nrep)
-    node_steps = sum(n / sec for sec, n in res)
-    value = node_steps / n_work
-    secs = sorted(sec for sec, _ in res)
-    sample = (f"{nrep} concurrent serial oracle replicas, each {args.steps} steps (after {args.warmup} "
-              f"warm-up) of the 48x48x41 mesh ({res[0][1]} nodes, dt=10 s), {secs[0]:.3f}-{secs[-1]:.3f} "
-              f"s/step per replica; summed node-steps/s scaled to {n_work} nodes")
+        res = pool.map(_replica_sample, [(args.steps, args.warmup, sample)] * nrep)
+    per_node = sum(n / sec for (sec, n), _, _ in res) / n_work
+    step_s = []                      # modelled full-size step time of each replica, per sample step
+    for _, samples, n_s in res:
+        step_s.append([modelled_step_seconds(t, iters, nfields, n_work / n_s) for t in samples])
+    value = sum(1.0 / float(np.mean(x)) for x in step_s)
+    t0 = {k: float(np.median([s[k] for _, ss, _ in res for s in ss])) for k in res[0][1][0]}
+    n_s = res[0][2]
+    sample_txt = (f"{nrep} concurrent serial oracle replicas; each timed {args.steps} samples (after {args.warmup} "
+                  f"untimed) of the components of one step on the {sample} mesh ({n_s} nodes, GCR solves capped "
+                  f"at one restart cycle): median s per call mpdata_field {t0['mpdata_field']:.3f}, prfr "
+                  f"{t0['prfr']:.3f}, div {t0['div']:.3f}, precon {t0['precon']:.3f}, laplc {t0['laplc']:.3f}, "
+                  f"GCR iteration {t0['iteration']:.3f}, diagnostics {t0['diagnostics']:.3f}; a step of the "
+                  f"{n_work}-node workload = {nfields} fields + 2 solves of {iters:g} GCR iterations in all, "
+                  f"scaled by nodes x{n_work / n_s:.2f}: {float(np.mean(step_s[0])):.0f} s per replica")
+    cfg = workload_config(name)
+    cfg["cpu_sample"] = (f"components of a step timed on the {sample} mesh and modelled at full size "
+                         f"({iters:g} GCR iterations per step, the count the FP64 GPU path measures on this "
+                         f"workload); not a run of the full workload")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": workload_config(DEFAULT),
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": nrep, "kind": "port", "sample": sample},
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": nrep, "kind": "port", "sample": sample_txt},
+            "per_node_extrapolation": {
+                "value": per_node, "unit": "steps/s",
+                "sample": f"{nrep} replicas x 2 real steps of the 48x48x41 mesh ({res[0][0][1]} nodes, "
+                          f"about half the GCR iterations per solve), node-steps/s summed and divided by {n_work}"},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -345,6 +439,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-replicas", type=int, default=0,
                     help="--impl reference: oracle replicas (default: one per host thread)")
+    ap.add_argument("--ref-sample", default=CPU_WORK_SAMPLE, choices=sorted(WORKLOADS),
+                    help="--impl reference and the CPU baseline: mesh on which the step's components are timed")
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -490,7 +586,9 @@ def main():
     # ---------------- variants on the same workload (reported beside the headline FP64 path)
     variants = {}
     if not args.no_variants:
-        for vname, prec, iprc in (("mixed", 1, 2), ("learned_mixed", 1, 3)):
+        base = P.iprc
+        plan = (("mixed", 1, 2), ("learned_mixed", 1, 3)) if base == 2 else (("mixed", 1, base),)
+        for vname, prec, iprc in plan:
             Pv = build_params(name, precision=prec)
             Pv.iprc = iprc
             weights_src = None
@@ -559,7 +657,7 @@ def main():
 
         # laplc's own column blocks as the line preconditioner (iprc = 4), FP64 and mixed.  Run
         # last and guarded: a failure here is reported in the line instead of ending the run.
-        for vname, prec in (("column_blocks_fp64", 0), ("column_blocks_mixed", 1)):
+        for vname, prec in ((("column_blocks_fp64", 0), ("column_blocks_mixed", 1)) if base == 2 else ()):
             try:
                 Pv = build_params(name, precision=prec)
                 Pv.iprc = 4
@@ -612,11 +710,26 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sec, n_sample = cpu_sample(3, 1)
-        v = (1.0 / sec) * n_sample / N
-        cpu = {"value": v, "unit": "steps/s", "cores": 1, "kind": "port",
-               "sample": f"3 oracle steps of the 48x48x41 mesh ({n_sample} nodes, dt=10 s), {sec:.3f} s/step, "
-                         f"per-node cost scaled to {N} nodes"}
+        # per-work model: components of a step timed on the sample mesh (1 thread), combined with
+        # this run's own GCR iteration count and field count at the workload's node count
+        ow, rmw = work_oracle(args.ref_sample)
+        work_sample(ow)                                   # untimed: first touch of the arrays
+        t = work_sample(ow)
+        del ow
+        iters_step = float(np.mean([a + b for a, b in iters]))
+        nfields = 4 + P.nscal
+        step_s = modelled_step_seconds(t, iters_step, nfields, N / rmw.npoin)
+        sec, n_sample = cpu_sample(2, 1)
+        cpu = {"value": 1.0 / step_s, "unit": "steps/s", "cores": 1, "kind": "port",
+               "sample": f"oracle components of one step timed once on the {args.ref_sample} mesh ({rmw.npoin} "
+                         f"nodes): mpdata_field {t['mpdata_field']:.3f} s, GCR iteration {t['iteration']:.3f} s, "
+                         f"prfr {t['prfr']:.3f}, div {t['div']:.3f}, precon {t['precon']:.3f}, laplc "
+                         f"{t['laplc']:.3f}, diagnostics {t['diagnostics']:.3f}; modelled at {N} nodes with this "
+                         f"run's {iters_step:.1f} GCR iterations per step and {nfields} fields: {step_s:.0f} s/step",
+               "per_node_extrapolation": {
+                   "value": (1.0 / sec) * n_sample / N, "unit": "steps/s",
+                   "sample": f"2 oracle steps of the 48x48x41 mesh ({n_sample} nodes, dt=10 s), {sec:.3f} s/step, "
+                             f"per-node cost scaled to {N} nodes"}}
 
     if rank == 0:
         last = diags[-1]

@@ -10,7 +10,7 @@
  * and of the node loops of the time-step driver `mpsolver` (ref.f:58-479) that sit between them,
  * so that every field stays resident on the GPU for a whole run.
  *
- * Conventions (they follow the Fortran caller, see the Fortran interface block in INTEGRATION.md):
+ * Conventions (they follow the Fortran caller):
  *   * REAL is double (the reference compiled with -fdefault-real-8 -fdefault-double-8).
  *   * INTEGER is int32; node/edge indices in mesh arrays are 1-based, as in the COMMON blocks.
  *   * 2-D Fortran arrays arrive as base pointers with their leading dimension (npoinx, nedgex,
@@ -325,13 +325,19 @@ int mpg_restart_read(mpg_handle h, const char *path, int format, int *ntime);
  *
  * `press` and `alap` are caller-owned DEVICE arrays of npoin doubles in reference node order on
  * the handle's device.  The work is queued on the handle's stream (mpg_get_stream) and the
- * call returns without waiting; order your own stream against it before reading alap.
+ * call returns without waiting.  Both directions need ordering against that stream: whatever
+ * writes `press` (a kernel or copy on another stream) must have completed, or be ordered before
+ * the call with an event the handle's stream waits on; and your own stream must wait for the
+ * handle's stream before it reads `alap`.
  * Scratch is a static device array sized for MPG_NOALLOC_MAX_NODES nodes (5 MiB), held by every
  * GPU that loads the library until the process exits; larger meshes get MPG_ERR_ARG.  The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress): make that first
- * call before any stream capture.  All calls share the one array, so calls that overlap on the
- * GPU (two handles, or two streams, on the same device) race; serialise them.  The call
- * allocates nothing: no cudaMalloc, cudaFree or allocating library routine. */
+ * call on a device looks up the array's device address (cudaGetSymbolAddress) and keeps it for
+ * the life of the process: make that first call before any stream capture, and do not call the
+ * entry point again after cudaDeviceReset on that device (the kept address belongs to the old
+ * context).  All calls share the one array, so calls that overlap on the GPU (two handles, or
+ * two streams, on the same device) race; serialise them.  The caller's current device is the
+ * same after the call as before.  The call allocates nothing: no cudaMalloc, cudaFree or
+ * allocating library routine. */
 #define MPG_NOALLOC_MAX_NODES 131072
 int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap, int impfl);
 

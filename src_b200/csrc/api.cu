@@ -1897,6 +1897,12 @@ extern "C" int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap
     if (h->dev < 0 || h->dev >= kNoallocMaxDevices)
         return mpg_fail(MPG_ERR_ARG, "laplc_noalloc: device index out of range");
     if (press == alap) return mpg_fail(MPG_ERR_ARG, "laplc_noalloc: input and output must differ");
+    // the caller's current device is put back on every return
+    struct RestoreDevice {
+        int prev = -1;
+        RestoreDevice() { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; }
+        ~RestoreDevice() { if (prev >= 0) cudaSetDevice(prev); }
+    } restore;
     MPG_CUDA(cudaSetDevice(h->dev));
     double *base;
     {

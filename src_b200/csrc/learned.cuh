@@ -324,9 +324,12 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const float *
         }
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // ---- epilogue: row k = 32w + lane, 32 channels
-        uint32_t r[32];
-        {
+        // ---- epilogue: row k = 32w + lane, 32 channels.  After a wait that gave up (ok is
+        // block-uniform) the accumulator is not read: the rows are written as NaN instead and the
+        // column loop ends.  The bounded wait guards against an arrival that never comes; it
+        // cannot make an MMA that is still running safe to abandon.
+        uint32_t r[32] = {};
+        if (ok) {
             const uint32_t taddr = tmem + ((uint32_t)(32 * w) << 16);
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
                          "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"

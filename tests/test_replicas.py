@@ -66,15 +66,26 @@ def test_single_rank_is_identity():
 
 def test_reference_arm_sums_replicas():
     """`bench.py --impl reference` runs one serial oracle replica per requested host thread and
-    reports their summed throughput on the workload's metric, with the core count."""
+    reports their summed throughput on the workload's metric, with the core count; the config
+    says that the value is modelled from components timed on a sample mesh."""
     import json
     import subprocess
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-                          "--steps", "1", "--warmup", "3", "--ref-replicas", "2"],
+                          "--steps", "1", "--warmup", "3", "--ref-replicas", "2", "--ref-sample", "fp64_48x48x41"],
                          capture_output=True, text=True, timeout=600, check=True).stdout
     line = json.loads(out.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["cpu_baseline"]["cores"] == 2 and line["e2e"]["value"] == line["value"]
+    assert "fp64_48x48x41" in line["config"]["cpu_sample"] and line["per_node_extrapolation"]["value"] > 0
+
+
+def test_step_model_adds_the_components():
+    """The per-work model: fields x MPDATA + two solves' fixed parts + iterations + diagnostics,
+    scaled by the node ratio."""
+    sys.path.insert(0, ROOT)
+    import bench
+    t = dict(mpdata_field=1.0, prfr=0.1, div=0.2, precon=0.3, laplc=0.4, iteration=0.5, diagnostics=0.6)
+    assert bench.modelled_step_seconds(t, 100, 5, 4.0) == pytest.approx(4.0 * (5 + 2 * 1.1 + 50 + 0.6))
 
 
 def test_bench_workloads():
