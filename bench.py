@@ -431,6 +431,52 @@ def workload_config(name):
             "l2": "inputs larger than L2 (each FP64 node field is 8*nodes bytes > 126 MB)"}
 
 
+def report_mixed_errors(args):
+    """The mixed-precision path against the FP64 path on the same workload, run side by side for
+    max(--error-steps) steps: relative L2 of u, v, w, theta' and pi' (prpot) at each requested
+    step, the GCR iterations of both, and the passive scalar's minimum, maximum and mass on the
+    FP64 path (sign, bounds and conservation).  The FP64 path agrees bit for bit with the oracle
+    replaying the GPU's summation order, so it stands for the FP64 oracle at a size the CPU
+    restatement cannot run in reasonable time.  Prints one JSON object."""
+    from src_b200.api import Solver
+    from src_b200.cabi import F_PRPOT, F_UNK
+    name = args.workload
+    want = sorted({int(x) for x in args.error_steps.split(",") if x.strip()})
+    cm, rm = build_mesh(name)
+    runs = {}
+    for tag, prec in (("fp64", 0), ("mixed", 1)):
+        s = Solver(build_params(name, precision=prec), rm, device=0)
+        s.setup()
+        if s.params.nscal:
+            s.set(F_UNK + 4, gaussian_scalar(rm))
+        runs[tag] = s
+    s64, smx = runs["fp64"], runs["mixed"]
+    m0 = s64.stats().mass[4] if s64.params.nscal else None
+    rows = []
+    for step in range(1, want[-1] + 1):
+        d64, dmx = s64.step(), smx.step()
+        if step in want:
+            err = {}
+            for k, nm in enumerate(("u", "v", "w", "theta")):
+                a, b = smx.get(F_UNK + k), s64.get(F_UNK + k)
+                err[nm] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+            a, b = smx.get(F_PRPOT), s64.get(F_PRPOT)
+            a, b = a - a.mean(), b - b.mean()          # pi' up to the constant of the periodic solve
+            err["pi"] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+            row = {"step": step, "rel_l2_mixed_vs_fp64": err,
+                   "gcr_iters_fp64": [d64.niter1, d64.niter], "gcr_iters_mixed": [dmx.niter1, dmx.niter],
+                   "divmx_fp64": d64.divmx, "divmx_mixed": dmx.divmx}
+            if m0 is not None:
+                row.update({"scalar_min_fp64": d64.smin[0], "scalar_max_fp64": d64.smax[0],
+                            "scalar_mass_rel_change_fp64": (d64.mass[4] - m0) / m0,
+                            "scalar_min_mixed": dmx.smin[0], "scalar_mass_rel_change_mixed": (dmx.mass[4] - m0) / m0})
+            rows.append(row)
+            print(json.dumps(row), file=sys.stderr, flush=True)
+    for s in runs.values():
+        s.close()
+    print(json.dumps({"report": "mixed_vs_fp64", "config": workload_config(name), "rows": rows}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -445,11 +491,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-variants", action="store_true", help="skip the mixed-precision variant")
+    ap.add_argument("--error-steps", default="",
+                    help="report mode: mixed vs FP64 errors at these steps (e.g. 1,50,200) instead of timing")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.error_steps:
+        report_mixed_errors(args)
         return
 
     import torch
@@ -503,7 +554,10 @@ def main():
     ms = e0.elapsed_time(e1)
     kt = s.kernel_times()
     s.kernel_timing(False)
-    ref_fields = {k: s.get(F_UNK + k) for k in range(4)} if not args.no_variants else None
+    ref_fields = None
+    if not args.no_variants:
+        ref_fields = {k: s.get(F_UNK + k) for k in range(4)}
+        ref_fields["pi"] = s.get(F_PRPOT) - s.get(F_PRPOT).mean()
     rates = [d.rate1 for d in diags if d.rate1 > 0]
     plain_rate = float(np.exp(np.mean(np.log(rates)))) if rates else 0.0
     ms_max = max_over_ranks(ms)
@@ -635,6 +689,8 @@ def main():
             for k, nm in enumerate(("u", "v", "w", "theta")):
                 a, b = sv.get(F_UNK + k), ref_fields[k]
                 err[nm] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+            a = sv.get(F_PRPOT)
+            err["pi"] = float(np.linalg.norm(a - a.mean() - ref_fields["pi"]) / max(np.linalg.norm(ref_fields["pi"]), 1e-300))
             variants[vname] = {
                 "value": whole_job_rate(world, args.steps, vms / 1000.0), "unit": "steps/s",
                 "ms_per_step": vms / args.steps,
@@ -689,6 +745,9 @@ def main():
                     for k, nm in enumerate(("u", "v", "w", "theta")):
                         a, b = sv.get(F_UNK + k), ref_fields[k]
                         err[nm] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+                    a = sv.get(F_PRPOT)
+                    err["pi"] = float(np.linalg.norm(a - a.mean() - ref_fields["pi"]) /
+                                      max(np.linalg.norm(ref_fields["pi"]), 1e-300))
                     vval = whole_job_rate(world, args.steps, vms / 1000.0)
                     variants[vname] = {
                         "value": vval, "unit": "steps/s", "ms_per_step": vms / args.steps,
