@@ -53,6 +53,8 @@ module mpgcr_f
      integer(c_int) :: itmn
      real(c_double) :: nn_rate
      integer(c_int) :: itraj
+     integer(c_int) :: itrp_c1, itrp_c2, itrp_cc
+     integer(c_int) :: mg_bugs
   end type mpg_params
 
   ! the COMMON arrays of /n/ /xyz/ /volume/ /edg/ /wge/ /bound/ /bpoints/ /terms/ /coin/ /per2/
@@ -138,6 +140,13 @@ module mpgcr_f
        import :: c_int, c_ptr, mpg_info
        type(c_ptr), value :: h
        type(mpg_info), intent(out) :: info
+     end function
+     integer(c_int) function mpg_set_coarse(h, level, mesh, match) bind(C, name="mpg_set_coarse")
+       import :: c_int, c_ptr, mpg_mesh_ref
+       type(c_ptr), value :: h
+       integer(c_int), value :: level
+       type(mpg_mesh_ref), intent(in) :: mesh
+       type(c_ptr), value :: match
      end function
      integer(c_int) function mpg_set_field(h, fid, src) bind(C, name="mpg_set_field")
        import :: c_int, c_ptr, c_double

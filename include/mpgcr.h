@@ -86,6 +86,18 @@ typedef struct mpg_params {
     int32_t itraj;               /* 1: velprd trajectory prediction of the advective velocity
                                   * (ref.f:4448-4528) in set-up and every step; the reference
                                   * hard-codes 0 (ref.f:111)                                       */
+    /* input_mg_v3.d, the multigrid V-cycle of precon (mg_flag = 1, ref.f:618-748): sweeps on the
+     * coarse mesh before and after the coarsest one, and on the coarsest mesh (/vcycle/) */
+    int32_t itrp_c1, itrp_c2, itrp_cc;
+    int32_t mg_bugs;             /* mg_flag = 1: 1 reproduces the reference's indexing, 0 corrects
+                                  * it.  The reference's restriction_unstr and prolongation_unstr
+                                  * take the neighbour loop counter as the neighbour's node number
+                                  * (ref.f:813-817, 911-915), laplc_c/laplc_cc read coefw at the
+                                  * coarse node's number (ref.f:1390-1392, 1482-1484), and the
+                                  * prolongation's refill pass first overwrites its own marks, so
+                                  * nodes with no coarse neighbour stay zero (ref.f:929-941).
+                                  * Corrected: neigh_list, coefw of the matched fine node, and
+                                  * refill passes until every node has a value.                    */
 } mpg_params;
 
 #define MPG_PREC_FP64  0
@@ -189,6 +201,16 @@ int mpg_analyze_wide(const mpg_params *prm, const mpg_mesh_ref *mesh, int impfl,
                      double *minv, double *cp);
 const char *mpg_last_error(void);
 int mpg_get_info(mpg_handle h, mpg_info *info);
+
+/* mg_flag = 1: attach the coarse (level 1) or coarsest (level 2) mesh of precon's V-cycle
+ * (ref.f:618-748), the meshes the reference reads from mesh3d_c.d and mesh3d_cc.d (ref.f:2343-2641),
+ * before mpg_setup.  `match` gives each node of the level its node in the next finer mesh, 1-based
+ * as in match1.d / match2.d (ref.f:2653-2672), or NULL to find it by coordinates within 1 m as
+ * `matching` does (ref.f:2684-2720).  laplc_c / laplc_cc (ref.f:1356-1533) run as laplc on the
+ * level's mesh; restriction_unstr / prolongation_unstr (ref.f:757-951) move residuals and
+ * corrections; params.mg_bugs picks the reference's indexing or the corrected one (see
+ * mpg_params).  The V-cycle runs inside the reference smoother (iprc = 1), in FP64. */
+int mpg_set_coarse(mpg_handle h, int level, const mpg_mesh_ref *mesh, const int32_t *match);
 
 /* Field exchange in reference node order: `n` = npoin values, contiguous. */
 int mpg_set_field(mpg_handle h, int fid, const double *src);

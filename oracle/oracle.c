@@ -8,7 +8,8 @@
  * -O2 -ffp-contract=off (no FMA contraction, no fast-math).
  *
  * Reference options restated: isfera=0 only (the spherical variant is out of scope),
- * iper=0 (open boundaries, mpdatam) or 2 (periodic, mpdatamper), mg_flag=0, ielast=0,
+ * iper=0 (open boundaries, mpdatam) or 2 (periodic, mpdatamper), mg_flag=0 or 1 (precon's V-cycle
+ * on two coarser meshes attached with orc_set_coarse), ielast=0,
  * itraj=0 or 1 (velprd).  Extensions beyond the reference
  * are marked NEW: the vertical-line preconditioner (iprc=2), runtime lord/itmn, passive
  * scalars, the FP64 mass sums and the per-solve residual contraction.
@@ -51,6 +52,13 @@ struct orc {
     int *bst, *blst;    /* boundary points per node (CSR), built on demand */
     int blocked;        /* 1: global sums in the GPU's reduction order (see rsum) */
     int ref_bugs;       /* 1 (default): reproduce the corner-minimum slip of ref.f:3853-3866 */
+    /* multigrid (mg_flag = 1, ref.f:618-748): the coarse (0) and coarsest (1) meshes as oracles
+     * of their own (laplc_c/_cc, bcv_c/_cc and derivative_c/_cc are laplc, bcv and derivative on
+     * those meshes), match1/match2 (coarse node -> node of the next finer mesh, 0-based) and the
+     * neighbour lists of neigh_definition (ref.f:2726-2767) of the next finer mesh */
+    struct orc *lev[2];
+    int *match[2];
+    int *nbp[2], *nbl[2];
 };
 
 /* ------------------------------------------------------------------ helpers */
@@ -571,7 +579,205 @@ void orc_line_solve(orc *o, const double *rhs, double *zout, int impfl) {
     free(a); free(m); free(cp); free(d);
 }
 
-/* ------------------------------------------------------------------ precon ref.f:482-753 (mg_flag=0) */
+/* ------------------------------------------------------------------ multigrid levels (mg_flag = 1) */
+/* neigh_definition ref.f:2726-2767: for every internal edge, then every boundary face, each end
+ * gets the other as its next neighbour (CSR, same order) */
+static void neigh_definition(const orc *m, int **ptr_out, int **lst_out) {
+    int n = m->npoin, ne = m->nedge + m->nbface;
+    int *ptr = iz(n + 1), *lst = iz(2 * ne), *fill = iz(n);
+    for (int e = 0; e < ne; ++e) {
+        int in = e < m->nedge;
+        int i1 = in ? m->ie1[e] : m->kb1[e - m->nedge], i2 = in ? m->ie2[e] : m->kb2[e - m->nedge];
+        ptr[i1 + 1]++; ptr[i2 + 1]++;
+    }
+    for (int i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+    for (int e = 0; e < ne; ++e) {
+        int in = e < m->nedge;
+        int i1 = in ? m->ie1[e] : m->kb1[e - m->nedge], i2 = in ? m->ie2[e] : m->kb2[e - m->nedge];
+        lst[ptr[i1] + fill[i1]++] = i2;
+        lst[ptr[i2] + fill[i2]++] = i1;
+    }
+    free(fill);
+    *ptr_out = ptr; *lst_out = lst;
+}
+
+/* matching ref.f:2684-2720: for every fine point, the first coarse point within 1 m in x, y and z
+ * takes it as its match (so the last such fine point wins) */
+static void matching(const orc *fine, const orc *crs, int *match) {
+    const double tol = 1.;
+    for (int ic = 0; ic < crs->npoin; ++ic) match[ic] = -1;
+    for (int ip = 0; ip < fine->npoin; ++ip)
+        for (int ic = 0; ic < crs->npoin; ++ic)
+            if (fabs(fine->x[ip] - crs->x[ic]) < tol && fabs(fine->y[ip] - crs->y[ic]) < tol
+                && fabs(fine->z[ip] - crs->z[ic]) < tol) {
+                match[ic] = ip;
+                break;
+            }
+}
+
+int orc_set_coarse(orc *o, int level, const mpg_mesh_ref *mesh, const int *match) {
+    if (!o || level < 1 || level > 2 || !mesh || o->lev[level - 1]) return 1;
+    if (level == 2 && !o->lev[0]) return 1;
+    mpg_params P = o->P;
+    P.mg_flag = 0;
+    orc *c = orc_create(&P, mesh);
+    if (!c) return 1;
+    const orc *finer = level == 1 ? o : o->lev[0];
+    int *m = iz(c->npoin);
+    if (match) for (int i = 0; i < c->npoin; ++i) m[i] = match[i];
+    else matching(finer, c, m);
+    for (int i = 0; i < c->npoin; ++i)
+        if (m[i] < 0 || m[i] >= finer->npoin) { free(m); orc_destroy(c); return 1; }
+    o->lev[level - 1] = c;
+    o->match[level - 1] = m;
+    neigh_definition(finer, &o->nbp[level - 1], &o->nbl[level - 1]);
+    return 0;
+}
+
+/* restriction_unstr ref.f:757-824: coarse value = mean over the matched fine node's neighbours of
+ * (s(ip) + s(neighbour))/2.  The reference takes the loop counter inei as the neighbour's node
+ * number (ref.f:813-817); mg_bugs = 0 uses neigh_list. */
+static void restriction(const orc *o, const double *s, double *sc, int flg) {
+    const orc *crs = o->lev[flg - 1];
+    const int *m = o->match[flg - 1], *ptr = o->nbp[flg - 1], *lst = o->nbl[flg - 1];
+    for (int ic = 0; ic < crs->npoin; ++ic) sc[ic] = 0.;
+    for (int ic = 0; ic < crs->npoin; ++ic) {
+        int ip = m[ic], nn = ptr[ip + 1] - ptr[ip];
+        for (int inei = 1; inei <= nn; ++inei) {
+            int j = o->P.mg_bugs ? inei - 1 : lst[ptr[ip] + inei - 1];
+            sc[ic] = sc[ic] + (s[ip] + s[j]) / 2.;
+        }
+        sc[ic] = sc[ic] / (double)nn;
+    }
+}
+
+/* prolongation_unstr ref.f:828-951: matched fine nodes take the coarse value; every other fine
+ * node the mean of its neighbours that have one (marked by aux != -99999).  The reference again
+ * takes the loop counter as the neighbour's node number (ref.f:911-915), and its refill pass
+ * (ref.f:929-941) first overwrites every mark, so it adds nothing: nodes with no neighbour holding
+ * a value stay 0.  mg_bugs = 0 uses neigh_list and repeats the pass over the nodes still without a
+ * value, each pass reading the values set by the previous ones, until every node has one. */
+static void prolongation(const orc *o, const double *sc, double *s, int flg) {
+    const orc *crs = o->lev[flg - 1];
+    const orc *fine = flg == 1 ? o : o->lev[0];
+    const int *m = o->match[flg - 1], *ptr = o->nbp[flg - 1], *lst = o->nbl[flg - 1];
+    const double nan = -99999.;
+    int n = fine->npoin;
+    double *aux = dz(n);
+    int *newly = iz(n);
+    for (int ip = 0; ip < n; ++ip) { s[ip] = 0.; aux[ip] = nan; }
+    for (int ic = 0; ic < crs->npoin; ++ic) { s[m[ic]] = sc[ic]; aux[m[ic]] = sc[ic]; }
+    for (int pass = 0; pass < 1000; ++pass) {
+        int unfilled = 0;
+        for (int ipa = 0; ipa < n; ++ipa) {
+            if (aux[ipa] != nan) continue;
+            double filled = 0.;
+            int nn = ptr[ipa + 1] - ptr[ipa];
+            for (int ineigh = 1; ineigh <= nn; ++ineigh) {
+                int j = o->P.mg_bugs ? ineigh - 1 : lst[ptr[ipa] + ineigh - 1];
+                if (aux[j] != nan) {
+                    s[ipa] = s[ipa] + s[j];
+                    filled = filled + 1.;
+                }
+            }
+            if (filled != 0.) { s[ipa] = s[ipa] / filled; newly[ipa] = 1; }
+            else unfilled = 1;
+        }
+        if (o->P.mg_bugs || !unfilled) break;
+        for (int ip = 0; ip < n; ++ip) if (newly[ip]) { aux[ip] = s[ip]; newly[ip] = 0; }
+    }
+    free(aux); free(newly);
+}
+
+void orc_mg_restrict(orc *o, const double *s, double *sc, int flg) { restriction(o, s, sc, flg); }
+void orc_mg_prolong(orc *o, const double *sc, double *s, int flg) { prolongation(o, sc, s, flg); }
+int orc_level_npoin(const orc *o, int level) {
+    return level == 0 ? o->npoin : (o->lev[level - 1] ? o->lev[level - 1]->npoin : 0);
+}
+
+/* set-up data of the coarse levels (mpsolver, ref.f:161-168): beta_timestep_unstr(2/3) on the
+ * level's own mesh and compute_d_unstr(2/3) with the fine rh0 restricted to the level
+ * (ref.f:1177-1194).  laplc_c/_cc then read rh0 of the matched fine node (ref.f:1413-1420,
+ * 1505-1512). */
+static void compute_d(orc *o);
+static void beta_timestep(orc *o);
+static void mg_setup_levels(orc *o) {
+    if (!o->lev[0] || !o->lev[1]) return;
+    const double *rh0 = o->f[MPG_F_RH0];
+    orc *c1 = o->lev[0], *c2 = o->lev[1];
+    restriction(o, rh0, c1->f[MPG_F_RH0], 1);
+    restriction(o, c1->f[MPG_F_RH0], c2->f[MPG_F_RH0], 2);
+    beta_timestep(c1); beta_timestep(c2);
+    compute_d(c1); compute_d(c2);
+    for (int ic = 0; ic < c1->npoin; ++ic) c1->f[MPG_F_RH0][ic] = rh0[o->match[0][ic]];
+    for (int ic = 0; ic < c2->npoin; ++ic) c2->f[MPG_F_RH0][ic] = rh0[o->match[0][o->match[1][ic]]];
+}
+
+/* coefw as laplc_c/_cc read it: the fine array at the coarse node's own number (ref.f:1390-1392,
+ * 1482-1484), or (mg_bugs = 0) at its matched fine node */
+static void mg_coefw(orc *o) {
+    const double *cw = o->f[MPG_F_COEFW];
+    for (int l = 0; l < 2; ++l) {
+        orc *c = o->lev[l];
+        for (int ic = 0; ic < c->npoin; ++ic) {
+            int ip = l == 0 ? o->match[0][ic] : o->match[0][o->match[1][ic]];
+            c->f[MPG_F_COEFW][ic] = o->P.mg_bugs ? cw[ic] : cw[ip];
+        }
+    }
+}
+
+static void mg_pstep(const orc *lv, double *pstep) {
+    for (int ip = 0; ip < lv->npoin; ++ip) {
+        if (lv->P.sm_flag1 == 1) pstep[ip] = (-1.) / lv->d1[ip];
+        else if (lv->P.sm_flag1 == 2) pstep[ip] = lv->betaunstr1;
+        else if (lv->P.sm_flag1 == 3) pstep[ip] = lv->betaunstr1 / (1. - lv->d1[ip] * lv->betaunstr1);
+    }
+}
+
+/* the V-cycle of precon after the first fine smoothing, ref.f:618-748 */
+static void mg_vcycle(orc *o, const double *rhs, double *p, double *r, const double *pstep, int impfl) {
+    orc *c1 = o->lev[0], *c2 = o->lev[1];
+    int n = o->npoin, n1 = c1->npoin, n2 = c2->npoin;
+    const double om = o->P.omega;
+    mg_coefw(o);
+    double *p_c = dz(n1), *r_c = dz(n1), *e_c = dz(n1), *rrhs_c = dz(n1), *rrhs_c_out = dz(n1), *ps_c = dz(n1);
+    double *p_cc = dz(n2), *r_cc = dz(n2), *rrhs_cc = dz(n2), *ps_cc = dz(n2);
+    double *rrhs = dz(n), *e = dz(n);
+    mg_pstep(c1, ps_c);
+    mg_pstep(c2, ps_cc);
+    orc_laplc(o, p, r, impfl);                                 /* ref.f:660-664 */
+    for (int ip = 0; ip < n; ++ip) rrhs[ip] = rhs[ip] - r[ip];
+    restriction(o, rrhs, rrhs_c, 1);
+    for (int ic = 0; ic < n1; ++ic) p_c[ic] = -(om * ps_c[ic] * rrhs_c[ic]);     /* ref.f:675-677 */
+    for (int it = 1; it <= o->P.itrp_c1; ++it) {
+        orc_laplc(c1, p_c, r_c, impfl);
+        for (int ic = 0; ic < n1; ++ic) p_c[ic] = p_c[ic] + om * ps_c[ic] * (r_c[ic] - rrhs_c[ic]);
+    }
+    orc_laplc(c1, p_c, r_c, impfl);                            /* ref.f:688-691 */
+    for (int ic = 0; ic < n1; ++ic) rrhs_c_out[ic] = rrhs_c[ic] - r_c[ic];
+    restriction(o, rrhs_c_out, rrhs_cc, 2);
+    for (int ic = 0; ic < n2; ++ic) p_cc[ic] = -(rrhs_cc[ic] * ps_cc[ic] * om);  /* ref.f:702-704 */
+    for (int it = 1; it <= o->P.itrp_cc; ++it) {
+        orc_laplc(c2, p_cc, r_cc, impfl);
+        for (int ic = 0; ic < n2; ++ic) p_cc[ic] = p_cc[ic] + om * ps_cc[ic] * (r_cc[ic] - rrhs_cc[ic]);
+    }
+    prolongation(o, p_cc, e_c, 2);                             /* ref.f:718-722 */
+    for (int ic = 0; ic < n1; ++ic) p_c[ic] = p_c[ic] + e_c[ic];
+    for (int it = 1; it <= o->P.itrp_c2; ++it) {
+        orc_laplc(c1, p_c, r_c, impfl);
+        for (int ic = 0; ic < n1; ++ic) p_c[ic] = p_c[ic] + om * ps_c[ic] * (r_c[ic] - rrhs_c[ic]);
+    }
+    prolongation(o, p_c, e, 1);                                /* ref.f:734-738 */
+    for (int ip = 0; ip < n; ++ip) p[ip] = p[ip] + e[ip];
+    for (int it = 1; it <= o->P.itrp2; ++it) {                 /* ref.f:742-747 */
+        orc_laplc(o, p, r, impfl);
+        for (int ip = 0; ip < n; ++ip) p[ip] = p[ip] + om * pstep[ip] * (r[ip] - rhs[ip]);
+    }
+    free(p_c); free(r_c); free(e_c); free(rrhs_c); free(rrhs_c_out); free(ps_c);
+    free(p_cc); free(r_cc); free(rrhs_cc); free(ps_cc); free(rrhs); free(e);
+}
+
+/* ------------------------------------------------------------------ precon ref.f:482-753 */
 void orc_precon(orc *o, const double *rhs, double *p, double *r, int iprc, int impfl) {
     int n = o->npoin;
     if (iprc == 0) {                                           /* ref.f:543-548 */
@@ -606,6 +812,7 @@ void orc_precon(orc *o, const double *rhs, double *p, double *r, int iprc, int i
         for (int ip = 0; ip < n; ++ip)
             p[ip] = p[ip] + o->P.omega * pstep[ip] * (r[ip] - rhs[ip]);
     }
+    if (o->P.mg_flag == 1 && o->lev[0] && o->lev[1]) mg_vcycle(o, rhs, p, r, pstep, impfl);
     free(pstep);
 }
 
@@ -1191,6 +1398,7 @@ void orc_setup(orc *o, mpg_diag *diag) {
     for (int ip = 0; ip < n; ++ip) o->timestp[ip] = P->delt;  /* input, ref.f:2507-2509 */
     beta_timestep(o);
     compute_d(o);
+    mg_setup_levels(o);                                        /* ref.f:161-168, levels 2 and 3 */
     for (int ip = 0; ip < n; ++ip) {                           /* ref.f:177-207 */
         o->ue[ip] = P->u0inf;
         o->ve[ip] = P->v0inf;
@@ -1346,7 +1554,7 @@ void orc_step(orc *o, mpg_diag *diag) {
 
 /* ------------------------------------------------------------------ construction */
 orc *orc_create(const mpg_params *prm, const mpg_mesh_ref *m) {
-    if (!prm || !m || prm->isfera != 0 || prm->mg_flag != 0 || prm->nscal < 0
+    if (!prm || !m || prm->isfera != 0 || (prm->mg_flag != 0 && prm->mg_flag != 1) || prm->nscal < 0
         || 4 + prm->nscal > MAXUNK || prm->lord < 1)
         return NULL;
     orc *o = (orc *)calloc(1, sizeof(orc));
@@ -1424,5 +1632,9 @@ void orc_destroy(orc *o) {
                     o->bst, o->blst};
     for (size_t i = 0; i < sizeof ptrs / sizeof ptrs[0]; ++i) free(ptrs[i]);
     for (int k = 0; k < MPG_F_COUNT; ++k) free(o->f[k]);
+    for (int l = 0; l < 2; ++l) {
+        if (o->lev[l]) orc_destroy(o->lev[l]);
+        free(o->match[l]); free(o->nbp[l]); free(o->nbl[l]);
+    }
     free(o);
 }

@@ -40,6 +40,17 @@ void   orc_set_ref_bugs(orc *o, int on);
 void   orc_wide_entries(orc *o, int impfl, double *lo, double *dg, double *hi);
 void   orc_wide_factors(orc *o, int impfl, double *lo, double *m, double *cp);
 void   orc_wide_solve(orc *o, const double *rhs, double *zout, int impfl);
+/* mg_flag = 1: attach the coarse (level 1, mesh3d_c.d) or coarsest (level 2, mesh3d_cc.d) mesh of
+ * precon's V-cycle (ref.f:618-748) before orc_setup, with its match array (coarse node -> node of
+ * the next finer mesh, 0-based) or NULL to find it by coordinates as `matching` does
+ * (ref.f:2684-2720).  params.mg_bugs selects the reference's indexing or the corrected one.
+ * Returns 0, or 1 for an argument the levels cannot use. */
+int    orc_set_coarse(orc *o, int level, const mpg_mesh_ref *mesh, const int *match);
+/* the V-cycle's transfers on their own: restriction_unstr / prolongation_unstr (ref.f:757-951)
+ * between level flg-1 and level flg (0 = the fine mesh), and the node count of a level */
+void   orc_mg_restrict(orc *o, const double *s, double *sc, int flg);
+void   orc_mg_prolong(orc *o, const double *sc, double *s, int flg);
+int    orc_level_npoin(const orc *o, int level);
 /* pointer to a field (same ids as the product) — n = npoin doubles */
 double *orc_field(orc *o, int fid);
 int    orc_npoin(const orc *o);

@@ -60,6 +60,11 @@ def lib():
         L.orc_wide_entries.argtypes = [vp, ip, dp, dp, dp]
         L.orc_wide_solve.argtypes = [vp, dp, dp, ip]
         L.orc_wide_factors.argtypes = [vp, ip, dp, dp, dp]
+        L.orc_set_coarse.argtypes = [vp, ip, vp, C.POINTER(C.c_int)]
+        L.orc_mg_restrict.argtypes = [vp, dp, dp, ip]
+        L.orc_mg_prolong.argtypes = [vp, dp, dp, ip]
+        L.orc_level_npoin.restype = ip
+        L.orc_level_npoin.argtypes = [vp, ip]
         _lib = L
     return _lib
 
@@ -91,6 +96,28 @@ class Oracle:
         if h:
             self.L.orc_destroy(h)
             self.h = None
+
+    def set_coarse(self, level: int, refmesh, match=None) -> None:
+        """Attach the coarse (1) or coarsest (2) mesh of the V-cycle (mg_flag = 1), with its match
+        array (coarse node -> node of the next finer mesh, 0-based) or None to match by
+        coordinates as the reference does."""
+        mm = MeshMarshal(refmesh)
+        m = None
+        if match is not None:
+            keep = np.ascontiguousarray(match, np.int32)
+            m = keep.ctypes.data_as(C.POINTER(C.c_int))
+        if self.L.orc_set_coarse(self.h, level, C.byref(mm.c), m) != 0:
+            raise ValueError("oracle rejected the coarse level")
+
+    def mg_restrict(self, s, flg):
+        out = np.zeros(self.L.orc_level_npoin(self.h, flg))
+        self.L.orc_mg_restrict(self.h, _p(np.ascontiguousarray(s, np.float64)), _p(out), flg)
+        return out
+
+    def mg_prolong(self, sc, flg):
+        out = np.zeros(self.L.orc_level_npoin(self.h, flg - 1))
+        self.L.orc_mg_prolong(self.h, _p(np.ascontiguousarray(sc, np.float64)), _p(out), flg)
+        return out
 
     # ---- fields
     def field(self, fid: int) -> np.ndarray:

@@ -32,7 +32,7 @@ EXPORTS = [
     "mpg_laplc_noalloc", "mpg_learned_init", "mpg_learned_set_params", "mpg_learned_get_params",
     "mpg_learned_forward", "mpg_learned_grad", "mpg_learned_train_pair", "mpg_learned_harvest",
     "mpg_learned_train_records", "mpg_learned_loss", "mpg_laplc_adjoint", "mpg_restart_write",
-    "mpg_restart_read", "mpg_velprd", "mpg_selftest_wait", "mpg_write_output",
+    "mpg_restart_read", "mpg_velprd", "mpg_selftest_wait", "mpg_write_output", "mpg_set_coarse",
 ]
 NPARAM = 9505
 
@@ -94,6 +94,7 @@ def lib():
         L.mpg_learned_loss.argtypes = [vp, ip]
         L.mpg_restart_write.argtypes = [vp, C.c_char_p, ip, ip]
         L.mpg_velprd.argtypes = [vp]
+        L.mpg_set_coarse.argtypes = [vp, ip, vp, vp]
         L.mpg_write_output.argtypes = [vp, C.c_char_p, vp, ip]
         L.mpg_selftest_wait.argtypes = [vp, ip, ip, C.POINTER(C.c_int)]
         L.mpg_restart_read.argtypes = [vp, C.c_char_p, ip, C.POINTER(C.c_int)]
@@ -162,6 +163,16 @@ class Solver:
 
     def __exit__(self, *a):
         self.close()
+
+    def set_coarse(self, level: int, refmesh, match=None) -> None:
+        """mg_flag = 1: attach the coarse (1) or coarsest (2) mesh of precon's V-cycle, with its
+        match array (0-based: coarse node -> node of the next finer mesh) or None to match by
+        coordinates as the reference does."""
+        mm = MeshMarshal(refmesh)
+        m = None
+        if match is not None:
+            m = np.ascontiguousarray(np.asarray(match) + 1, np.int32)
+        _check(self.L.mpg_set_coarse(self.h, level, C.byref(mm.c), m.ctypes.data if m is not None else None))
 
     # ---------------------------------------------------------------- fields
     def set(self, fid: int, values) -> None:

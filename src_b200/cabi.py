@@ -32,6 +32,7 @@ class MpgParams(C.Structure):
         ("strat", C.c_double), ("tetbar", C.c_double), ("g", C.c_double),
         ("iprc", C.c_int32), ("nscal", C.c_int32), ("precision", C.c_int32), ("itmn", C.c_int32),
         ("nn_rate", C.c_double), ("itraj", C.c_int32),
+        ("itrp_c1", C.c_int32), ("itrp_c2", C.c_int32), ("itrp_cc", C.c_int32), ("mg_bugs", C.c_int32),
     ]
 
 
@@ -150,6 +151,10 @@ class RunParams:
     itmn: int = 3
     nn_rate: float = 0.0
     itraj: int = 0
+    itrp_c1: int = 1
+    itrp_c2: int = 1
+    itrp_cc: int = 2
+    mg_bugs: int = 1
 
     def to_c(self) -> MpgParams:
         p = MpgParams()
@@ -188,7 +193,7 @@ class RunParams:
             f.write(f"{self.omega}\n")
             f.write("sweeps\n")
             f.write("itrp1 itrp2 itrp_c1 itrp_c2 itrp_cc\n")
-            f.write(f"{self.itrp1} {self.itrp2} 0 0 0\n")
+            f.write(f"{self.itrp1} {self.itrp2} {self.itrp_c1} {self.itrp_c2} {self.itrp_cc}\n")
             f.write("match_flag\n")
             f.write("1\n")
         with open(os.path.join(directory, "inputre.d"), "w") as f:

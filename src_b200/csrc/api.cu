@@ -11,6 +11,10 @@
 #include "kernels.cuh"
 #include "learned.cuh"
 #include "mpdata.cuh"
+#include "mg.cuh"
+
+#include <algorithm>
+#include <unordered_map>
 #include "mpgcr_internal.h"
 
 using namespace mpgk;
@@ -84,6 +88,25 @@ struct mpg_solver {
     HostStatic hs;
     std::vector<int32_t> iperm;
     KTimer kt;
+    // multigrid V-cycle (mg_flag = 1): the transfer data to the coarse (0) and coarsest (1) mesh,
+    // whose own handles run laplc_c / laplc_cc on this handle's stream
+    struct MgLevel {
+        mpg_solver *sub = nullptr;
+        int32_t *match = nullptr;                            // coarse node -> finer node (internal)
+        int32_t *nbp = nullptr, *nbl = nullptr, *bugnb = nullptr;   // finer mesh's neighbour lists
+        int passes = 1;                                      // prolongation filling passes
+        double *aux = nullptr;                               // finer-mesh scratch of the prolongation
+        uint8_t *flag = nullptr;
+        double *p = nullptr, *r = nullptr, *e = nullptr, *rrhs = nullptr, *rrhs_out = nullptr;  // coarse arrays
+        std::vector<int32_t> match_ref;                      // coarse ref node -> finer ref node
+        std::vector<double> rh0_restricted;                  // finest rh0 restricted here (ref order)
+    } mg[2];
+    double *mg_rrhs = nullptr, *mg_e = nullptr;          // fine-mesh arrays of the V-cycle
+    bool borrowed_stream = false;                        // a coarse level runs on its parent's stream
+    // kept for the V-cycle's set-up when mg_flag = 1 (and on a coarse level's handle): the mesh's
+    // neighbour lists in neigh_definition order and its coordinates, reference numbering
+    std::vector<int32_t> nb_ptr_ref, nb_lst_ref;
+    std::vector<double> cx_ref, cy_ref, cz_ref;
     struct NN {
         bool geom = false, infer = false, train = false, have_params = false;
         float *prm = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
@@ -314,7 +337,203 @@ int op_wide(mpg_handle h, const double *rhs, TO *p, int impfl, int acc) {
     return check_launch("wide line solve");
 }
 
-// precon(rhs, p, r, iprc, elas, impfl), mg_flag = 0 (ref.f:482-753); `zero_r` restores the
+// ------------------------------------------------------------------------------ multigrid (host side)
+// neigh_definition (ref.f:2726-2767) in reference numbering: for every internal edge, then every
+// boundary face, each end gets the other as its next neighbour (CSR)
+void mg_neigh_definition(const mpg_mesh_ref *m, std::vector<int32_t> &ptr, std::vector<int32_t> &lst) {
+    const int n = m->npoin;
+    const int64_t ne = (int64_t)m->nedge + m->nbface;
+    auto ends = [&](int64_t e, int &i1, int &i2) {
+        if (e < m->nedge) { i1 = m->iedge[e] - 1; i2 = m->iedge[(size_t)m->nedgex + e] - 1; }
+        else { const int64_t b = e - m->nedge; i1 = m->kbface[b] - 1; i2 = m->kbface[(size_t)m->nfacesx + b] - 1; }
+    };
+    ptr.assign(n + 1, 0);
+    for (int64_t e = 0; e < ne; ++e) { int a, b; ends(e, a, b); ptr[a + 1]++; ptr[b + 1]++; }
+    for (int i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+    lst.assign(ptr[n], 0);
+    std::vector<int32_t> fill(n, 0);
+    for (int64_t e = 0; e < ne; ++e) {
+        int a, b; ends(e, a, b);
+        lst[ptr[a] + fill[a]++] = b;
+        lst[ptr[b] + fill[b]++] = a;
+    }
+}
+
+void mg_coords(const mpg_mesh_ref *m, std::vector<double> &x, std::vector<double> &y, std::vector<double> &z) {
+    const int n = m->npoin;
+    x.assign(m->coord, m->coord + n);
+    y.assign(m->coord + m->npoinx, m->coord + m->npoinx + n);
+    z.assign(m->coord + 2 * (size_t)m->npoinx, m->coord + 2 * (size_t)m->npoinx + n);
+}
+
+// matching (ref.f:2684-2720): for every fine point in order, the first coarse point within 1 m in
+// x, y and z takes it as its match (so the last such fine point wins); -1 where none
+std::vector<int32_t> mg_matching(const std::vector<double> &fx, const std::vector<double> &fy,
+                                 const std::vector<double> &fz, const std::vector<double> &cx,
+                                 const std::vector<double> &cy, const std::vector<double> &cz) {
+    const double tol = 1.;
+    auto key = [](double x, double y, double z) {
+        const int64_t K = 1 << 21;
+        return (((int64_t)std::floor(x) + K / 2) * K + ((int64_t)std::floor(y) + K / 2)) * K +
+               ((int64_t)std::floor(z) + K / 2);
+    };
+    std::unordered_map<int64_t, std::vector<int32_t>> bins;
+    for (size_t ic = 0; ic < cx.size(); ++ic) bins[key(cx[ic], cy[ic], cz[ic])].push_back((int32_t)ic);
+    std::vector<int32_t> match(cx.size(), -1);
+    for (size_t ip = 0; ip < fx.size(); ++ip) {
+        int32_t best = -1;
+        for (int dx = -1; dx <= 1; ++dx)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dz = -1; dz <= 1; ++dz) {
+                    auto it = bins.find(key(fx[ip] + dx, fy[ip] + dy, fz[ip] + dz));
+                    if (it == bins.end()) continue;
+                    for (int32_t ic : it->second)
+                        if (std::fabs(fx[ip] - cx[ic]) < tol && std::fabs(fy[ip] - cy[ic]) < tol &&
+                            std::fabs(fz[ip] - cz[ic]) < tol && (best < 0 || ic < best))
+                            best = ic;
+                }
+        if (best >= 0) match[best] = (int32_t)ip;
+    }
+    return match;
+}
+
+// restriction_unstr (ref.f:757-824) on the host, reference numbering
+std::vector<double> mg_restrict_host(const std::vector<double> &s, const std::vector<int32_t> &match,
+                                     const std::vector<int32_t> &ptr, const std::vector<int32_t> &lst, int bugs) {
+    std::vector<double> sc(match.size(), 0.);
+    for (size_t ic = 0; ic < match.size(); ++ic) {
+        const int ip = match[ic], nn = ptr[ip + 1] - ptr[ip];
+        for (int k = 0; k < nn; ++k) {
+            const int j = bugs ? k : lst[ptr[ip] + k];
+            sc[ic] = sc[ic] + (s[ip] + s[j]) / 2.;
+        }
+        sc[ic] = sc[ic] / (double)nn;
+    }
+    return sc;
+}
+
+// compute_d_unstr(2/3) (ref.f:1112-1284) on a coarser mesh with the restricted rh0, reference
+// numbering
+std::vector<double> mg_compute_d(const mpg_mesh_ref *m, const std::vector<double> &rh0u, double dt) {
+    const int n = m->npoin;
+    std::vector<double> dix(n, 0.), diy(n, 0.), diz(n, 0.), d(n, 0.);
+    const int64_t ne = (int64_t)m->nedge + m->nbface;
+    for (int64_t e = 0; e < ne; ++e) {
+        int i1, i2;
+        double sx, sy, sz;
+        if (e < m->nedge) {
+            i1 = m->iedge[e] - 1; i2 = m->iedge[(size_t)m->nedgex + e] - 1;
+            sx = m->sn[e]; sy = m->sn[(size_t)m->nedgex + e]; sz = m->sn[2 * (size_t)m->nedgex + e];
+        } else {
+            const int64_t b = e - m->nedge;
+            i1 = m->kbface[b] - 1; i2 = m->kbface[(size_t)m->nfacesx + b] - 1;
+            sx = m->sb[b]; sy = m->sb[(size_t)m->nfacesx + b]; sz = m->sb[2 * (size_t)m->nfacesx + b];
+        }
+        const double v1 = m->vol[i1], v2 = m->vol[i2];
+        dix[i1] = dix[i1] + sx * sx * rh0u[i2] / v2;
+        dix[i2] = dix[i2] + sx * sx * rh0u[i1] / v1;
+        diy[i1] = diy[i1] + sy * sy * rh0u[i2] / v2;
+        diy[i2] = diy[i2] + sy * sy * rh0u[i1] / v1;
+        diz[i1] = diz[i1] + sz * sz * rh0u[i2] / v2;
+        diz[i2] = diz[i2] + sz * sz * rh0u[i1] / v1;
+    }
+    for (int i = 0; i < n; ++i) d[i] = -0.5 * dt * (dix[i] + diy[i] + diz[i]) / (4 * m->vol[i] * rh0u[i]);
+    return d;
+}
+
+// filling passes prolongation_unstr needs until every finer node has a value (the corrected
+// variant; the reference makes one); -1 if some node can never get one
+int mg_fill_passes(int nfine, const std::vector<int32_t> &match, const std::vector<int32_t> &ptr,
+                   const std::vector<int32_t> &lst) {
+    std::vector<uint8_t> set(nfine, 0), nw(nfine, 0);
+    for (int32_t ip : match) set[ip] = 1;
+    for (int pass = 1; pass <= 1000; ++pass) {
+        bool unset = false, progress = false;
+        for (int i = 0; i < nfine; ++i) {
+            if (set[i]) continue;
+            bool any = false;
+            for (int k = ptr[i]; k < ptr[i + 1] && !any; ++k) any = set[lst[k]] != 0;
+            if (any) { nw[i] = 1; progress = true; } else unset = true;
+        }
+        if (!unset) return pass;
+        if (!progress) return -1;
+        for (int i = 0; i < nfine; ++i) if (nw[i]) { set[i] = 1; nw[i] = 0; }
+    }
+    return -1;
+}
+
+// the finer mesh's field s restricted to level lv's mesh
+int mg_restrict(mpg_handle h, mpg_solver::MgLevel &lv, const double *s, double *sc) {
+    {
+        KTIME(KT_MISC);
+        k_mg_restrict<<<grid(lv.sub->N), kThreads, 0, h->st>>>(lv.sub->N, lv.match, lv.nbp, lv.nbl, lv.bugnb,
+                                                                h->P.mg_bugs, s, sc);
+    }
+    return check_launch("mg restriction");
+}
+
+// level lv's field sc prolongated to the finer mesh of nfine nodes
+int mg_prolong(mpg_handle h, mpg_solver::MgLevel &lv, int nfine, const double *sc, double *s) {
+    {
+        KTIME(KT_MISC);
+        k_mg_prolong_init<<<grid(nfine), kThreads, 0, h->st>>>(nfine, s, lv.aux, lv.flag);
+        k_mg_inject<<<grid(lv.sub->N), kThreads, 0, h->st>>>(lv.sub->N, lv.match, sc, s, lv.aux);
+        for (int pass = 0; pass < lv.passes; ++pass) {
+            k_mg_fill<<<grid(nfine), kThreads, 0, h->st>>>(nfine, lv.nbp, lv.nbl, lv.bugnb, h->P.mg_bugs, lv.aux,
+                                                           s, lv.flag);
+            k_mg_commit<<<grid(nfine), kThreads, 0, h->st>>>(nfine, s, lv.aux, lv.flag);
+        }
+    }
+    return check_launch("mg prolongation");
+}
+
+int mg_relax(mpg_handle a, double *p, double *r, const double *rhs, int sweeps, int impfl);
+
+// the V-cycle of precon after the first fine smoothing (ref.f:618-748)
+int mg_vcycle(mpg_handle h, const double *rhs, double *p, double *r, int impfl) {
+    auto &L1 = h->mg[0], &L2 = h->mg[1];
+    mpg_solver *c1 = L1.sub, *c2 = L2.sub;
+    const int N = h->N, N1 = c1->N, N2 = c2->N;
+    const double om = h->P.omega;
+    const int sm = h->P.sm_flag1;
+    int rc;
+    if ((rc = op_laplc(h, p, r, impfl))) return rc;                            // ref.f:660-664
+    {
+        KTIME(KT_MISC);
+        k_sub<<<grid(N), kThreads, 0, h->st>>>(N, rhs, r, h->mg_rrhs);
+    }
+    if ((rc = mg_restrict(h, L1, h->mg_rrhs, L1.rrhs))) return rc;
+    {
+        KTIME(KT_MISC);                                                       // ref.f:675-677
+        k_mg_first<<<grid(N1), kThreads, 0, h->st>>>(N1, 0, sm, om, c1->betaunstr1, c1->f[MPG_F_D1], L1.rrhs, L1.p);
+    }
+    if ((rc = mg_relax(c1, L1.p, L1.r, L1.rrhs, h->P.itrp_c1, impfl))) return rc;
+    if ((rc = op_laplc(c1, L1.p, L1.r, impfl))) return rc;                   // ref.f:688-691
+    {
+        KTIME(KT_MISC);
+        k_sub<<<grid(N1), kThreads, 0, h->st>>>(N1, L1.rrhs, L1.r, L1.rrhs_out);
+    }
+    if ((rc = mg_restrict(h, L2, L1.rrhs_out, L2.rrhs))) return rc;
+    {
+        KTIME(KT_MISC);                                                       // ref.f:702-704
+        k_mg_first<<<grid(N2), kThreads, 0, h->st>>>(N2, 1, sm, om, c2->betaunstr1, c2->f[MPG_F_D1], L2.rrhs, L2.p);
+    }
+    if ((rc = mg_relax(c2, L2.p, L2.r, L2.rrhs, h->P.itrp_cc, impfl))) return rc;
+    if ((rc = mg_prolong(h, L2, N1, L2.p, L1.e))) return rc;                  // ref.f:718-722
+    {
+        KTIME(KT_MISC);
+        k_add<<<grid(N1), kThreads, 0, h->st>>>(N1, L1.e, L1.p);
+    }
+    if ((rc = mg_relax(c1, L1.p, L1.r, L1.rrhs, h->P.itrp_c2, impfl))) return rc;
+    if ((rc = mg_prolong(h, L1, N, L1.p, h->mg_e))) return rc;                // ref.f:734-738
+    {
+        KTIME(KT_MISC);
+        k_add<<<grid(N), kThreads, 0, h->st>>>(N, h->mg_e, p);
+    }
+    return mg_relax(h, p, r, rhs, h->P.itrp2, impfl);                          // ref.f:742-747
+}
+
+// precon(rhs, p, r, iprc, elas, impfl) (ref.f:482-753); `zero_r` restores the
 // reference's clearing of r when a caller may look at it.
 int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, int impfl, bool zero_r) {
     const int N = h->N;
@@ -394,7 +613,28 @@ int op_precon(mpg_handle h, const double *rhs, double *p, double *r, int iprc, i
                                                       h->f[MPG_F_D1], r, rhs, p);
         }
     }
+    if (h->P.mg_flag == 1) {
+        if (!h->mg[0].sub || !h->mg[1].sub)
+            return mpg_fail(MPG_ERR_ARG, "mg_flag=1 needs both coarser meshes (mpg_set_coarse levels 1 and 2)");
+        int rc = mg_vcycle(h, rhs, p, r, impfl);
+        if (rc) return rc;
+    }
     return check_launch("precon smoother");
+}
+
+// itrp relaxation sweeps p += omega*pstep*(laplc(p) - rhs) on mesh handle `a` (its d1 and beta)
+int mg_relax(mpg_handle a, double *p, double *r, const double *rhs, int sweeps, int impfl) {
+    for (int it = 1; it <= sweeps; ++it) {
+        int rc = op_laplc(a, p, r, impfl);
+        if (rc) return rc;
+        {
+            mpg_handle h = a;
+            KTIME(KT_MISC);
+            k_smooth<<<grid(a->N), kThreads, 0, a->st>>>(a->N, a->P.sm_flag1, a->P.omega, a->betaunstr1,
+                                                         a->f[MPG_F_D1], r, rhs, p);
+        }
+    }
+    return check_launch("mg relaxation");
 }
 
 // the preconditioner inside gcrk, writing its result in the direction type T
@@ -1354,7 +1594,9 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     *out = nullptr;
     if (prm->isfera != 0) return mpg_fail(MPG_ERR_UNSUPPORTED, "isfera=1 (spherical variant) is not provided");
     if (prm->iper != 2 && prm->iper != 0) return mpg_fail(MPG_ERR_ARG, "iper must be 0 or 2");
-    if (prm->mg_flag != 0) return mpg_fail(MPG_ERR_UNSUPPORTED, "mg_flag=1 (multigrid V-cycle) is not provided");
+    if (prm->mg_flag != 0 && prm->mg_flag != 1) return mpg_fail(MPG_ERR_ARG, "mg_flag must be 0 or 1");
+    if (prm->mg_flag == 1 && (prm->iprc != 1 || prm->precision != MPG_PREC_FP64))
+        return mpg_fail(MPG_ERR_UNSUPPORTED, "mg_flag=1 runs inside the reference smoother: iprc = 1, FP64");
     if (prm->ielast != 0) return mpg_fail(MPG_ERR_UNSUPPORTED, "ielast=1 is not provided");
     if (prm->lord < 1 || prm->lord > MPG_MAX_LORD) return mpg_fail(MPG_ERR_ARG, "lord out of range 1..16");
     if (prm->nscal < 0 || 4 + prm->nscal > MPG_MAX_UNK) return mpg_fail(MPG_ERR_ARG, "nscal out of range 0..12");
@@ -1480,6 +1722,11 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     }
     if ((rc = upload(h, &h->d_iperm, hm.iperm))) return fail(rc);
     if ((rc = dalloc(h, &h->dbuf, h->hs.la[0].size()))) return fail(rc);
+    if (prm->mg_flag == 1) {
+        mg_neigh_definition(mesh, h->nb_ptr_ref, h->nb_lst_ref);
+        mg_coords(mesh, h->cx_ref, h->cy_ref, h->cz_ref);
+        if ((rc = dalloc(h, &h->mg_rrhs, N)) || (rc = dalloc(h, &h->mg_e, N))) return fail(rc);
+    }
     e = cudaStreamSynchronize(h->st);
     if (e != cudaSuccess) return fail(mpg_fail(MPG_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e)));
     *out = h;
@@ -1489,12 +1736,113 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
 extern "C" int mpg_destroy(mpg_handle h) {
     if (!h) return MPG_OK;
     if (h->st) cudaStreamSynchronize(h->st);
+    for (auto &lv : h->mg)
+        if (lv.sub) mpg_destroy(lv.sub);
     kt_collect(h);
     for (cudaEvent_t e : h->kt.pool) cudaEventDestroy(e);
     for (void *p : h->allocs) cudaFree(p);
     if (h->h_res) cudaFreeHost(h->h_res);
-    if (h->st) cudaStreamDestroy(h->st);
+    if (h->st && !h->borrowed_stream) cudaStreamDestroy(h->st);
     delete h;
+    return MPG_OK;
+}
+
+// Attaches the coarse (level 1, the reference's mesh3d_c.d) or coarsest (level 2, mesh3d_cc.d)
+// mesh of precon's V-cycle (ref.f:618-748) to a handle created with mg_flag = 1.  The level gets a
+// handle of its own on the parent's stream (laplc_c / laplc_cc are laplc on that mesh), the match
+// map (given, 1-based as in match1.d / match2.d, or found by coordinates as `matching` does), the
+// finer mesh's neighbour lists, and the set-up data mpsolver computes for levels 2 and 3
+// (ref.f:161-168): beta_timestep_unstr on the level's mesh and compute_d_unstr with the finest rh0
+// restricted to it.  laplc_c/_cc read rh0 of the matched finest node and coefw at the node's own
+// number (mg_bugs = 1) or at the matched finest node (mg_bugs = 0).
+extern "C" int mpg_set_coarse(mpg_handle h, int level, const mpg_mesh_ref *mesh, const int32_t *match) {
+    if (!h || !mesh) return mpg_fail(MPG_ERR_ARG, "set_coarse: null argument");
+    if (h->P.mg_flag != 1) return mpg_fail(MPG_ERR_ARG, "set_coarse: the handle was not created with mg_flag = 1");
+    if (level != 1 && level != 2) return mpg_fail(MPG_ERR_ARG, "set_coarse: level must be 1 or 2");
+    if (level == 2 && !h->mg[0].sub) return mpg_fail(MPG_ERR_ARG, "set_coarse: attach level 1 first");
+    if (h->mg[level - 1].sub) return mpg_fail(MPG_ERR_ARG, "set_coarse: level already attached");
+    mpg_params Ps = h->P;
+    Ps.mg_flag = 0;
+    mpg_handle c = nullptr;
+    int rc = mpg_create(&Ps, mesh, h->dev, &c);
+    if (rc) return rc;
+    cudaStreamSynchronize(c->st);
+    cudaStreamDestroy(c->st);
+    c->st = h->st;
+    c->borrowed_stream = true;
+    auto fail = [&](int code) { mpg_destroy(c); return code; };
+    mpg_solver *fine = level == 1 ? h : h->mg[0].sub;     // the next finer mesh
+    const std::vector<int32_t> &fptr = fine->nb_ptr_ref, &flst = fine->nb_lst_ref;
+    const int nf = fine->N, nc = c->N;
+    std::vector<int32_t> m(nc);
+    if (match) {
+        for (int i = 0; i < nc; ++i) m[i] = match[i] - 1;
+    } else {
+        std::vector<double> x, y, z;
+        mg_coords(mesh, x, y, z);
+        m = mg_matching(fine->cx_ref, fine->cy_ref, fine->cz_ref, x, y, z);
+    }
+    for (int i = 0; i < nc; ++i)
+        if (m[i] < 0 || m[i] >= nf)
+            return fail(mpg_fail(MPG_ERR_MESH, "set_coarse: coarse node " + std::to_string(i + 1) +
+                                                   " has no matching node in the finer mesh"));
+    if (level == 1) {            // the coarse level keeps its own lists for the next restriction
+        mg_neigh_definition(mesh, c->nb_ptr_ref, c->nb_lst_ref);
+        mg_coords(mesh, c->cx_ref, c->cy_ref, c->cz_ref);
+    }
+    auto &lv = h->mg[level - 1];
+    const int bugs = h->P.mg_bugs;
+    // finest-mesh rh0 and coefw in reference numbering
+    std::vector<int32_t> perm_f(h->N);
+    for (int n = 0; n < h->N; ++n) perm_f[h->iperm[n]] = n;
+    std::vector<double> rh0r(h->N), cwr(h->N);
+    for (int i = 0; i < h->N; ++i) { rh0r[i] = h->hs.rh0[perm_f[i]]; cwr[i] = h->hs.coefw[perm_f[i]]; }
+    // the level's node -> finest node; the finest rh0 restricted to the level; its compute_d
+    std::vector<int32_t> to_finest(nc);
+    for (int i = 0; i < nc; ++i) to_finest[i] = level == 1 ? m[i] : h->mg[0].match_ref[m[i]];
+    lv.rh0_restricted = mg_restrict_host(level == 1 ? rh0r : h->mg[0].rh0_restricted, m, fptr, flst, bugs);
+    const std::vector<double> dref = mg_compute_d(mesh, lv.rh0_restricted, h->P.delt);
+    std::vector<int32_t> perm_c(nc);
+    for (int n = 0; n < nc; ++n) perm_c[c->iperm[n]] = n;
+    std::vector<double> rh0c(nc), cwc(nc), dc(nc);
+    for (int i = 0; i < nc; ++i) {
+        rh0c[perm_c[i]] = rh0r[to_finest[i]];
+        cwc[perm_c[i]] = bugs ? cwr[i] : cwr[to_finest[i]];
+        dc[perm_c[i]] = dref[i];
+    }
+    MPG_CUDA(cudaMemcpyAsync(c->f[MPG_F_RH0], rh0c.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, h->st));
+    MPG_CUDA(cudaMemcpyAsync(c->f[MPG_F_COEFW], cwc.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, h->st));
+    MPG_CUDA(cudaMemcpyAsync(c->f[MPG_F_D1], dc.data(), sizeof(double) * nc, cudaMemcpyHostToDevice, h->st));
+    // transfer data in internal numbering: match, the finer mesh's lists, the loop-counter nodes
+    std::vector<int32_t> perm_fine(nf);
+    for (int n = 0; n < nf; ++n) perm_fine[fine->iperm[n]] = n;
+    std::vector<int32_t> mi(nc), ptr_i(nf + 1, 0), lst_i(flst.size());
+    for (int i = 0; i < nc; ++i) mi[perm_c[i]] = perm_fine[m[i]];
+    int maxdeg = 0;
+    for (int i = 0; i < nf; ++i) {
+        const int deg = fptr[i + 1] - fptr[i];
+        ptr_i[perm_fine[i] + 1] = deg;
+        maxdeg = std::max(maxdeg, deg);
+    }
+    for (int n = 0; n < nf; ++n) ptr_i[n + 1] += ptr_i[n];
+    for (int i = 0; i < nf; ++i) {
+        const int n = perm_fine[i];
+        for (int k = 0; k < fptr[i + 1] - fptr[i]; ++k) lst_i[ptr_i[n] + k] = perm_fine[flst[fptr[i] + k]];
+    }
+    if (maxdeg > nf) return fail(mpg_fail(MPG_ERR_MESH, "set_coarse: finer mesh smaller than a node degree"));
+    std::vector<int32_t> bugnb(std::max(maxdeg, 1), 0);
+    for (int k = 0; k < maxdeg; ++k) bugnb[k] = perm_fine[k];
+    lv.passes = bugs ? 1 : mg_fill_passes(nf, m, fptr, flst);
+    if (lv.passes < 0)
+        return fail(mpg_fail(MPG_ERR_MESH, "set_coarse: some finer nodes cannot be reached from the coarse ones"));
+    lv.match_ref = m;
+    if ((rc = upload(h, &lv.match, mi)) || (rc = upload(h, &lv.nbp, ptr_i)) || (rc = upload(h, &lv.nbl, lst_i)) ||
+        (rc = upload(h, &lv.bugnb, bugnb)) || (rc = dalloc(h, &lv.aux, nf)) || (rc = dalloc(h, &lv.flag, nf)) ||
+        (rc = dalloc(c, &lv.p, nc)) || (rc = dalloc(c, &lv.r, nc)) || (rc = dalloc(c, &lv.e, nc)) ||
+        (rc = dalloc(c, &lv.rrhs, nc)) || (rc = dalloc(c, &lv.rrhs_out, nc)))
+        return fail(rc);
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    lv.sub = c;
     return MPG_OK;
 }
 

@@ -287,6 +287,39 @@ def generate(nx: int, ny: Optional[int] = None, L: int = 41, Lx: float = 120e3,
             jit[Ir == nxx - 1, 1] = jit[(Ir == 0), 1]
             jit[Jr == nyy - 1, 0] = jit[(Jr == 0), 0]
     xy = base + jit
+    return _build(xy, nx, ny, L, Lx, Ly, H, h0, half_width, stretch_dz0, periodic, torus, duplicates,
+                  nxx if not torus else nx, nyy if not torus else ny)
+
+
+def coarsen(cm: ColumnMesh) -> ColumnMesh:
+    """The mesh on every other column of a torus mesh made by ``generate``: the nodes of even
+    grid row and column (every node keeps its exact position, terrain height and levels), newly
+    Delaunay-triangulated on the torus with their own median-dual metrics.  These are the coarser
+    meshes of the multigrid V-cycle (the reference reads them as ``mesh3d_c.d`` and
+    ``mesh3d_cc.d``, ref.f:2343-2641); every coarse node coincides with a fine node, as the
+    reference's ``matching`` (ref.f:2684-2720) requires.  Levels are not coarsened."""
+    if not cm.periodic or cm.coin is not None or cm.nx % 2 or cm.ny % 2:
+        raise ValueError("coarsen takes a torus mesh with an even number of columns each way")
+    xy = cm.xy.reshape(cm.ny, cm.nx, 2)[::2, ::2].reshape(-1, 2).copy()
+    out = _build(xy, cm.nx // 2, cm.ny // 2, cm.L, cm.Lx, cm.Ly, cm.H, cm.h0, cm.half_width, None,
+                 True, True, False, cm.nx // 2, cm.ny // 2)
+    out.zeta = np.asarray(cm.zeta).copy()
+    out.zeta_half = np.asarray(cm.zeta_half).copy()
+    return out
+
+
+def coarse_match(fine: ColumnMesh, coarse: ColumnMesh) -> np.ndarray:
+    """For every node of a ``coarsen``-ed mesh, its node in the fine mesh (0-based, in the node
+    numbering of ``to_reference``): the reference's ``match`` arrays (ref.f:2684-2720)."""
+    cols = np.arange(fine.ncol).reshape(fine.ny, fine.nx)[::2, ::2].ravel()
+    if not np.array_equal(fine.xy[cols], coarse.xy):
+        raise ValueError("coarse columns are not the even-index columns of the fine mesh")
+    return (cols[:, None] * fine.L + np.arange(fine.L)[None, :]).ravel()
+
+
+def _build(xy, nx, ny, L, Lx, Ly, H, h0, half_width, stretch_dz0, periodic, torus, duplicates, nxx, nyy):
+    """Mesh on the horizontal points ``xy`` (see ``generate``)."""
+    hx, hy = Lx / nx, Ly / ny
     ncol = xy.shape[0]
 
     if torus:
