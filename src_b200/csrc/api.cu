@@ -81,6 +81,7 @@ struct mpg_solver {
     double *psi1 = nullptr, *g3[3] = {}, *mx = nullptr, *mn = nullptr;
     MpScratchT<float> Sf{};
     float *psi1f = nullptr, *g3f[3] = {}, *mxf = nullptr, *mnf = nullptr;
+    double *psi1d = nullptr;       // mixed precision: the first-pass field kept in FP64 for the update
     // /itero/
     int32_t niter = 0, nitsm = 0, icount = 0, gstatus = 0, last_fallbacks = 0;
     double eer = 0., eem = 0., dvmx_last = 0., rl2_last = 0., rate_last = 0.;
@@ -1341,16 +1342,20 @@ int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
     const T *vol = G::vol(h), *rh0 = G::rh0(h);
     const int N = h->N;
     auto &S = B::S(h);
+    // the node updates of both passes run in FP64 on FP64 vol and rh0, from face fluxes in T; in
+    // mixed precision the first-pass field is kept in FP64 too, so the fields' mass changes only
+    // by FP64 round-off
+    const MpUpdate U64{std::is_same<T, float>::value ? h->psi1d : nullptr, h->vol, h->f[MPG_F_RH0], h->P.delt};
     {
         KTIME(KT_MP_DONOR);
         if (h->P.iper == 2) {
             k_mp_donor<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h),
-                                                                  MpInflow{nullptr, 0., 0});
+                                                                  MpInflow{nullptr, 0., 0}, U64);
         } else {
             // afree = (u0inf, v0inf, w0inf, 0, 1) (ref.f:125-129); iflag = 1 takes ue per node
             const double af = iflag == 2 ? h->P.v0inf : iflag == 3 ? h->P.w0inf : 0.;
             k_mp_donor<T, true><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h),
-                                                                 MpInflow{h->ue, af, iflag});
+                                                                 MpInflow{h->ue, af, iflag}, U64);
         }
     }
     {
@@ -1377,8 +1382,7 @@ int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
     }
     {
         KTIME(KT_MP_PASS2);
-        k_mp_pass2<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::g(h, 0), B::g(h, 1), vol, rh0, dt,
-                                                       psi);
+        k_mp_pass2<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::g(h, 0), B::g(h, 1), U64, psi);
     }
     return check_launch("mpdata");
 }
@@ -1704,7 +1708,7 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     if (prm->precision == MPG_PREC_MIXED) {
         float *aunh, *aunv, *Ah, *Av;
         if ((rc = dalloc(h, &aunh, nh)) || (rc = dalloc(h, &aunv, N)) || (rc = dalloc(h, &Ah, nh)) ||
-            (rc = dalloc(h, &Av, N)) || (rc = dalloc(h, &h->psi1f, N)) || (rc = dalloc(h, &h->mxf, N)) ||
+            (rc = dalloc(h, &Av, N)) || (rc = dalloc(h, &h->psi1f, N)) || (rc = dalloc(h, &h->psi1d, N)) || (rc = dalloc(h, &h->mxf, N)) ||
             (rc = dalloc(h, &h->mnf, N)))
             return fail(rc);
         for (int q = 0; q < 3; ++q)

@@ -80,6 +80,15 @@ struct MpInflow {
     int iflag;
 };
 
+// FP64 node update of both passes: psi_new = psi_old - arh2*dt/vol/rh0 with arh2 summed in FP64
+// from the face fluxes (FP64, or FP32 in mixed precision, where psi1d keeps the first-pass field
+// in FP64 beside its FP32 copy; null in FP64)
+struct MpUpdate {
+    double *psi1d;
+    const double *vol, *rh0;
+    double dt;
+};
+
 // donor-cell pass: fl = psi_a*max(0,aun) + psi_b*min(0,aun); a gets +fl, b gets -fl.
 // OPEN selects mpdatam's first-pass boundary closure (ref.f:3143-3169): every boundary point
 // of a type other than 11, 5 or 6 carries the flux aunbb1 = -divv that balances the node's face
@@ -88,17 +97,18 @@ struct MpInflow {
 template <class T, bool OPEN>
 __global__ void k_mp_donor(ColMesh M, MpScratchT<T> S, const double *__restrict__ psi,
                            const T *__restrict__ vol, const T *__restrict__ rh0, T dt,
-                           T *__restrict__ psi1, MpInflow in) {
+                           T *__restrict__ psi1, MpInflow in, MpUpdate U) {
     NODE_BEGIN
     const T pn = (T)psi[n];
-    T arh2 = 0., divv = 0.;
+    double arh2 = 0.;
+    T divv = 0.;
     for_faces(M, c, k, n,
         [&](const Face &f) { return V4T<T>{(f.vert ? S.aunv : S.aunh)[f.si], (T)psi[f.j], T(0), T(0)}; },
         [&](const Face &f, const V4T<T> &v) {
             const T aun = v.a;
             const T pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
             const T fl = pa * (T(0) > aun ? T(0) : aun) + pb * (T(0) < aun ? T(0) : aun);
-            arh2 = f.sub ? arh2 - fl : arh2 + fl;
+            arh2 = f.sub ? arh2 - (double)fl : arh2 + (double)fl;
             if (OPEN) divv = f.sub ? divv - aun : divv + aun;
         });
     if (OPEN) {
@@ -107,12 +117,14 @@ __global__ void k_mp_donor(ColMesh M, MpScratchT<T> S, const double *__restrict_
             const T fin = in.iflag == 1 ? (T)in.ue[n] : (T)in.afree;
             T fl1 = fin * (T(0) < aunbb1 ? T(0) : aunbb1) + pn * (T(0) > aunbb1 ? T(0) : aunbb1);
             if (be.type == 11 || be.type == 5 || be.type == 6) fl1 = T(0);
-            arh2 = arh2 + fl1 * T(1);
+            arh2 = arh2 + (double)(fl1 * T(1));
         });
     } else if (has_boundary(M, c, k)) {
-        arh2 = arh2 + T(0) * T(1);
+        arh2 = arh2 + (double)(T(0) * T(1));
     }
-    psi1[n] = pn - arh2 * dt / vol[n] / rh0[n];
+    const double p1 = psi[n] - arh2 * U.dt / U.vol[n] / U.rh0[n];
+    psi1[n] = (T)p1;
+    if (U.psi1d) U.psi1d[n] = p1;
 }
 
 // gradient of psi1 (three derivative calls) and the neighbourhood max/min; OPEN adds the
@@ -217,12 +229,11 @@ __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
 
 template <class T>
 __global__ void k_mp_pass2(ColMesh M, MpScratchT<T> S, const T *__restrict__ psi1,
-                           const T *__restrict__ cp, const T *__restrict__ cn,
-                           const T *__restrict__ vol, const T *__restrict__ rh0, T dt,
+                           const T *__restrict__ cp, const T *__restrict__ cn, MpUpdate U,
                            double *__restrict__ psi2) {
     NODE_BEGIN
     const T cpn = cp[n], cnn = cn[n];
-    T arh2 = 0.;
+    double arh2 = 0.;
     for_faces(M, c, k, n,
         [&](const Face &f) { return V4T<T>{(f.vert ? S.Av : S.Ah)[f.si], cp[f.j], cn[f.j], T(0)}; },
         [&](const Face &f, const V4T<T> &v) {
@@ -231,10 +242,11 @@ __global__ void k_mp_pass2(ColMesh M, MpScratchT<T> S, const T *__restrict__ psi
             const T cpa = f.sub ? v.b : cpn, cna = f.sub ? v.c : cnn;
             const T cpb = f.sub ? cpn : v.b, cnb = f.sub ? cnn : v.c;
             const T lim = a > T(0) ? a * tmin(tmin(T(1), cpb), cna) : a * tmin(tmin(T(1), cnb), cpa);
-            arh2 = f.sub ? arh2 - lim : arh2 + lim;
+            arh2 = f.sub ? arh2 - (double)lim : arh2 + (double)lim;
         });
-    if (has_boundary(M, c, k)) arh2 = arh2 + T(0) * T(1);
-    psi2[n] = (double)(psi1[n] - arh2 * dt / vol[n] / rh0[n]);
+    if (has_boundary(M, c, k)) arh2 = arh2 + (double)(T(0) * T(1));
+    const double p1 = U.psi1d ? U.psi1d[n] : (double)psi1[n];
+    psi2[n] = p1 - arh2 * U.dt / U.vol[n] / U.rh0[n];
 }
 
 // ------------------------------------------------------------------------------ mpsolver node loops

@@ -6,7 +6,8 @@ on size, since the CPU oracle needs minutes per step there:
 * MPDATA with the nonoscillatory option keeps the positive scalar non-negative and within its
   initial maximum;
 * every pressure solve stops on the reference's test max|r| <= eps0/dt;
-* the mixed-precision path stays within the stated tolerance of the FP64 path;
+* the mixed-precision path stays within the stated tolerance of the FP64 path and conserves the
+  scalar's mass to FP64 round-off as well;
 * laplc is W-self-adjoint for impfl = 0 (<A u, v>_W = <u, A v>_W) and its adjoint entry point
   satisfies the adjoint identity for impfl = 1;
 * results are run-to-run deterministic (bit-identical) at this size as well.
@@ -66,11 +67,15 @@ def test_fullsize_conservation_sign_and_stopping(big_mesh):
 def test_fullsize_mixed_precision_within_tolerance(big_mesh):
     rm = big_mesh
     a, _ = _run(rm, 0, 2)
-    b, _ = _run(rm, 1, 2)
+    b, db = _run(rm, 1, 2)
     with a, b:
         for k, tol in ((0, 1e-6), (1, 1e-3), (2, 1e-3), (3, 1e-3)):
             x, y = b.get(F_UNK + k), a.get(F_UNK + k)
             assert np.linalg.norm(x - y) / np.linalg.norm(y) < tol, k
+        # FP32 face fluxes with FP64 node updates: the scalar's mass to FP64 round-off
+        w = rm.vol * b.get(F_RH0)
+        m0 = np.sum(w * _scalar(rm))
+        assert abs(db[-1].mass[4] - m0) <= 1e-11 * m0
 
 
 def test_fullsize_laplc_adjoint_and_determinism(big_mesh):
