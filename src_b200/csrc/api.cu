@@ -12,6 +12,7 @@
 #include "learned.cuh"
 #include "mpdata.cuh"
 #include "mg.cuh"
+#include "periodic.cuh"
 
 #include <algorithm>
 #include <unordered_map>
@@ -104,6 +105,7 @@ struct mpg_solver {
     } mg[2];
     double *mg_rrhs = nullptr, *mg_e = nullptr;          // fine-mesh arrays of the V-cycle
     bool borrowed_stream = false;                        // a coarse level runs on its parent's stream
+    CopyList CL{};                                       // periodic copy groups (duplicate-node form)
     // kept for the V-cycle's set-up when mg_flag = 1 (and on a coarse level's handle): the mesh's
     // neighbour lists in neigh_definition order and its coordinates, reference numbering
     std::vector<int32_t> nb_ptr_ref, nb_lst_ref;
@@ -272,11 +274,16 @@ int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
         KTIME(KT_LAP_GRAD);
         k_lap_grad<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
                                                           (T)h->P.delt, impfl, B::F(h));
+        if (h->CL.n)
+            k_cp_lap_grad<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, p, B::vol(h), B::rh0(h), B::coefw(h),
+                                                                    h->ue, (T)h->P.delt, impfl, B::F(h));
     }
     {
         KTIME(KT_LAP_DIV);
         const int PL = (h->L + 1) / 2;
         k_lap_div2<T><<<grid(h->NC * PL), kThreads, 0, h->st>>>(h->M, PL, B::F(h), B::vol(h), B::rh0(h), alap);
+        if (h->CL.n)
+            k_cp_lap_div<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, B::F(h), B::vol(h), B::rh0(h), alap);
     }
     return check_launch("laplc");
 }
@@ -298,8 +305,13 @@ int op_prfr(mpg_handle h, const double *p, const double *us, const double *vs, c
             double *vo, double *wo, int impfl) {
     {
         KTIME(KT_PRFR);
+        if (h->CL.n && (uo == us || vo == vs || wo == ws))
+            return mpg_fail(MPG_ERR_ARG, "prfr with periodic copy lists: outputs must differ from the inputs");
         k_prfr<<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, us, vs, ws, h->vol, h->f[MPG_F_COEFW], h->ue, h->P.delt,
                                                    impfl, uo, vo, wo);
+        if (h->CL.n)
+            k_cp_prfr<<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, p, us, vs, ws, h->vol, h->f[MPG_F_COEFW],
+                                                             h->ue, h->P.delt, impfl, uo, vo, wo);
     }
     return check_launch("prfr");
 }
@@ -308,6 +320,9 @@ int op_div(mpg_handle h, const double *ua, const double *va, const double *wa, d
     {
         KTIME(KT_DIV);
         k_div<<<grid(h->N), kThreads, 0, h->st>>>(h->M, ua, va, wa, h->vol, h->f[MPG_F_RH0], iflg, rhs);
+        if (h->CL.n)
+            k_cp_div<<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, ua, va, wa, h->vol, h->f[MPG_F_RH0], iflg,
+                                                            rhs);
     }
     return check_launch("div");
 }
@@ -719,6 +734,7 @@ nn::Geom nn_geom(mpg_handle h) {
 int nn_alloc_infer(mpg_handle h) {
     auto &S = h->nn;
     int rc;
+    if (h->CL.n) return mpg_fail(MPG_ERR_UNSUPPORTED, "learned preconditioner: periodic copy lists are not provided");
     if (!S.geom) {
         const size_t nh = (size_t)h->NE2 * h->L, n = h->N;
         if ((rc = dalloc(h, &S.Th, nh)) || (rc = dalloc(h, &S.Tv, n)) || (rc = dalloc(h, &S.iDh, n)) ||
@@ -783,12 +799,10 @@ void nn_layers(mpg_handle h, const nn::Geom &G, double *qd, float *qf, bool trai
         // CTAs resident per SM from the kernel's own footprint: registers, static shared memory
         // (with the largest carveout requested) and the 512 tensor-memory columns of an SM.  The
         // occupancy API reported 1 for these kernels, which measured 2.8x slower than 4.
-        cudaFuncSetAttribute(nn::k_nn_col<NS, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(nn::k_nn_col<NS, false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(nn::k_nn_col<NS, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(nn::k_nn_col<NS, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(nn::k_nn_col<NS, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         int per_sm = 1 << 30, sms = 0, regs_sm = 65536, smem_sm = 228 * 1024;
-        const void *fns[3] = {(const void *)nn::k_nn_col<NS, true, false>, (const void *)nn::k_nn_col<NS, false, false>,
-                              (const void *)nn::k_nn_col<NS, false, true>};
+        const void *fns[2] = {(const void *)nn::k_nn_col<NS, false>, (const void *)nn::k_nn_col<NS, true>};
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
         cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, h->dev);
         cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->dev);
@@ -805,16 +819,18 @@ void nn_layers(mpg_handle h, const nn::Geom &G, double *qd, float *qf, bool trai
     }
     const int nb = std::min(h->NC, S.col_ctas);
     const size_t W = (size_t)nn::C * nn::K3;
-    nn::k_nn_col<NS, true, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
-        h->M, G, nullptr, S.X0, S.Wbf, S.prm, 0, nullptr, nullptr, S.H[1], nullptr, nullptr,
-        train ? S.H[0] : nullptr, train ? S.Xs[0] : nullptr, nullptr, S.err);
+    // h0 of every node once (kept in H[0], which training also needs), then the three layers
+    nn::k_nn_h0<<<(int)(((size_t)h->N * 4 + 255) / 256), 256, 0, h->st>>>(h->N, S.X0, S.prm, S.H[0]);
+    nn::k_nn_col<NS, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, S.H[0], S.Wbf, S.prm, 0, nullptr, nullptr, S.H[1], nullptr, nullptr,
+        train ? S.Xs[0] : nullptr, nullptr, S.err);
     __nv_bfloat16 *h2 = train ? S.H[2] : S.H[0];
-    nn::k_nn_col<NS, false, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
-        h->M, G, S.H[1], nullptr, S.Wbf + W, S.prm, 1, nullptr, nullptr, h2, nullptr, nullptr,
-        nullptr, train ? S.Xs[1] : nullptr, nullptr, S.err);
-    nn::k_nn_col<NS, false, true><<<nb, nn::COL_THREADS, 0, h->st>>>(
-        h->M, G, h2, nullptr, S.Wbf + 2 * W, S.prm, 2, S.z, S.sc, train ? S.H[3] : nullptr, qd, qf,
-        nullptr, train ? S.Xs[2] : nullptr, train ? S.Y : nullptr, S.err);
+    nn::k_nn_col<NS, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, S.H[1], S.Wbf + W, S.prm, 1, nullptr, nullptr, h2, nullptr, nullptr,
+        train ? S.Xs[1] : nullptr, nullptr, S.err);
+    nn::k_nn_col<NS, true><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, h2, S.Wbf + 2 * W, S.prm, 2, S.z, S.sc, train ? S.H[3] : nullptr, qd, qf,
+        train ? S.Xs[2] : nullptr, train ? S.Y : nullptr, S.err);
 }
 
 // forward pass on residual r: z = M^{-1} r (impfl coefficients), sigma, the network; q in T.
@@ -1351,6 +1367,8 @@ int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
         if (h->P.iper == 2) {
             k_mp_donor<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h),
                                                                   MpInflow{nullptr, 0., 0}, U64);
+            if (h->CL.n)
+                k_cp_mp_donor<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, S, psi, B::psi1(h), U64);
         } else {
             // afree = (u0inf, v0inf, w0inf, 0, 1) (ref.f:125-129); iflag = 1 takes ue per node
             const double af = iflag == 2 ? h->P.v0inf : iflag == 3 ? h->P.w0inf : 0.;
@@ -1360,9 +1378,15 @@ int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
     }
     {
         KTIME(KT_MP_GRADB);
-        if (h->P.iper == 2)
+        if (h->P.iper == 2) {
             k_mp_grad_bounds<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), B::g(h, 0), B::g(h, 1),
                                                                         B::g(h, 2), B::mx(h), B::mn(h));
+            if (h->CL.n) {
+                k_cp_mp_grad<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, B::psi1(h), B::g(h, 0),
+                                                                       B::g(h, 1), B::g(h, 2));
+                k_cp_bounds<T><<<grid(h->CL.ngroups), kThreads, 0, h->st>>>(h->CL, B::psi1(h), B::mx(h), B::mn(h));
+            }
+        }
         else
             k_mp_grad_bounds<T, true><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), B::g(h, 0), B::g(h, 1),
                                                                        B::g(h, 2), B::mx(h), B::mn(h));
@@ -1379,10 +1403,16 @@ int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
         KTIME(KT_MP_CPCN);
         k_mp_cpcn<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::mx(h), B::mn(h), vol, rh0, dt,
                                                       B::g(h, 0), B::g(h, 1));
+        if (h->CL.n)
+            k_cp_mp_cpcn<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, S, B::psi1(h), B::mx(h), B::mn(h), vol,
+                                                                   rh0, dt, B::g(h, 0), B::g(h, 1));
     }
     {
         KTIME(KT_MP_PASS2);
         k_mp_pass2<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::g(h, 0), B::g(h, 1), U64, psi);
+        if (h->CL.n)
+            k_cp_mp_pass2<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, S, B::psi1(h), B::g(h, 0), B::g(h, 1),
+                                                                    U64, psi);
     }
     return check_launch("mpdata");
 }
@@ -1424,8 +1454,12 @@ int op_velprd(mpg_handle h) {
         KTIME(KT_NODE);
         k_velprd_pre<<<grid(N), kThreads, 0, h->st>>>(N, F, h->P.delt);
         const U3 U{{F.uuu[0], F.uuu[1], F.uuu[2]}};
-        for (int q = 0; q < 3; ++q)
+        for (int q = 0; q < 3; ++q) {
             k_velprd_grad<<<grid(N), kThreads, 0, h->st>>>(h->M, F.ud[q], h->vol, U, h->P.delt, u1[q]);
+            if (h->CL.n)
+                k_cp_velprd_grad<<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, F.ud[q], h->vol, U, h->P.delt,
+                                                                        u1[q]);
+        }
         k_fill<<<grid(N), kThreads, 0, h->st>>>(N, pp, 0.0);
         for (int q = 0; q < 3; ++q) k_fill<<<grid(N), kThreads, 0, h->st>>>(N, ff[q], 0.0);
     }
@@ -1611,6 +1645,21 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     HostColumnMesh hm;
     int rc = mpg_build_column_mesh(mesh, &hm);
     if (rc) return rc;
+    // the reference's duplicate-node periodic form: copies keep their own faces, every edge sum
+    // is completed over the copy group (cyclicr), and the copies' volumes are summed at set-up
+    // (ref.f:99-103)
+    std::vector<double> pvol;
+    mpg_mesh_ref msh = *mesh;
+    if (!hm.cp_node.empty()) {
+        if (prm->iper != 2) return mpg_fail(MPG_ERR_ARG, "periodic copy lists (icoin/icoin2/icoin4) need iper = 2");
+        if (prm->iprc == 3 || prm->iprc == 4 || prm->mg_flag == 1)
+            return mpg_fail(MPG_ERR_UNSUPPORTED, "with periodic copy lists the preconditioner is iprc 0, 1 or 2 "
+                                                 "without the V-cycle");
+        pvol = mpg_periodic_volumes(mesh);
+        msh.vol = pvol.data();
+        for (int n = 0; n < hm.N; ++n) hm.vol[n] = pvol[hm.iperm[n]];
+    }
+    mesh = &msh;
     mpg_solver *h = new mpg_solver();
     h->P = *prm;
     h->dev = device;
@@ -1726,6 +1775,17 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     }
     if ((rc = upload(h, &h->d_iperm, hm.iperm))) return fail(rc);
     if ((rc = dalloc(h, &h->dbuf, h->hs.la[0].size()))) return fail(rc);
+    if (!hm.cp_node.empty()) {
+        CopyList &CL = h->CL;
+        int32_t *a, *b, *c2, *d, *e2, *f2;
+        if ((rc = upload(h, &a, hm.cp_node)) || (rc = upload(h, &b, hm.cp_gbeg)) || (rc = upload(h, &c2, hm.cp_gsize)) ||
+            (rc = upload(h, &d, hm.cp_members)) || (rc = upload(h, &e2, hm.cp_grp)) || (rc = upload(h, &f2, hm.cp_grpsize)))
+            return fail(rc);
+        CL.n = (int32_t)hm.cp_node.size();
+        CL.node = a; CL.gbeg = b; CL.gsize = c2; CL.members = d;
+        CL.ngroups = (int32_t)hm.cp_grp.size();
+        CL.grp = e2; CL.grpsize = f2;
+    }
     if (prm->mg_flag == 1) {
         mg_neigh_definition(mesh, h->nb_ptr_ref, h->nb_lst_ref);
         mg_coords(mesh, h->cx_ref, h->cy_ref, h->cz_ref);
@@ -1891,6 +1951,7 @@ extern "C" int mpg_derivative(mpg_handle h, int unk, int out, int idx) {
     FLD(b, out);
     if (a == b) return mpg_fail(MPG_ERR_ARG, "derivative: input and output must differ");
     k_derivative<<<grid(h->N), kThreads, 0, h->st>>>(h->M, a, b, idx);
+    if (h->CL.n) k_cp_derivative<<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, a, b, idx);
     return check_launch("derivative");
 }
 
@@ -1912,6 +1973,7 @@ extern "C" int mpg_laplc(mpg_handle h, int press, int alap, int impfl) {
 }
 
 extern "C" int mpg_laplc_adjoint(mpg_handle h, int y, int out, int impfl) {
+    if (h && h->CL.n) return mpg_fail(MPG_ERR_UNSUPPORTED, "laplc_adjoint: periodic copy lists are not provided");
     if (!h) return mpg_fail(MPG_ERR_ARG, "null handle");
     FLD(yy, y);
     FLD(oo, out);
@@ -2249,6 +2311,7 @@ extern "C" int mpg_laplc_noalloc(mpg_handle h, const double *press, double *alap
     if (h->dev < 0 || h->dev >= kNoallocMaxDevices)
         return mpg_fail(MPG_ERR_ARG, "laplc_noalloc: device index out of range");
     if (press == alap) return mpg_fail(MPG_ERR_ARG, "laplc_noalloc: input and output must differ");
+    if (h->CL.n) return mpg_fail(MPG_ERR_UNSUPPORTED, "laplc_noalloc: periodic copy lists are not provided");
     // the caller's current device is put back on every return
     struct RestoreDevice {
         int prev = -1;

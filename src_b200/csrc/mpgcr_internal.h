@@ -74,9 +74,15 @@ struct HostColumnMesh {
     bool bitwise_order = true;      // per-node sums follow the reference edge order exactly
     // node-ordered geometry (internal order)
     std::vector<double> x, y, z, vol;
+    // the reference's periodic duplicate-node lists (icoin, icoin2, icoin4) as copy groups in
+    // list order, internal node numbers: every copy node with its group, and the groups
+    std::vector<int32_t> cp_node, cp_gbeg, cp_gsize, cp_members, cp_grp, cp_grpsize;
 };
 
 int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out);
+// the reference's set-up sum of the copies' volumes (cyclicr, cyclicr2, cyclicr4 on vol,
+// ref.f:99-103): vol of every node, with each group's members replaced by their sum
+std::vector<double> mpg_periodic_volumes(const mpg_mesh_ref *m);
 
 // Static per-node quantities computed on the host at creation (internal order), restating the
 // set-up part of mpsolver: rhprof/thprof, absorbers, beta_timestep_unstr, compute_d_unstr,

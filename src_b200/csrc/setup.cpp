@@ -57,10 +57,10 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out) {
     if (!m->coord || !m->vol || (m->nedge && (!m->iedge || !m->sn)) ||
         (m->nbface && (!m->kbface || !m->sb)) || (m->nboun && (!m->ibpoin || !m->anp || !m->sbb)))
         return mpg_fail(MPG_ERR_ARG, "null mesh array");
-    if (m->ncoin || m->ncoin2 || m->ncoin4)
-        return mpg_fail(MPG_ERR_UNSUPPORTED,
-                        "periodic duplicate-node lists (icoin/icoin2/icoin4) are not supported; "
-                        "give the periodic mesh as a torus (wrap-around edges, empty lists)");
+    if ((m->ncoin && !m->icoin) || (m->ncoin2 && !m->icoin2) || (m->ncoin4 && !m->icoin4) || m->ncoin < 0 ||
+        m->ncoin2 < 0 || m->ncoin4 < 0 || (m->ncoin && m->ldcoin < m->ncoin) ||
+        (m->ncoin2 && m->nfacesx < m->ncoin2) || (m->ncoin4 && m->nfacesx < m->ncoin4))
+        return mpg_fail(MPG_ERR_ARG, "periodic lists: null array or leading dimension smaller than the count");
     const double *X = m->coord, *Y = m->coord + m->npoinx, *Z = m->coord + 2 * (size_t)m->npoinx;
 
     // ---- 1. columns = nodes with bitwise-equal (x, y), in order of first appearance
@@ -283,7 +283,54 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out) {
         out->x[n] = X[i]; out->y[n] = Y[i]; out->z[n] = Z[i]; out->vol[n] = m->vol[i];
     }
     out->NC = NC; out->L = L; out->N = npoin; out->NE2 = NE2;
+
+    // ---- 8. periodic copy groups (icoin pairs, icoin2 pairs, icoin4 quadruples), list order
+    out->cp_node.clear(); out->cp_gbeg.clear(); out->cp_gsize.clear();
+    out->cp_members.clear(); out->cp_grp.clear(); out->cp_grpsize.clear();
+    std::vector<uint8_t> seen(npoin, 0);
+    struct Lst { const int32_t *a; int n, w; size_t ld; };
+    const Lst lists[3] = {{m->icoin, m->ncoin, 2, (size_t)m->ldcoin}, {m->icoin2, m->ncoin2, 2, (size_t)m->nfacesx},
+                          {m->icoin4, m->ncoin4, 4, (size_t)m->nfacesx}};
+    for (const Lst &l : lists)
+        for (int g = 0; g < l.n; ++g) {
+            const int32_t off = (int32_t)out->cp_members.size();
+            out->cp_grp.push_back(off);
+            out->cp_grpsize.push_back(l.w);
+            for (int q = 0; q < l.w; ++q) {
+                const int i = l.a[(size_t)q * l.ld + g] - 1;
+                if (i < 0 || i >= npoin) return mpg_fail(MPG_ERR_MESH, "periodic list names a node out of range");
+                if (seen[i]) return mpg_fail(MPG_ERR_UNSUPPORTED, "a node appears in more than one periodic copy group");
+                seen[i] = 1;
+                out->cp_members.push_back(out->perm[i]);
+            }
+            for (int q = 0; q < l.w; ++q) {
+                out->cp_node.push_back(out->cp_members[off + q]);
+                out->cp_gbeg.push_back(off);
+                out->cp_gsize.push_back(l.w);
+            }
+        }
     return MPG_OK;
+}
+
+std::vector<double> mpg_periodic_volumes(const mpg_mesh_ref *m) {
+    std::vector<double> v(m->vol, m->vol + m->npoin);
+    auto pairs = [&](const int32_t *a, int n, size_t ld) {        // cyclicr / cyclicr2
+        std::vector<double> uc(n);
+        for (int c = 0; c < n; ++c) uc[c] = v[a[c] - 1] + v[a[ld + c] - 1];
+        for (int c = 0; c < n; ++c) { v[a[c] - 1] = uc[c]; v[a[ld + c] - 1] = uc[c]; }
+    };
+    if (m->ncoin) pairs(m->icoin, m->ncoin, (size_t)m->ldcoin);
+    if (m->ncoin2) pairs(m->icoin2, m->ncoin2, (size_t)m->nfacesx);
+    if (m->ncoin4) {                                                // cyclicr4
+        const size_t ld = m->nfacesx;
+        const int32_t *a = m->icoin4;
+        std::vector<double> uc(m->ncoin4);
+        for (int c = 0; c < m->ncoin4; ++c)
+            uc[c] = v[a[c] - 1] + v[a[ld + c] - 1] + v[a[2 * ld + c] - 1] + v[a[3 * ld + c] - 1];
+        for (int c = 0; c < m->ncoin4; ++c)
+            for (int q = 0; q < 4; ++q) v[a[q * ld + c] - 1] = uc[c];
+    }
+    return v;
 }
 
 // Static set-up quantities (internal order).  Each block names the reference lines it

@@ -93,12 +93,18 @@ def test_analyze_rejects_non_column_mesh(small_mesh):
     assert e.value.code == 3
 
 
-def test_analyze_rejects_periodic_lists(small_mesh):
-    cm, rm = small_mesh
-    dup = mesh.RefMesh(**{**rm.__dict__})
-    dup.icoin = np.array([[0, 1]], np.int32)
+def test_analyze_periodic_duplicate_form():
+    """The reference's duplicate-node periodic form (icoin/icoin2/icoin4 copy lists) is accepted;
+    a node named in two copy groups is not."""
+    m = mesh.generate(6, L=5, seed=2, duplicates=True)
+    rm = m.to_reference()
+    info = api.analyze_mesh(rm)
+    assert info["ncol"] == 49 and info["nlev"] == 5
+    bad = mesh.RefMesh(**{**rm.__dict__})
+    bad.icoin2 = rm.icoin2.copy()
+    bad.icoin2[0, 0] = rm.icoin[0, 0]
     with pytest.raises(api.MpgError) as e:
-        api.analyze_mesh(dup)
+        api.analyze_mesh(bad)
     assert e.value.code == 5
 
 

@@ -43,6 +43,7 @@ def test_wide_solve_bitwise(case, impfl):
     name, rm = case
     P = params(name)
     o = Oracle(P, rm)
+    o.setup()                    # rh0 and coefw, which the column blocks depend on
     r = np.random.default_rng(31).standard_normal(rm.npoin)
     with Solver(P, rm) as s:
         s.set(W0, r)
