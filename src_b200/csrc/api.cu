@@ -81,8 +81,9 @@ struct mpg_solver {
     MpScratch S{};
     double *psi1 = nullptr, *g3[3] = {}, *mx = nullptr, *mn = nullptr;
     MpScratchT<float> Sf{};
-    float *psi1f = nullptr, *g3f[3] = {}, *mxf = nullptr, *mnf = nullptr;
-    double *psi1d = nullptr;       // mixed precision: the first-pass field kept in FP64 for the update
+    float *psi1f = nullptr, *g3f[3] = {};
+    // mixed precision: the first-pass field, the FCT bounds and the limiter ratios in FP64
+    double *psi1d = nullptr, *mxd = nullptr, *mnd = nullptr, *cpd = nullptr, *cnd = nullptr;
     // /itero/
     int32_t niter = 0, nitsm = 0, icount = 0, gstatus = 0, last_fallbacks = 0;
     double eer = 0., eem = 0., dvmx_last = 0., rl2_last = 0., rate_last = 0.;
@@ -799,10 +800,12 @@ void nn_layers(mpg_handle h, const nn::Geom &G, double *qd, float *qf, bool trai
         // CTAs resident per SM from the kernel's own footprint: registers, static shared memory
         // (with the largest carveout requested) and the 512 tensor-memory columns of an SM.  The
         // occupancy API reported 1 for these kernels, which measured 2.8x slower than 4.
-        cudaFuncSetAttribute(nn::k_nn_col<NS, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        cudaFuncSetAttribute(nn::k_nn_col<NS, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(nn::k_nn_col<NS, true, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(nn::k_nn_col<NS, false, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(nn::k_nn_col<NS, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         int per_sm = 1 << 30, sms = 0, regs_sm = 65536, smem_sm = 228 * 1024;
-        const void *fns[2] = {(const void *)nn::k_nn_col<NS, false>, (const void *)nn::k_nn_col<NS, true>};
+        const void *fns[3] = {(const void *)nn::k_nn_col<NS, true, false>, (const void *)nn::k_nn_col<NS, false, false>,
+                              (const void *)nn::k_nn_col<NS, false, true>};
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
         cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, h->dev);
         cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, h->dev);
@@ -819,18 +822,16 @@ void nn_layers(mpg_handle h, const nn::Geom &G, double *qd, float *qf, bool trai
     }
     const int nb = std::min(h->NC, S.col_ctas);
     const size_t W = (size_t)nn::C * nn::K3;
-    // h0 of every node once (kept in H[0], which training also needs), then the three layers
-    nn::k_nn_h0<<<(int)(((size_t)h->N * 4 + 255) / 256), 256, 0, h->st>>>(h->N, S.X0, S.prm, S.H[0]);
-    nn::k_nn_col<NS, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
-        h->M, G, S.H[0], S.Wbf, S.prm, 0, nullptr, nullptr, S.H[1], nullptr, nullptr,
-        train ? S.Xs[0] : nullptr, nullptr, S.err);
+    nn::k_nn_col<NS, true, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, nullptr, S.X0, S.Wbf, S.prm, 0, nullptr, nullptr, S.H[1], nullptr, nullptr,
+        train ? S.H[0] : nullptr, train ? S.Xs[0] : nullptr, nullptr, S.err);
     __nv_bfloat16 *h2 = train ? S.H[2] : S.H[0];
-    nn::k_nn_col<NS, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
-        h->M, G, S.H[1], S.Wbf + W, S.prm, 1, nullptr, nullptr, h2, nullptr, nullptr,
-        train ? S.Xs[1] : nullptr, nullptr, S.err);
-    nn::k_nn_col<NS, true><<<nb, nn::COL_THREADS, 0, h->st>>>(
-        h->M, G, h2, S.Wbf + 2 * W, S.prm, 2, S.z, S.sc, train ? S.H[3] : nullptr, qd, qf,
-        train ? S.Xs[2] : nullptr, train ? S.Y : nullptr, S.err);
+    nn::k_nn_col<NS, false, false><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, S.H[1], nullptr, S.Wbf + W, S.prm, 1, nullptr, nullptr, h2, nullptr, nullptr,
+        nullptr, train ? S.Xs[1] : nullptr, nullptr, S.err);
+    nn::k_nn_col<NS, false, true><<<nb, nn::COL_THREADS, 0, h->st>>>(
+        h->M, G, h2, nullptr, S.Wbf + 2 * W, S.prm, 2, S.z, S.sc, train ? S.H[3] : nullptr, qd, qf,
+        nullptr, train ? S.Xs[2] : nullptr, train ? S.Y : nullptr, S.err);
 }
 
 // forward pass on residual r: z = M^{-1} r (impfl coefficients), sigma, the network; q in T.
@@ -1324,13 +1325,19 @@ template <> struct MpBuf<double> {
     static double *g(mpg_handle h, int d) { return h->g3[d]; }
     static double *mx(mpg_handle h) { return h->mx; }
     static double *mn(mpg_handle h) { return h->mn; }
+    static double *psi1d(mpg_handle h) { return h->psi1; }     // the first-pass field in FP64
+    static double *cp(mpg_handle h) { return h->g3[0]; }       // the gradient buffers, dead by then
+    static double *cn(mpg_handle h) { return h->g3[1]; }
 };
 template <> struct MpBuf<float> {
     static MpScratchT<float> &S(mpg_handle h) { return h->Sf; }
     static float *psi1(mpg_handle h) { return h->psi1f; }
     static float *g(mpg_handle h, int d) { return h->g3f[d]; }
-    static float *mx(mpg_handle h) { return h->mxf; }
-    static float *mn(mpg_handle h) { return h->mnf; }
+    static double *mx(mpg_handle h) { return h->mxd; }
+    static double *mn(mpg_handle h) { return h->mnd; }
+    static double *psi1d(mpg_handle h) { return h->psi1d; }
+    static double *cp(mpg_handle h) { return h->cpd; }
+    static double *cn(mpg_handle h) { return h->cnd; }
 };
 
 template <class T>
@@ -1358,38 +1365,41 @@ int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
     const T *vol = G::vol(h), *rh0 = G::rh0(h);
     const int N = h->N;
     auto &S = B::S(h);
-    // the node updates of both passes run in FP64 on FP64 vol and rh0, from face fluxes in T; in
-    // mixed precision the first-pass field is kept in FP64 too, so the fields' mass changes only
-    // by FP64 round-off
-    const MpUpdate U64{std::is_same<T, float>::value ? h->psi1d : nullptr, h->vol, h->f[MPG_F_RH0], h->P.delt};
+    // face fluxes and the antidiffusive velocity in T; the node work of both passes (donor fluxes
+    // from the FP64 field, FCT bounds, in/out sums, limiter ratios, updates) in FP64 on FP64 vol
+    // and rh0, with the first-pass field kept in FP64 beside its T copy in mixed precision
+    const bool mixed = std::is_same<T, float>::value;
+    const MpUpdate U64{mixed ? h->psi1d : nullptr, h->vol, h->f[MPG_F_RH0], h->P.delt};
+    const double *b1 = B::psi1d(h);                       // the FP64 first-pass field
     {
         KTIME(KT_MP_DONOR);
         if (h->P.iper == 2) {
-            k_mp_donor<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h),
+            k_mp_donor<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, B::psi1(h),
                                                                   MpInflow{nullptr, 0., 0}, U64);
             if (h->CL.n)
                 k_cp_mp_donor<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, S, psi, B::psi1(h), U64);
         } else {
             // afree = (u0inf, v0inf, w0inf, 0, 1) (ref.f:125-129); iflag = 1 takes ue per node
             const double af = iflag == 2 ? h->P.v0inf : iflag == 3 ? h->P.w0inf : 0.;
-            k_mp_donor<T, true><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, vol, rh0, dt, B::psi1(h),
+            k_mp_donor<T, true><<<grid(N), kThreads, 0, h->st>>>(h->M, S, psi, B::psi1(h),
                                                                  MpInflow{h->ue, af, iflag}, U64);
         }
     }
     {
         KTIME(KT_MP_GRADB);
+        const double *bsrc = mixed ? b1 : nullptr;
         if (h->P.iper == 2) {
-            k_mp_grad_bounds<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), B::g(h, 0), B::g(h, 1),
-                                                                        B::g(h, 2), B::mx(h), B::mn(h));
+            k_mp_grad_bounds<T, false><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), bsrc, B::g(h, 0),
+                                                                        B::g(h, 1), B::g(h, 2), B::mx(h), B::mn(h));
             if (h->CL.n) {
                 k_cp_mp_grad<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, B::psi1(h), B::g(h, 0),
                                                                        B::g(h, 1), B::g(h, 2));
-                k_cp_bounds<T><<<grid(h->CL.ngroups), kThreads, 0, h->st>>>(h->CL, B::psi1(h), B::mx(h), B::mn(h));
+                k_cp_bounds<<<grid(h->CL.ngroups), kThreads, 0, h->st>>>(h->CL, b1, B::mx(h), B::mn(h));
             }
         }
         else
-            k_mp_grad_bounds<T, true><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), B::g(h, 0), B::g(h, 1),
-                                                                       B::g(h, 2), B::mx(h), B::mn(h));
+            k_mp_grad_bounds<T, true><<<grid(N), kThreads, 0, h->st>>>(h->M, B::psi1(h), bsrc, B::g(h, 0),
+                                                                       B::g(h, 1), B::g(h, 2), B::mx(h), B::mn(h));
     }
     AntiArgs<T> A{B::psi1(h), B::g(h, 0), B::g(h, 1), B::g(h, 2), vol, rh0,
                   U3{{h->f[MPG_F_UUU], h->f[MPG_F_UUU + 1], h->f[MPG_F_UUU + 2]}}, dt};
@@ -1398,20 +1408,19 @@ int op_mpdata_field_t(mpg_handle h, double *psi, int iflag) {
         KTIME(KT_MP_ANTI);
         k_mp_anti<T><<<grid(nt), kThreads, 0, h->st>>>(h->M, S, A);
     }
-    // cp, cn reuse the gradient buffers (dead after the antidiffusive fluxes)
     {
         KTIME(KT_MP_CPCN);
-        k_mp_cpcn<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::mx(h), B::mn(h), vol, rh0, dt,
-                                                      B::g(h, 0), B::g(h, 1));
+        k_mp_cpcn<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, b1, B::mx(h), B::mn(h), h->vol, h->f[MPG_F_RH0],
+                                                      h->P.delt, B::cp(h), B::cn(h));
         if (h->CL.n)
-            k_cp_mp_cpcn<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, S, B::psi1(h), B::mx(h), B::mn(h), vol,
-                                                                   rh0, dt, B::g(h, 0), B::g(h, 1));
+            k_cp_mp_cpcn<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, S, b1, B::mx(h), B::mn(h), h->vol,
+                                                                   h->f[MPG_F_RH0], h->P.delt, B::cp(h), B::cn(h));
     }
     {
         KTIME(KT_MP_PASS2);
-        k_mp_pass2<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::g(h, 0), B::g(h, 1), U64, psi);
+        k_mp_pass2<T><<<grid(N), kThreads, 0, h->st>>>(h->M, S, B::psi1(h), B::cp(h), B::cn(h), U64, psi);
         if (h->CL.n)
-            k_cp_mp_pass2<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, S, B::psi1(h), B::g(h, 0), B::g(h, 1),
+            k_cp_mp_pass2<T><<<grid(h->CL.n), kThreads, 0, h->st>>>(h->M, h->CL, S, B::psi1(h), B::cp(h), B::cn(h),
                                                                     U64, psi);
     }
     return check_launch("mpdata");
@@ -1757,8 +1766,8 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
     if (prm->precision == MPG_PREC_MIXED) {
         float *aunh, *aunv, *Ah, *Av;
         if ((rc = dalloc(h, &aunh, nh)) || (rc = dalloc(h, &aunv, N)) || (rc = dalloc(h, &Ah, nh)) ||
-            (rc = dalloc(h, &Av, N)) || (rc = dalloc(h, &h->psi1f, N)) || (rc = dalloc(h, &h->psi1d, N)) || (rc = dalloc(h, &h->mxf, N)) ||
-            (rc = dalloc(h, &h->mnf, N)))
+            (rc = dalloc(h, &Av, N)) || (rc = dalloc(h, &h->psi1f, N)) || (rc = dalloc(h, &h->psi1d, N)) || (rc = dalloc(h, &h->mxd, N)) ||
+            (rc = dalloc(h, &h->mnd, N)) || (rc = dalloc(h, &h->cpd, N)) || (rc = dalloc(h, &h->cnd, N)))
             return fail(rc);
         for (int q = 0; q < 3; ++q)
             if ((rc = dalloc(h, &h->g3f[q], N))) return fail(rc);

@@ -130,25 +130,26 @@ __device__ __forceinline__ uint32_t tc_core_off(int row, int kc, int groups) {
 // 128x32x96 BF16 product (tcgen05.mma, FP32 accumulator in tensor memory), and in the epilogue
 // warp w reads TMEM lanes 32w..32w+31 (rows 32w + lane), all 32 columns: each thread holds a
 // whole output row.
-// The first layer reads h0 = relu(W_in x + b_in), computed once per node by k_nn_h0.
+//   FIRST: the layer input h0 = relu(W_in x + b_in) is computed on the fly from the node
+//          features x (X0, FP32 [N][4]) of the column and of each neighbour;
 //   LAST:  the epilogue applies the output layer, y = w_out . h3 + b_out, q = z + y s / |b|,
 //          instead of storing h3 (kept only when training).
-// Training keeps H (the layer output), Xs (the layer input rows) and Y.
+// Training keeps H (h0 with FIRST, the layer output), Xs (the layer input rows) and Y.
 constexpr int COL_THREADS = 128;
 constexpr int COL_MAXL = 128;
-constexpr int NF = 3;            // adjacency entries whose neighbour rows are in flight together
 
-template <int NS, bool LAST>
+template <int NS, bool FIRST, bool LAST>
 __global__ void __launch_bounds__(COL_THREADS)
-k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin,
+k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin, const float *__restrict__ X0,
          const __nv_bfloat16 *__restrict__ Wbf, const float *__restrict__ prm, int layer,
          const double *__restrict__ z, const double *__restrict__ sc,
          __nv_bfloat16 *__restrict__ Hout, double *__restrict__ qd, float *__restrict__ qf,
-         __nv_bfloat16 *__restrict__ Xs, float *__restrict__ Y, int *__restrict__ err) {
+         __nv_bfloat16 *__restrict__ Hkeep0, __nv_bfloat16 *__restrict__ Xs, float *__restrict__ Y,
+         int *__restrict__ err) {
     __shared__ __align__(1024) uint8_t sA[TCM * K3 * 2];          // 24 KB operand tile
     __shared__ __align__(1024) uint8_t sB[C * K3 * 2];            // 6 KB weights
     __shared__ __align__(16) __nv_bfloat16 sH[COL_MAXL * C];      // own rows (8 KB)
-    __shared__ float sBias[C], sWout[C + 1];
+    __shared__ float sBias[C], sWin[C * FIN + C], sWout[C + 1];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
@@ -165,6 +166,7 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin,
         if (row >= L) *reinterpret_cast<uint4 *>(sA + tc_core_off(row, kc, TCM / 8)) = make_uint4(0, 0, 0, 0);
     }
     if (tid < C) sBias[tid] = bias[tid];
+    if (FIRST) for (int i = tid; i < C * FIN + C; i += COL_THREADS) sWin[i] = prm[OFF_WIN + i];
     if (LAST && tid <= C) sWout[tid] = prm[OFF_WOUT + tid];
     if (w == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -183,15 +185,35 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin,
     const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
     uint32_t phase = 0;
     bool ok = true;
+    // the first layer's input rows: h0 = bf16(relu(W_in x + b_in)), channels 8w..8w+7
+    auto h0_row = [&](const float4 x, float *o) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int c = 8 * w + i;
+            float u = sWin[C * FIN + c] + sWin[c * FIN + 0] * x.x + sWin[c * FIN + 1] * x.y +
+                      sWin[c * FIN + 2] * x.z + sWin[c * FIN + 3] * x.w;
+            o[i] = __bfloat162float(__float2bfloat16(u > 0.f ? u : 0.f));
+        }
+    };
     for (int c = blockIdx.x; c < M.NC && ok; c += gridDim.x) {
         const int base = c * L;
         // ---- own rows (octet w) into sH
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int k = lane + 32 * s;
-            if (k < L)
-                *reinterpret_cast<B8 *>(sH + k * C + 8 * w) =
-                    *reinterpret_cast<const B8 *>(Hin + (size_t)(base + k) * C + 8 * w);
+            if (k < L) {
+                B8 v;
+                if (FIRST) {
+                    float o[8];
+                    h0_row(*reinterpret_cast<const float4 *>(X0 + (size_t)(base + k) * FIN), o);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) v.v[i] = __floats2bfloat162_rn(o[2 * i], o[2 * i + 1]);
+                    if (Hkeep0) *reinterpret_cast<B8 *>(Hkeep0 + (size_t)(base + k) * C + 8 * w) = v;
+                } else {
+                    v = *reinterpret_cast<const B8 *>(Hin + (size_t)(base + k) * C + 8 * w);
+                }
+                *reinterpret_cast<B8 *>(sH + k * C + 8 * w) = v;
+            }
         }
         // ---- horizontal aggregation: ah = sum_f w_f h_j, wsum = sum_f w_f
         float ah[NS][8], wsum[NS], ih[NS];
@@ -204,42 +226,32 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin,
             for (int i = 0; i < 8; ++i) ah[s][i] = 0.f;
         }
         const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
-        // NF adjacency entries per round: the neighbour rows of all their horizontal faces are
-        // requested before any is accumulated (vertical entries are skipped; the faces are still
-        // added in list order)
-        for (int j = beg; j < end; j += NF) {
-            int2 en[NF];
-            uint4 v[NF][NS];
-            float t[NF][NS];
+        for (int j = beg; j < end; ++j) {
+            const int2 en = __ldg(&M.cadj[j]);
+            if (en.x < 0) continue;                      // vertical faces: below, from sH
+            const int e = en.x >> 1, nb = en.y * L;
+            uint4 v[NS];
+            float t[NS];
 #pragma unroll
-            for (int u = 0; u < NF; ++u) en[u] = j + u < end ? __ldg(&M.cadj[j + u]) : make_int2(-1, 0);
-#pragma unroll
-            for (int u = 0; u < NF; ++u) {
-                if (en[u].x < 0) continue;               // vertical faces: below, from sH
-                const int e = en[u].x >> 1, nb = en[u].y * L;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) {
-                    const int k = lane + 32 * s;
-                    if (k < L) {
-                        v[u][s] = *reinterpret_cast<const uint4 *>(Hin + (size_t)(nb + k) * C + 8 * w);
-                        t[u][s] = G.Th[(size_t)e * L + k];
-                    }
+            for (int s = 0; s < NS; ++s) {
+                const int k = lane + 32 * s;
+                if (k < L) {
+                    if (FIRST) v[s] = *reinterpret_cast<const uint4 *>(X0 + (size_t)(nb + k) * FIN);
+                    else v[s] = *reinterpret_cast<const uint4 *>(Hin + (size_t)(nb + k) * C + 8 * w);
+                    t[s] = G.Th[(size_t)e * L + k];
                 }
             }
 #pragma unroll
-            for (int u = 0; u < NF; ++u) {
-                if (en[u].x < 0) continue;
+            for (int s = 0; s < NS; ++s) {
+                const int k = lane + 32 * s;
+                if (k >= L) continue;
+                float hj[8];
+                if (FIRST) h0_row(*reinterpret_cast<const float4 *>(&v[s]), hj);
+                else b8_to_f(*reinterpret_cast<const B8 *>(&v[s]), hj);
+                const float wt = t[s] * ih[s];
+                wsum[s] += wt;
 #pragma unroll
-                for (int s = 0; s < NS; ++s) {
-                    const int k = lane + 32 * s;
-                    if (k >= L) continue;
-                    float hj[8];
-                    b8_to_f(*reinterpret_cast<const B8 *>(&v[u][s]), hj);
-                    const float wt = t[u][s] * ih[s];
-                    wsum[s] += wt;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) ah[s][i] += wt * hj[i];
-                }
+                for (int i = 0; i < 8; ++i) ah[s][i] += wt * hj[i];
             }
         }
         __syncwarp();
@@ -371,32 +383,6 @@ k_nn_col(ColMesh M, Geom G, const __nv_bfloat16 *__restrict__ Hin,
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (w == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_TMEM_COLS));
-}
-
-// the first layer's input h0 = bf16(relu(W_in x + b_in)) of every node, once (BF16 [N][C])
-__global__ void k_nn_h0(int N, const float *__restrict__ X0, const float *__restrict__ prm,
-                        __nv_bfloat16 *__restrict__ H0) {
-    __shared__ float sW[C * FIN + C];
-    for (int i = threadIdx.x; i < C * FIN + C; i += blockDim.x) sW[i] = prm[OFF_WIN + i];
-    __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n = t >> 2, oct = t & 3;            // four threads per node, eight channels each
-    if (n >= N) return;
-    const float4 x = *reinterpret_cast<const float4 *>(X0 + (size_t)n * FIN);
-    B8 v;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        float o[2];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int c = 8 * oct + 2 * i + q;
-            const float u = sW[C * FIN + c] + sW[c * FIN + 0] * x.x + sW[c * FIN + 1] * x.y +
-                            sW[c * FIN + 2] * x.z + sW[c * FIN + 3] * x.w;
-            o[q] = u > 0.f ? u : 0.f;
-        }
-        v.v[i] = __floats2bfloat162_rn(o[0], o[1]);
-    }
-    *reinterpret_cast<B8 *>(H0 + (size_t)n * C + 8 * oct) = v;
 }
 
 // node features x = [r/s, z|b|/s, ln(Dv/Dh)/8, bnd] (FP32 [N][4])

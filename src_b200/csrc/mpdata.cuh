@@ -80,9 +80,12 @@ struct MpInflow {
     int iflag;
 };
 
-// FP64 node update of both passes: psi_new = psi_old - arh2*dt/vol/rh0 with arh2 summed in FP64
+// FP64 node work of both passes: psi_new = psi_old - arh2*dt/vol/rh0 with arh2 summed in FP64
 // from the face fluxes (FP64, or FP32 in mixed precision, where psi1d keeps the first-pass field
-// in FP64 beside its FP32 copy; null in FP64)
+// in FP64 beside its FP32 copy; null in FP64).  The donor fluxes use the FP64 field, and the FCT
+// bounds, in/out sums and limiter ratios are FP64 too, so that the limiter's guarantees (sign and
+// bounds of the field) hold for the FP64 values it updates, and its mass changes only by FP64
+// round-off.
 struct MpUpdate {
     double *psi1d;
     const double *vol, *rh0;
@@ -96,33 +99,31 @@ struct MpUpdate {
 // (ref.f:3732-3738).
 template <class T, bool OPEN>
 __global__ void k_mp_donor(ColMesh M, MpScratchT<T> S, const double *__restrict__ psi,
-                           const T *__restrict__ vol, const T *__restrict__ rh0, T dt,
                            T *__restrict__ psi1, MpInflow in, MpUpdate U) {
     NODE_BEGIN
-    const T pn = (T)psi[n];
-    double arh2 = 0.;
-    T divv = 0.;
+    const double pn = psi[n];
+    double arh2 = 0., divv = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4T<T>{(f.vert ? S.aunv : S.aunh)[f.si], (T)psi[f.j], T(0), T(0)}; },
-        [&](const Face &f, const V4T<T> &v) {
-            const T aun = v.a;
-            const T pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
-            const T fl = pa * (T(0) > aun ? T(0) : aun) + pb * (T(0) < aun ? T(0) : aun);
-            arh2 = f.sub ? arh2 - (double)fl : arh2 + (double)fl;
+        [&](const Face &f) { return V4{(double)(f.vert ? S.aunv : S.aunh)[f.si], psi[f.j], 0., 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double aun = v.a;
+            const double pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
+            const double fl = pa * (0. > aun ? 0. : aun) + pb * (0. < aun ? 0. : aun);
+            arh2 = f.sub ? arh2 - fl : arh2 + fl;
             if (OPEN) divv = f.sub ? divv - aun : divv + aun;
         });
     if (OPEN) {
         for_boundary(M, c, k, [&](const BEntry &be) {
-            const T aunbb1 = -divv;
-            const T fin = in.iflag == 1 ? (T)in.ue[n] : (T)in.afree;
-            T fl1 = fin * (T(0) < aunbb1 ? T(0) : aunbb1) + pn * (T(0) > aunbb1 ? T(0) : aunbb1);
-            if (be.type == 11 || be.type == 5 || be.type == 6) fl1 = T(0);
-            arh2 = arh2 + (double)(fl1 * T(1));
+            const double aunbb1 = -divv;
+            const double fin = in.iflag == 1 ? in.ue[n] : in.afree;
+            double fl1 = fin * (0. < aunbb1 ? 0. : aunbb1) + pn * (0. > aunbb1 ? 0. : aunbb1);
+            if (be.type == 11 || be.type == 5 || be.type == 6) fl1 = 0.;
+            arh2 = arh2 + fl1 * 1.;
         });
     } else if (has_boundary(M, c, k)) {
-        arh2 = arh2 + (double)(T(0) * T(1));
+        arh2 = arh2 + 0. * 1.;
     }
-    const double p1 = psi[n] - arh2 * U.dt / U.vol[n] / U.rh0[n];
+    const double p1 = pn - arh2 * U.dt / U.vol[n] / U.rh0[n];
     psi1[n] = (T)p1;
     if (U.psi1d) U.psi1d[n] = p1;
 }
@@ -130,12 +131,14 @@ __global__ void k_mp_donor(ColMesh M, MpScratchT<T> S, const double *__restrict_
 // gradient of psi1 (three derivative calls) and the neighbourhood max/min; OPEN adds the
 // derivative's boundary closure of iper = 0 (mpdatam)
 template <class T, bool OPEN>
-__global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, T *__restrict__ gx,
-                                 T *__restrict__ gy, T *__restrict__ gz,
-                                 T *__restrict__ mx, T *__restrict__ mn) {
+__global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, const double *__restrict__ psi1d,
+                                 T *__restrict__ gx, T *__restrict__ gy, T *__restrict__ gz,
+                                 double *__restrict__ mx, double *__restrict__ mn) {
     NODE_BEGIN
     const T pn = psi1[n];
-    T ax = 0., ay = 0., az = 0., hi = T(-1.e15), lo = T(1.e15);
+    const double bn = psi1d ? psi1d[n] : (double)pn;       // the bounds come from the FP64 field
+    T ax = 0., ay = 0., az = 0.;
+    double hi = -1.e15, lo = 1.e15;
     for_faces(M, c, k, n,
         [&](const Face &f) {
             V4T<T> v;
@@ -149,10 +152,11 @@ __global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, T *__res
             const T tx = v.a * u, ty = v.b * u, tz = v.c * u;
             if (f.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
             else       { ax = ax + tx; ay = ay + ty; az = az + tz; }
-            hi = hi > pn ? hi : pn;
-            hi = hi > pj ? hi : pj;
-            lo = lo < pn ? lo : pn;
-            lo = lo < pj ? lo : pj;
+            const double bj = psi1d ? psi1d[f.j] : (double)pj;
+            hi = hi > bn ? hi : bn;
+            hi = hi > bj ? hi : bj;
+            lo = lo < bn ? lo : bn;
+            lo = lo < bj ? lo : bj;
         });
     if (OPEN) {                                         // derivative's closure, ref.f:4007-4014
         for_boundary(M, c, k, [&](const BEntry &be) {
@@ -201,24 +205,24 @@ __global__ void k_mp_anti(ColMesh M, MpScratchT<T> S, AntiArgs<T> A) {
     }
 }
 
-// in/out sums and the limiter ratios
+// in/out sums and the limiter ratios, in FP64 from the face fluxes A (FP32 in mixed precision)
 template <class T>
-__global__ void k_mp_cpcn(ColMesh M, MpScratchT<T> S, const T *__restrict__ psi1,
-                          const T *__restrict__ mx, const T *__restrict__ mn,
-                          const T *__restrict__ vol, const T *__restrict__ rh0, T dt,
-                          T *__restrict__ cp, T *__restrict__ cn) {
+__global__ void k_mp_cpcn(ColMesh M, MpScratchT<T> S, const double *__restrict__ psi1,
+                          const double *__restrict__ mx, const double *__restrict__ mn,
+                          const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
+                          double *__restrict__ cp, double *__restrict__ cn) {
     NODE_BEGIN
-    T rin = 0., rout = 0.;
+    double rin = 0., rout = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4T<T>{(f.vert ? S.Av : S.Ah)[f.si], T(0), T(0), T(0)}; },
-        [&](const Face &f, const V4T<T> &v) {
-            const T a = v.a;
-            const T pp = T(0) > a ? T(0) : a, pn = -(T(0) < a ? T(0) : a);
+        [&](const Face &f) { return V4{(double)(f.vert ? S.Av : S.Ah)[f.si], 0., 0., 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double a = v.a;
+            const double pp = 0. > a ? 0. : a, pn = -(0. < a ? 0. : a);
             if (!f.sub) { rin = rin + pn; rout = rout + pp; }
             else        { rin = rin + pp; rout = rout + pn; }
         });
-    const T tol = T(1.e-10);
-    const T p = psi1[n], v = vol[n], r = rh0[n];
+    const double tol = 1.e-10;
+    const double p = psi1[n], v = vol[n], r = rh0[n];
     cp[n] = (mx[n] - p) * v * r / (rin * dt + tol);
     cn[n] = (p - mn[n]) * v * r / (rout * dt + tol);
 }
@@ -229,22 +233,22 @@ __device__ __forceinline__ T tmin(T a, T b) { return a < b ? a : b; }
 
 template <class T>
 __global__ void k_mp_pass2(ColMesh M, MpScratchT<T> S, const T *__restrict__ psi1,
-                           const T *__restrict__ cp, const T *__restrict__ cn, MpUpdate U,
+                           const double *__restrict__ cp, const double *__restrict__ cn, MpUpdate U,
                            double *__restrict__ psi2) {
     NODE_BEGIN
-    const T cpn = cp[n], cnn = cn[n];
+    const double cpn = cp[n], cnn = cn[n];
     double arh2 = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4T<T>{(f.vert ? S.Av : S.Ah)[f.si], cp[f.j], cn[f.j], T(0)}; },
-        [&](const Face &f, const V4T<T> &v) {
-            const T a = v.a;
+        [&](const Face &f) { return V4{(double)(f.vert ? S.Av : S.Ah)[f.si], cp[f.j], cn[f.j], 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double a = v.a;
             // canonical ends: first = this node unless sub
-            const T cpa = f.sub ? v.b : cpn, cna = f.sub ? v.c : cnn;
-            const T cpb = f.sub ? cpn : v.b, cnb = f.sub ? cnn : v.c;
-            const T lim = a > T(0) ? a * tmin(tmin(T(1), cpb), cna) : a * tmin(tmin(T(1), cnb), cpa);
-            arh2 = f.sub ? arh2 - (double)lim : arh2 + (double)lim;
+            const double cpa = f.sub ? v.b : cpn, cna = f.sub ? v.c : cnn;
+            const double cpb = f.sub ? cpn : v.b, cnb = f.sub ? cnn : v.c;
+            const double lim = a > 0. ? a * tmin(tmin(1., cpb), cna) : a * tmin(tmin(1., cnb), cpa);
+            arh2 = f.sub ? arh2 - lim : arh2 + lim;
         });
-    if (has_boundary(M, c, k)) arh2 = arh2 + (double)(T(0) * T(1));
+    if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;
     const double p1 = U.psi1d ? U.psi1d[n] : (double)psi1[n];
     psi2[n] = p1 - arh2 * U.dt / U.vol[n] / U.rh0[n];
 }

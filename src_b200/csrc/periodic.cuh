@@ -145,17 +145,17 @@ __global__ void k_cp_velprd_grad(ColMesh M, CopyList CL, const double *__restric
 template <class T>
 __device__ __forceinline__ double donor_partial(const ColMesh &M, const MpScratchT<T> &S, const double *psi, int c,
                                                 int k, int n) {
-    const T pn = (T)psi[n];
+    const double pn = psi[n];
     double arh2 = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4T<T>{(f.vert ? S.aunv : S.aunh)[f.si], (T)psi[f.j], T(0), T(0)}; },
-        [&](const Face &f, const V4T<T> &v) {
-            const T aun = v.a;
-            const T pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
-            const T fl = pa * (T(0) > aun ? T(0) : aun) + pb * (T(0) < aun ? T(0) : aun);
-            arh2 = f.sub ? arh2 - (double)fl : arh2 + (double)fl;
+        [&](const Face &f) { return V4{(double)(f.vert ? S.aunv : S.aunh)[f.si], psi[f.j], 0., 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double aun = v.a;
+            const double pa = f.sub ? v.b : pn, pb = f.sub ? pn : v.b;
+            const double fl = pa * (0. > aun ? 0. : aun) + pb * (0. < aun ? 0. : aun);
+            arh2 = f.sub ? arh2 - fl : arh2 + fl;
         });
-    if (has_boundary(M, c, k)) arh2 = arh2 + (double)(T(0) * T(1));
+    if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;
     return arh2;
 }
 
@@ -191,26 +191,27 @@ template <class T> __device__ __forceinline__ T mx2(T a, T b) { return a > b ? a
 template <class T> __device__ __forceinline__ T mn2(T a, T b) { return a < b ? a : b; }
 
 // the FCT bounds over the periodic lists (ref.f:3821-3867), one thread per group, members in
-// order; a corner's minima are taken over unkmx as in the reference (ref.f:3853-3866)
-template <class T>
-__global__ void k_cp_bounds(CopyList CL, const T *__restrict__ psi1, T *__restrict__ mx, T *__restrict__ mn) {
+// order, on the FP64 first-pass field; a corner's minima are taken over unkmx as in the reference
+// (ref.f:3853-3866)
+__global__ void k_cp_bounds(CopyList CL, const double *__restrict__ psi1, double *__restrict__ mx,
+                            double *__restrict__ mn) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= CL.ngroups) return;
     const int32_t *m = CL.members + CL.grp[g];
     if (CL.grpsize[g] == 2) {
         const int i1 = m[0], i2 = m[1];
-        const T p1 = psi1[i1], p2 = psi1[i2];
+        const double p1 = psi1[i1], p2 = psi1[i2];
         mx[i1] = mx2(mx2(mx2(mx[i1], p1), p2), mx[i2]);
         mn[i1] = mn2(mn2(mn2(mn[i1], p1), p2), mn[i2]);
         mx[i2] = mx2(mx2(mx2(mx[i2], p1), p2), mx[i1]);
         mn[i2] = mn2(mn2(mn2(mn[i2], p1), p2), mn[i1]);
     } else {
-        const T p1 = psi1[m[0]], p2 = psi1[m[1]], p3 = psi1[m[2]], p4 = psi1[m[3]];
-        const T pmx = mx2(mx2(mx2(p1, p2), p3), p4), pmn = mn2(mn2(mn2(p1, p2), p3), p4);
+        const double p1 = psi1[m[0]], p2 = psi1[m[1]], p3 = psi1[m[2]], p4 = psi1[m[3]];
+        const double pmx = mx2(mx2(mx2(p1, p2), p3), p4), pmn = mn2(mn2(mn2(p1, p2), p3), p4);
         for (int q = 0; q < 4; ++q) {
-            const T u = mx2(mx2(mx2(mx[m[0]], mx[m[1]]), mx[m[2]]), mx[m[3]]);
+            const double u = mx2(mx2(mx2(mx[m[0]], mx[m[1]]), mx[m[2]]), mx[m[3]]);
             mx[m[q]] = mx2(u, pmx);
-            const T l = mn2(mn2(mn2(mx[m[0]], mx[m[1]]), mx[m[2]]), mx[m[3]]);
+            const double l = mn2(mn2(mn2(mx[m[0]], mx[m[1]]), mx[m[2]]), mx[m[3]]);
             mn[m[q]] = mn2(l, pmn);
         }
     }
@@ -218,61 +219,62 @@ __global__ void k_cp_bounds(CopyList CL, const T *__restrict__ psi1, T *__restri
 
 // in/out sums of one node over its own faces, as in k_mp_cpcn
 template <class T>
-__device__ __forceinline__ void cpcn_partial(const ColMesh &M, const MpScratchT<T> &S, int c, int k, int n, T &rin,
-                                             T &rout) {
+__device__ __forceinline__ void cpcn_partial(const ColMesh &M, const MpScratchT<T> &S, int c, int k, int n,
+                                             double &rin, double &rout) {
     rin = 0.; rout = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4T<T>{(f.vert ? S.Av : S.Ah)[f.si], T(0), T(0), T(0)}; },
-        [&](const Face &f, const V4T<T> &v) {
-            const T a = v.a;
-            const T pp = T(0) > a ? T(0) : a, pn = -(T(0) < a ? T(0) : a);
+        [&](const Face &f) { return V4{(double)(f.vert ? S.Av : S.Ah)[f.si], 0., 0., 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double a = v.a;
+            const double pp = 0. > a ? 0. : a, pn = -(0. < a ? 0. : a);
             if (!f.sub) { rin = rin + pn; rout = rout + pp; }
             else        { rin = rin + pp; rout = rout + pn; }
         });
 }
 
 template <class T>
-__global__ void k_cp_mp_cpcn(ColMesh M, CopyList CL, MpScratchT<T> S, const T *__restrict__ psi1,
-                             const T *__restrict__ mx, const T *__restrict__ mn, const T *__restrict__ vol,
-                             const T *__restrict__ rh0, T dt, T *__restrict__ cp, T *__restrict__ cn) {
+__global__ void k_cp_mp_cpcn(ColMesh M, CopyList CL, MpScratchT<T> S, const double *__restrict__ psi1,
+                             const double *__restrict__ mx, const double *__restrict__ mn,
+                             const double *__restrict__ vol, const double *__restrict__ rh0, double dt,
+                             double *__restrict__ cp, double *__restrict__ cn) {
     COPY_BEGIN
     (void)c; (void)k;
-    T rin = 0., rout = 0.;
+    double rin = 0., rout = 0.;
     for (int q = 0; q < gs; ++q) {
         const int x = mem[q], cx = x / M.L, kx = x - cx * M.L;
-        T a, b;
+        double a, b;
         cpcn_partial<T>(M, S, cx, kx, x, a, b);
         rin = q == 0 ? a : rin + a;
         rout = q == 0 ? b : rout + b;
     }
-    const T tol = T(1.e-10);
-    const T p = psi1[n], v = vol[n], r = rh0[n];
+    const double tol = 1.e-10;
+    const double p = psi1[n], v = vol[n], r = rh0[n];
     cp[n] = (mx[n] - p) * v * r / (rin * dt + tol);
     cn[n] = (p - mn[n]) * v * r / (rout * dt + tol);
 }
 
 // limited second-pass sum of one node over its own faces, as in k_mp_pass2
 template <class T>
-__device__ __forceinline__ double pass2_partial(const ColMesh &M, const MpScratchT<T> &S, const T *cp, const T *cn,
-                                                int c, int k, int n) {
-    const T cpn = cp[n], cnn = cn[n];
+__device__ __forceinline__ double pass2_partial(const ColMesh &M, const MpScratchT<T> &S, const double *cp,
+                                                const double *cn, int c, int k, int n) {
+    const double cpn = cp[n], cnn = cn[n];
     double arh2 = 0.;
     for_faces(M, c, k, n,
-        [&](const Face &f) { return V4T<T>{(f.vert ? S.Av : S.Ah)[f.si], cp[f.j], cn[f.j], T(0)}; },
-        [&](const Face &f, const V4T<T> &v) {
-            const T a = v.a;
-            const T cpa = f.sub ? v.b : cpn, cna = f.sub ? v.c : cnn;
-            const T cpb = f.sub ? cpn : v.b, cnb = f.sub ? cnn : v.c;
-            const T lim = a > T(0) ? a * tmin(tmin(T(1), cpb), cna) : a * tmin(tmin(T(1), cnb), cpa);
-            arh2 = f.sub ? arh2 - (double)lim : arh2 + (double)lim;
+        [&](const Face &f) { return V4{(double)(f.vert ? S.Av : S.Ah)[f.si], cp[f.j], cn[f.j], 0.}; },
+        [&](const Face &f, const V4 &v) {
+            const double a = v.a;
+            const double cpa = f.sub ? v.b : cpn, cna = f.sub ? v.c : cnn;
+            const double cpb = f.sub ? cpn : v.b, cnb = f.sub ? cnn : v.c;
+            const double lim = a > 0. ? a * tmin(tmin(1., cpb), cna) : a * tmin(tmin(1., cnb), cpa);
+            arh2 = f.sub ? arh2 - lim : arh2 + lim;
         });
-    if (has_boundary(M, c, k)) arh2 = arh2 + (double)(T(0) * T(1));
+    if (has_boundary(M, c, k)) arh2 = arh2 + 0. * 1.;
     return arh2;
 }
 
 template <class T>
 __global__ void k_cp_mp_pass2(ColMesh M, CopyList CL, MpScratchT<T> S, const T *__restrict__ psi1,
-                              const T *__restrict__ cp, const T *__restrict__ cn, MpUpdate U,
+                              const double *__restrict__ cp, const double *__restrict__ cn, MpUpdate U,
                               double *__restrict__ psi2) {
     COPY_BEGIN
     (void)c; (void)k;
