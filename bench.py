@@ -226,7 +226,7 @@ CPU_WORK_SAMPLE = "fp64_256x256x81"
 # costs into a per-step cost, because a single full-size step of the serial restatement takes
 # about 25 minutes (5 MPDATA fields and ~240 GCR iterations over 21.2M nodes).  The b200 arm's
 # cpu_baseline uses the count its own run measured instead.
-GCR_ITERS_PER_STEP = {"fp64_512x512x81": 239.9, "fp64_256x256x81": 150.0, "fp64_48x48x41": 130.0}
+GCR_ITERS_PER_STEP = {"fp64_512x512x81": 226.4, "fp64_256x256x81": 165.0, "fp64_48x48x41": 130.0}
 
 
 def cpu_sample(steps, warmup):
