@@ -711,6 +711,32 @@ def main():
                                                    "forward, corrects the vertical-line preconditioner"})
             sv.close()
 
+        # the learned correction on a hill it was not trained on: the 256x256x81 family's held-out
+        # seed, plain mixed vs learned + mixed with the committed weights (fallback threshold = the
+        # training run's plain contraction, so the network is kept while it contracts faster per
+        # iteration); guarded like the variants below
+        if base == 2:
+            try:
+                from src_b200 import learned, mesh as _mesh
+                from src_b200.cabi import RunParams
+                w_h, rate_h = learned.load_weights()
+                sd = learned.HELDOUT_SEED
+                rm_h = _mesh.generate(256, L=81, seed=sd, h0=learned.seed_h0(sd)).to_reference()
+                P_h = RunParams(delt=6.0, lord=3, eps0=1e-8, itr=200, itrp1=1, lipps=1, strat=0.01 ** 2 / 9.80616,
+                                nn_rate=rate_h, precision=1)
+                res = learned.compare(rm_h, P_h, w_h, steps=3, warm=1, device=local)
+                variants["learned_heldout_256x256x81"] = {
+                    "mesh": f"256x256x81, seed {sd} (not trained on), h0 = {learned.seed_h0(sd):.1f} m",
+                    "precision": "mixed, both paths",
+                    "first_solve_iters_plain": res["plain"]["first_solve_iters"],
+                    "first_solve_iters_learned": res["learned"]["first_solve_iters"],
+                    "ms_per_step_plain": round(res["plain"]["ms_per_step"], 2),
+                    "ms_per_step_learned": round(res["learned"]["ms_per_step"], 2),
+                    "fallbacks": res["learned"]["fallbacks"], "nn_rate": rate_h,
+                    "timing": "host wall clock around 3 synchronised steps after 1 warm-up"}
+            except Exception as exc:                      # reported, not fatal
+                variants["learned_heldout_256x256x81"] = {"error": f"{type(exc).__name__}: {exc}"[:300]}
+
         # laplc's own column blocks as the line preconditioner (iprc = 4), FP64 and mixed.  Run
         # last and guarded: a failure here is reported in the line instead of ending the run.
         for vname, prec in ((("column_blocks_fp64", 0), ("column_blocks_mixed", 1)) if base == 2 else ()):

@@ -87,20 +87,26 @@ def compare(refmesh, params: RunParams, weights, steps: int = 5, warm: int = 2, 
 
 
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "learned_weights.npz")
+HELDOUT_SEED = 8        # the training family uses seeds 0..7; seed 8 is never trained on
 
 
-def train_seeds(nx: int = 256, levels: int = 81, seeds=range(8), steps: int = 8, every: int = 4,
-                max_records: int = 48, epochs: int = 2, lr: float = 2e-3, dt: float = 6.0, device: int = 0,
+def seed_h0(seed: int) -> float:
+    """Hill height of seed `seed` in the training family: the seed-th draw of U(200, 600) m."""
+    rng = np.random.default_rng(1234)
+    return float(rng.uniform(200.0, 600.0, size=seed + 1)[seed])
+
+
+def train_seeds(nx: int = 256, levels: int = 81, seeds=range(8), steps: int = 100, every: int = 6,
+                max_records: int = 48, epochs: int = 1, lr: float = 2e-3, dt: float = 6.0, device: int = 0,
                 log=print):
     """Training run of the learned preconditioner on the 256x256x81 workload family: one mesh per
-    seed (jittered columns, Agnesi hill with h0 drawn uniformly from 200-600 m), plain solves
-    harvested for `steps` steps each, weights carried from seed to seed.  Returns
-    (weights, plain_rate, history)."""
+    seed (jittered columns, Agnesi hill with h0 drawn uniformly from 200-600 m), plain solves of
+    `steps` steps each harvested every `every`-th GCR iteration and trained on after every step,
+    weights carried from seed to seed.  Returns (weights, plain_rate, history)."""
     from . import mesh
-    rng = np.random.default_rng(1234)
     w, hist, rates = None, [], []
     for sd in seeds:
-        h0 = float(rng.uniform(200.0, 600.0))
+        h0 = seed_h0(int(sd))
         cm = mesh.generate(nx, L=levels, seed=int(sd), h0=h0)
         rm = cm.to_reference()
         P = RunParams(delt=dt, lord=3, eps0=1e-8, itr=200, iprc=2, itrp1=1, lipps=1,
@@ -131,28 +137,32 @@ if __name__ == "__main__":
     ap.add_argument("--nx", type=int, default=256)
     ap.add_argument("--levels", type=int, default=81)
     ap.add_argument("--seeds", type=int, default=8)
-    ap.add_argument("--steps", type=int, default=8)
-    ap.add_argument("--epochs", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--every", type=int, default=6)
+    ap.add_argument("--epochs", type=int, default=1)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--compare", action="store_true",
-                    help="instead of training: plain vs learned (saved weights) on one seeded mesh of this size")
+                    help="instead of training: plain vs learned (saved weights, mixed precision) on the held-out "
+                         "seed's mesh of this size")
+    ap.add_argument("--compare-seed", type=int, default=HELDOUT_SEED)
     a = ap.parse_args()
     if a.compare:
         from . import mesh
         w, rate = load_weights(a.out)
-        rm = mesh.generate(a.nx, L=a.levels, seed=0, h0=400.0).to_reference()
+        rm = mesh.generate(a.nx, L=a.levels, seed=a.compare_seed, h0=seed_h0(a.compare_seed)).to_reference()
         P = RunParams(delt=6.0, lord=3, eps0=1e-8, itr=200, itrp1=1, lipps=1, strat=0.01 ** 2 / 9.80616,
-                      nn_rate=rate)
+                      nn_rate=rate, precision=1)
         res = compare(rm, P, w, steps=3, warm=1)
         du = float(np.abs(res["learned"]["u"] - res["plain"]["u"]).max())
         print(json.dumps({k: {kk: vv for kk, vv in v.items() if kk != "u"} for k, v in res.items()} |
                          {"max_abs_du": du, "nn_rate": rate}), flush=True)
         raise SystemExit(0)
     t0 = time.time()
-    w, rate, hist = train_seeds(a.nx, a.levels, range(a.seeds), a.steps, epochs=a.epochs, lr=a.lr,
+    w, rate, hist = train_seeds(a.nx, a.levels, range(a.seeds), a.steps, every=a.every, epochs=a.epochs, lr=a.lr,
                                 log=lambda e: print(json.dumps(e), flush=True))
-    meta = {"nx": a.nx, "levels": a.levels, "seeds": a.seeds, "steps": a.steps, "epochs": a.epochs, "lr": a.lr,
+    meta = {"nx": a.nx, "levels": a.levels, "seeds": a.seeds, "steps": a.steps, "every": a.every,
+            "epochs": a.epochs, "lr": a.lr,
             "pairs": int(sum(h["pairs"] for h in hist)), "train_s": round(time.time() - t0, 1)}
     save_weights(a.out, w, rate, meta)
     print(json.dumps({"saved": a.out, "plain_rate": rate, **meta}), flush=True)
