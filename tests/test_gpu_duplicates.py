@@ -102,26 +102,35 @@ def test_gcrk_and_steps_bitwise(dup):
 
 
 def test_mixed_precision_duplicate_form(dup):
-    """FP32 operator, directions and MPDATA fluxes on the duplicate form: within the mixed path's
-    tolerances of the FP64 oracle (3e-6 for u on these small meshes), the scalar non-negative.
+    """FP32 operator, directions and MPDATA fluxes on the duplicate form, against the FP64 oracle;
+    the scalar stays non-negative.  On these small meshes the pressure solve stops at the
+    iteration limit (8x8x9) or just under eps0, so where it stops moves the small fields: the
+    FP64 oracle's own v, w, theta' change by up to 7e-4 when eps0 goes from 1e-8 to 1e-9.  The
+    bound for each small field is therefore three times that change (at least 1e-4).
     (The sum of vol*rh0*psi over all nodes is not an invariant of this form: every copy carries
     its group's summed volume and edge sums, so the FP64 reference does not conserve it either.)"""
     rm, _, _ = dup
-    o = Oracle(RunParams(delt=10.0, nscal=1), rm)
-    o.setup()
     x, y, z = rm.coord.T
     g = np.exp(-((x - 30e3) ** 2 + (y - 60e3) ** 2 + (z - 5e3) ** 2) / (2 * 5e3 ** 2))
-    o.set(F_UNK + 4, g)
+    ref = {}
+    for eps0 in (1e-8, 1e-9):
+        o = Oracle(RunParams(delt=10.0, nscal=1, eps0=eps0), rm)
+        o.setup()
+        o.set(F_UNK + 4, g)
+        for _ in range(3):
+            o.step()
+        ref[eps0] = [o.get(F_UNK + k) for k in range(5)]
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
     with Solver(RunParams(delt=10.0, nscal=1, precision=1), rm) as s:
         s.setup()
         s.set(F_UNK + 4, g)
         for _ in range(3):
-            o.step()
             d = s.step()
-        rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)
-        assert rel(s.get(F_UNK), o.get(F_UNK)) <= 3e-6
+        assert rel(s.get(F_UNK), ref[1e-8][0]) <= 3e-6
         for k in (1, 2, 3):
-            assert rel(s.get(F_UNK + k), o.get(F_UNK + k)) <= 1e-4, k
+            tol = max(1e-4, 3.0 * rel(ref[1e-9][k], ref[1e-8][k]))
+            assert rel(s.get(F_UNK + k), ref[1e-8][k]) <= tol, (k, tol)
+        assert rel(s.get(F_UNK + 4), ref[1e-8][4]) <= 1e-6
         assert d.smin[0] >= 0.0
 
 
