@@ -98,6 +98,7 @@ def algorithmic_bytes(cls, N, Eh, Ev):
     table = {
         "lap_grad": 56 * N + 24 * E,      # p, vol, rh0, coefw in; S; Fx, Fy, Fz out
         "lap_div": 48 * N + 24 * E,       # Fx, Fy, Fz, vol, rh0 in; S; alap out
+        "laplc": 40 * N + 24 * E,         # both halves in one launch: p, vol, rh0, coefw in; S; alap out
         "prfr": 72 * N + 24 * E,          # p, u*, v*, w*, vol, coefw in; S; u, v, w out
         "div": 48 * N + 24 * E,           # u, v, w, vol, rh0 in; S; rhs out
         "line_solve": 40 * N,             # rhs, a, m, c' in; p out
@@ -114,7 +115,7 @@ def algorithmic_bytes(cls, N, Eh, Ev):
 
 def rule_bytes(cls, N, Eh, Ev, b=8):
     """Algorithmic bytes per launch by the workload's counting rule for the reference's
-    operators, b bytes per value: a gradient G or divergence D moves (8+3b)E + 6bN, prfr
+    operators, b bytes per value: a gradient G or divergence D moves (8+3b)E + 6bN, laplc G + D, prfr
     (8+3b)E + 9bN, the line solve 5bN.  The 8 bytes per face are the reference's two int32 edge
     indices, which the column layout does not read (it derives neighbours from a per-column
     adjacency list), so for the edge kernels these bytes exceed what the kernel must move;
@@ -123,6 +124,7 @@ def rule_bytes(cls, N, Eh, Ev, b=8):
     table = {
         "lap_grad": (8 + 3 * b) * E + 6 * b * N,
         "lap_div": (8 + 3 * b) * E + 6 * b * N,
+        "laplc": 2 * ((8 + 3 * b) * E + 6 * b * N),     # laplc = G + D
         "div": (8 + 3 * b) * E + 6 * b * N,
         "prfr": (8 + 3 * b) * E + 9 * b * N,
         "line_solve": 5 * b * N,
@@ -417,14 +419,16 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def workload_config(name):
+def workload_config(name, iprc=None):
     nx, L, dt, h0, lord, nscal = WORKLOADS[name]
+    if iprc is None:
+        iprc = WORKLOAD_EXTRA.get(name, {}).get("iprc", 2)
     return {"workload": f"plain FP64 MPDATA+GCR step, {nx}x{nx} jittered periodic columns x {L} levels "
                         f"({nx * nx * L} nodes), Agnesi hill h0={h0:g} m, dt={dt:g} s",
             "nodes": nx * nx * L, "edges": 3 * nx * nx * L + nx * nx * (L - 1), "levels": L, "dt_s": dt,
             "gcr": f"GCR({lord}) to max|r|*dt<=1e-8, " + (
-                "laplc's column blocks as the line preconditioner" if WORKLOAD_EXTRA.get(name, {}).get("iprc") == 4
-                else "vertical-line preconditioner"),
+                "laplc's column blocks as the line preconditioner" if iprc == 4
+                else "vertical-line preconditioner" if iprc == 2 else f"preconditioner iprc={iprc}"),
             **({"levels_stretched_lowest_dz_m": WORKLOAD_EXTRA[name]["stretch_dz0"],
                 "N_per_s": WORKLOAD_EXTRA[name]["N"]} if name in WORKLOAD_EXTRA else {}),
             "mpdata": "iord=2 + nonoscillatory (FCT)", "passive_scalars": nscal,
@@ -488,6 +492,8 @@ def main():
     ap.add_argument("--ref-sample", default=CPU_WORK_SAMPLE, choices=sorted(WORKLOADS),
                     help="--impl reference and the CPU baseline: mesh on which the step's components are timed")
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--iprc", type=int, default=None, choices=[1, 2, 4],
+                    help="preconditioner of the plain path (default: the workload's own)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-variants", action="store_true", help="skip the mixed-precision variant")
@@ -517,6 +523,8 @@ def main():
     name = args.workload
     cm, rm = build_mesh(name)
     P = build_params(name)
+    if args.iprc is not None:
+        P.iprc = args.iprc
     s = Solver(P, rm, device=local)
     info = s.info()
     d0 = s.setup()
@@ -821,7 +829,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": workload_config(name),
+                "config": workload_config(name, P.iprc),
                 "ms_per_pressure_solve": round(ms_solve, 3),
                 "gcr_iters_per_solve": round(float(np.mean([a for p in iters for a in p])), 2),
                 "gcr_iters_first_solve": round(float(np.mean([p[0] for p in iters])), 2),

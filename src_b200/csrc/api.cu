@@ -2,6 +2,7 @@
 // reference subroutines on device-resident fields, and the mpsolver driver.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <type_traits>
@@ -32,11 +33,13 @@ extern "C" const char *mpg_last_error(void) { return g_err.c_str(); }
 // ------------------------------------------------------------------------------ kernel timing
 enum KClass {
     KT_LAP_GRAD, KT_LAP_DIV, KT_PRFR, KT_DIV, KT_LINE, KT_REDUCE, KT_GCR_UPD, KT_AUN, KT_MP_DONOR,
-    KT_MP_GRADB, KT_MP_ANTI, KT_MP_CPCN, KT_MP_PASS2, KT_NODE, KT_COURANT, KT_MISC, KT_NN, KT_SOLVE, KT_COUNT
+    KT_MP_GRADB, KT_MP_ANTI, KT_MP_CPCN, KT_MP_PASS2, KT_NODE, KT_COURANT, KT_MISC, KT_NN, KT_SOLVE, KT_LAPLC,
+    KT_COUNT
 };
 static const char *kKNames[KT_COUNT] = {
     "lap_grad", "lap_div", "prfr", "div", "line_solve", "reduce", "gcr_update", "aun", "mp_donor",
-    "mp_grad_bounds", "mp_anti", "mp_cpcn", "mp_pass2", "node_loops", "courant", "misc", "learned", "pressure_solve"};
+    "mp_grad_bounds", "mp_anti", "mp_cpcn", "mp_pass2", "node_loops", "courant", "misc", "learned", "pressure_solve",
+    "laplc"};
 
 struct KTimer {
     bool on = false;
@@ -107,6 +110,8 @@ struct mpg_solver {
     double *mg_rrhs = nullptr, *mg_e = nullptr;          // fine-mesh arrays of the V-cycle
     bool borrowed_stream = false;                        // a coarse level runs on its parent's stream
     CopyList CL{};                                       // periodic copy groups (duplicate-node form)
+    LapSched lap{};                                      // fused laplc's work order (total 0: two launches)
+    int lap_ctas[2] = {0, 0};                            // its persistent grid, FP64 and FP32 instantiations
     // kept for the V-cycle's set-up when mg_flag = 1 (and on a coarse level's handle): the mesh's
     // neighbour lists in neigh_definition order and its coordinates, reference numbering
     std::vector<int32_t> nb_ptr_ref, nb_lst_ref;
@@ -268,9 +273,44 @@ template <> struct Buf<float> {
     static const float *coefw(mpg_handle h) { return h->coefwf; }
 };
 
+// the fused kernel's grid: every block resident at once (one persistent block per slot)
+template <class T>
+int lap_fused_ctas(mpg_handle h) {
+    int &n = h->lap_ctas[std::is_same<T, float>::value ? 1 : 0];
+    if (!n) {
+        int sms = 0, per_sm = 0;
+        MPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev));
+        MPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lap_fused<T>, kThreads, 0));
+        n = std::max(1, sms) * std::max(1, per_sm);
+    }
+    return MPG_OK;
+}
+
+// the fused laplc's wait gave up (never expected: every awaited item has started): report it once
+int lap_fused_check(mpg_handle h) {
+    if (!h->lap.total) return MPG_OK;
+    int32_t e = 0;
+    MPG_CUDA(cudaMemcpyAsync(&e, h->lap.state + 3, sizeof e, cudaMemcpyDeviceToHost, h->st));
+    MPG_CUDA(cudaStreamSynchronize(h->st));
+    if (e) {
+        MPG_CUDA(cudaMemsetAsync(h->lap.state + 3, 0, sizeof e, h->st));
+        return mpg_fail(MPG_ERR_CUDA, "laplc: a wait for gradient fluxes gave up; the result is not valid");
+    }
+    return MPG_OK;
+}
+
 template <class T>
 int op_laplc_t(mpg_handle h, const T *p, T *alap, int impfl) {
     using B = Buf<T>;
+    if (h->lap.total) {
+        int rc;
+        if ((rc = lap_fused_ctas<T>(h))) return rc;
+        KTIME(KT_LAPLC);
+        k_lap_fused<T><<<h->lap_ctas[std::is_same<T, float>::value ? 1 : 0], kThreads, 0, h->st>>>(
+            h->M, (h->L + 1) / 2, h->lap, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue, (T)h->P.delt, impfl, B::F(h),
+            alap);
+        return check_launch("laplc");
+    }
     {
         KTIME(KT_LAP_GRAD);
         k_lap_grad<T><<<grid(h->N), kThreads, 0, h->st>>>(h->M, p, B::vol(h), B::rh0(h), B::coefw(h), h->ue,
@@ -1305,6 +1345,7 @@ int op_gcrk_t(mpg_handle h, double *p, const double *u1, const double *v1, const
     h->nitsm = h->nitsm + nlc;
     h->icount = h->icount + 1;
     h->gstatus = status;
+    if ((rc = lap_fused_check(h))) return rc;
     h->dvmx_last = dvmx;
     h->rl2_last = rl2;
     return MPG_OK;
@@ -1795,6 +1836,24 @@ extern "C" int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int d
         CL.ngroups = (int32_t)hm.cp_grp.size();
         CL.grp = e2; CL.grpsize = f2;
     }
+    // MPG_LAPLC_FUSED=1: laplc's two halves in one persistent launch (k_lap_fused), not with copy
+    // lists (their fix-up runs between the halves).  Bit-identical; measured slower than the two
+    // launches on the 21.2M-node workload, hence not the default.
+    const char *fused = std::getenv("MPG_LAPLC_FUSED");
+    if (hm.cp_node.empty() && fused && fused[0] == '1') {
+        // a divergence item's ticket comes one grid's worth of items after its last dependency
+        if ((rc = lap_fused_ctas<double>(h)) || (rc = lap_fused_ctas<float>(h))) return fail(rc);
+        std::vector<int32_t> sched, dptr;
+        std::vector<int2> drng;
+        const int32_t NG = mpg_laplc_schedule(hm, kThreads, std::max(h->lap_ctas[0], h->lap_ctas[1]), sched,
+                                              dptr, drng);
+        int32_t *a, *b, *f, *st;
+        int2 *r;
+        if ((rc = upload(h, &a, sched)) || (rc = upload(h, &b, dptr)) || (rc = upload(h, &r, drng)) ||
+            (rc = dalloc(h, &f, (size_t)NG)) || (rc = dalloc(h, &st, 4)))
+            return fail(rc);
+        h->lap = LapSched{a, b, r, f, st, (int32_t)sched.size()};
+    }
     if (prm->mg_flag == 1) {
         mg_neigh_definition(mesh, h->nb_ptr_ref, h->nb_lst_ref);
         mg_coords(mesh, h->cx_ref, h->cy_ref, h->cz_ref);
@@ -1950,7 +2009,7 @@ extern "C" int mpg_get_field(mpg_handle h, int fid, double *dst) {
     if (rc) return rc;
     MPG_CUDA(cudaMemcpyAsync(dst, h->stage, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->st));
     MPG_CUDA(cudaStreamSynchronize(h->st));
-    return MPG_OK;
+    return lap_fused_check(h);
 }
 
 extern "C" int mpg_derivative(mpg_handle h, int unk, int out, int idx) {

@@ -106,16 +106,24 @@ template <> struct FaceVec<float> {
 // the three flux components between the halves of laplc: three FP64 arrays, or one packed
 // float4 per node in mixed precision (one 16-byte load per neighbour)
 template <class T> struct Flux;
+// (load_cg reads through L2 only: for fluxes written by other blocks of the same launch)
 template <> struct Flux<double> {
     double *x, *y, *z;
     __device__ void store(int n, double a, double b, double c) const { x[n] = a; y[n] = b; z[n] = c; }
     __device__ void load(int n, double &a, double &b, double &c) const { a = x[n]; b = y[n]; c = z[n]; }
+    __device__ void load_cg(int n, double &a, double &b, double &c) const {
+        a = __ldcg(x + n); b = __ldcg(y + n); c = __ldcg(z + n);
+    }
 };
 template <> struct Flux<float> {
     float4 *v;
     __device__ void store(int n, float a, float b, float c) const { v[n] = make_float4(a, b, c, 0.f); }
     __device__ void load(int n, float &a, float &b, float &c) const {
         const float4 t = v[n];
+        a = t.x; b = t.y; c = t.z;
+    }
+    __device__ void load_cg(int n, float &a, float &b, float &c) const {
+        const float4 t = __ldcg(v + n);
         a = t.x; b = t.y; c = t.z;
     }
 };
@@ -273,13 +281,14 @@ __global__ void k_bcv(ColMesh M, double *u, double *v, double *w, const double *
     u[n] = a; v[n] = b; w[n] = d;
 }
 
-// laplc first half (ref.f:1303-1338): gradient, scaling, bcv(.,0.), times rh0.  T is the
-// storage and arithmetic type (double; float for the mixed-precision solve).
+// laplc first half (ref.f:1303-1338) at node n: gradient, scaling, bcv(.,0.), times rh0.  T is
+// the storage and arithmetic type (double; float for the mixed-precision solve).
 template <class T>
-__global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const T *__restrict__ p, const T *__restrict__ vol,
-                                         const T *__restrict__ rh0, const T *__restrict__ coefw,
-                                         const double *__restrict__ ue, T dt, int impfl, Flux<T> F) {
-    NODE_BEGIN
+__device__ __forceinline__ void lap_grad_node(const ColMesh &M, int n, const T *__restrict__ p,
+                                              const T *__restrict__ vol, const T *__restrict__ rh0,
+                                              const T *__restrict__ coefw, const double *__restrict__ ue, T dt,
+                                              int impfl, const Flux<T> &F) {
+    const int c = n / M.L, k = n - c * M.L;
     T gx, gy, gz;
     grad3<T>(M, p, c, k, n, gx, gy, gz);
     const T v = vol[n];
@@ -290,6 +299,15 @@ __global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const T *__restrict__ p, con
     bcv_node<T>(M, c, k, n, ue, 0.0, dx, dy, dz);
     const T r = rh0[n];
     F.store(n, dx * r, dy * r, dz * r);
+}
+
+template <class T>
+__global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const T *__restrict__ p, const T *__restrict__ vol,
+                                         const T *__restrict__ rh0, const T *__restrict__ coefw,
+                                         const double *__restrict__ ue, T dt, int impfl, Flux<T> F) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M.N) return;
+    lap_grad_node<T>(M, n, p, vol, rh0, coefw, ue, dt, impfl, F);
 }
 
 // laplc second half (ref.f:1339-1350): alap = (Dx(Fx) + Dy(Fy) + Dz(Fz)) / (vol*rh0)
@@ -334,27 +352,31 @@ __device__ __forceinline__ Face2 decode_face2(int2 en, int n0, int k0, int L, bo
 // 64 registers: the two nodes' operands of a face in flight together
 constexpr int kLapPairMinBlocks = 4;
 
-template <class T>
-__global__ void __launch_bounds__(kThreads, kLapPairMinBlocks)
-k_lap_div2(ColMesh M, int PL, const Flux<T> F, const T *__restrict__ vol, const T *__restrict__ rh0,
-           T *__restrict__ alap) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= M.NC * PL) return;
+// level pair t of laplc's second half; CG: the fluxes were written by other blocks of the same
+// launch (read through L2)
+template <class T, bool CG = false>
+__device__ __forceinline__ void lap_div_pair(const ColMesh &M, int PL, int t, const Flux<T> &F,
+                                             const T *__restrict__ vol, const T *__restrict__ rh0,
+                                             T *__restrict__ alap) {
     const int c = t / PL, L = M.L, k0 = 2 * (t - c * PL), n0 = c * L + k0;
     const bool two = k0 + 1 < L;
+    auto fl = [&](int n, T &a, T &b, T &d) {
+        if (CG) F.load_cg(n, a, b, d);
+        else F.load(n, a, b, d);
+    };
     T f0x, f0y, f0z, f1x = 0., f1y = 0., f1z = 0.;
-    F.load(n0, f0x, f0y, f0z);
-    if (two) F.load(n0 + 1, f1x, f1y, f1z);
+    fl(n0, f0x, f0y, f0z);
+    if (two) fl(n0 + 1, f1x, f1y, f1z);
     T a0x = 0., a0y = 0., a0z = 0., a1x = 0., a1y = 0., a1z = 0.;
     const int beg = __ldg(&M.cptr[c]), end = __ldg(&M.cptr[c + 1]);
     for (int j = beg; j < end; ++j) {
         const Face2 f = decode_face2(__ldg(&M.cadj[j]), n0, k0, L, two);
         T sx0, sy0, sz0, sx1 = 0., sy1 = 0., sz1 = 0., g0x, g0y, g0z, g1x = 0., g1y = 0., g1z = 0.;
         FaceVec<T>::load(M, f.vert, f.s0, sx0, sy0, sz0);
-        F.load(f.j0, g0x, g0y, g0z);
+        fl(f.j0, g0x, g0y, g0z);
         if (two) {
             FaceVec<T>::load(M, f.vert, f.s1, sx1, sy1, sz1);
-            F.load(f.j1, g1x, g1y, g1z);
+            fl(f.j1, g1x, g1y, g1z);
         }
         if (f.v0) {
             const T tx = sx0 * ((f0x + g0x) * T(0.5));
@@ -386,6 +408,124 @@ k_lap_div2(ColMesh M, int PL, const Flux<T> F, const T *__restrict__ vol, const 
             });
         }
         alap[n] = (dx + dy + dz) / (vol[n] * rh0[n]);
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads, kLapPairMinBlocks)
+k_lap_div2(ColMesh M, int PL, const Flux<T> F, const T *__restrict__ vol, const T *__restrict__ rh0,
+           T *__restrict__ alap) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= M.NC * PL) return;
+    lap_div_pair<T>(M, PL, t, F, vol, rh0, alap);
+}
+
+// ------------------------------------------------------------------------------ fused laplc
+// Both halves of laplc in one persistent launch.  The work is cut into gradient items (kThreads
+// consecutive nodes each, k_lap_grad's blocks) and divergence items (kThreads level pairs each,
+// k_lap_div2's blocks).  Blocks take tickets from a counter in order; `sched` maps ticket to item
+// and places every divergence item after the last gradient item it reads, so a divergence item
+// runs while the fluxes and face vectors it reads are still in L2 from the gradient pass a few
+// hundred items earlier, instead of a second full sweep over HBM.  Before reading, a divergence
+// item waits for the flags of the gradient items in its dependency ranges.  Every such item
+// holds an earlier ticket, so the block working on it has started and needs nothing else: the
+// wait always ends.  The wait is bounded all the same; when it gives up it records an error in
+// state[3] and the item goes ahead (the host reports the error).  Each node's arithmetic is
+// k_lap_grad's and k_lap_div2's, so the result is bit-identical to the two-launch form.
+// Measured at 512x512x81 (FP64): 2.00 ms per laplc against 1.71 ms for the two launches, although
+// DRAM traffic falls by 43% (L2 hit rate 65%).  The gathers are latency-bound, and the kernel's
+// 64 registers (the divergence's) hold the gradient items to 32 warps per SM where k_lap_grad
+// runs 48.  The library therefore launches the two halves unless MPG_LAPLC_FUSED=1 at creation.
+//
+// state: [0] next ticket, [1] blocks finished, [2] launches completed (the epoch), [3] error.
+// The last block to finish resets [0] and [1] and advances [2], so the next launch on the
+// stream starts from a clean counter; gradient flags hold the epoch of the launch that wrote them.
+struct LapSched {
+    const int32_t *sched;    // [total] item per ticket: g >= 0 gradient item g, -(d+1) divergence item d
+    const int32_t *dptr;     // [ND+1] dependency ranges of each divergence item
+    const int2 *drng;        // inclusive ranges of gradient items
+    int32_t *flag;           // [NG]
+    int32_t *state;          // [4]
+    int32_t total;
+};
+
+__device__ __forceinline__ int ld_acquire_gpu(const int32_t *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int32_t *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+#ifndef MPG_LAPF_SPINS
+#define MPG_LAPF_SPINS (1LL << 22)
+#endif
+#ifndef MPG_LAPF_MINB
+#define MPG_LAPF_MINB 4
+#endif
+
+template <class T>
+__global__ void __launch_bounds__(kThreads, MPG_LAPF_MINB)
+k_lap_fused(ColMesh M, int PL, LapSched S, const T *__restrict__ p, const T *__restrict__ vol,
+            const T *__restrict__ rh0, const T *__restrict__ coefw, const double *__restrict__ ue, T dt,
+            int impfl, Flux<T> F, T *__restrict__ alap) {
+    __shared__ int s_ticket[2];
+    __shared__ int s_epoch;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_epoch = *(volatile int32_t *)&S.state[2] + 1;
+        s_ticket[0] = atomicAdd(&S.state[0], 1);
+    }
+    __syncthreads();
+    const int epoch = s_epoch;
+    const int NP = M.NC * PL;
+    for (int buf = 0;; buf ^= 1) {
+        const int ticket = s_ticket[buf];
+        if (ticket >= S.total) break;
+        if (tid == 0) s_ticket[buf ^ 1] = atomicAdd(&S.state[0], 1);   // in flight during this item
+        const int item = __ldg(&S.sched[ticket]);
+        if (item >= 0) {
+            const int n = item * kThreads + tid;
+            if (n < M.N) lap_grad_node<T>(M, n, p, vol, rh0, coefw, ue, dt, impfl, F);
+            // the barrier orders every thread's flux stores before thread 0's release, which is
+            // cumulative: a block that acquires the flag sees all of them (one release per item;
+            // a fence in every thread serialises the SM)
+            __syncthreads();
+            if (tid == 0) st_release_gpu(&S.flag[item], epoch);
+        } else {
+            const int d = -item - 1;
+            // warp 0 acquires the flags of the gradient items this item reads; the barrier then
+            // passes the acquired fluxes on to the whole block
+            if (tid < 32) {
+                bool ok = true;
+                const int rb = __ldg(&S.dptr[d]), re = __ldg(&S.dptr[d + 1]);
+                for (int r = rb; r < re; ++r) {
+                    const int2 g = __ldg(&S.drng[r]);
+                    for (int i = g.x + tid; i <= g.y; i += 32) {
+                        long long spins = 0;
+                        while (ld_acquire_gpu(&S.flag[i]) != epoch) {
+                            if (++spins > MPG_LAPF_SPINS) { ok = false; break; }
+                            __nanosleep(64);
+                        }
+                    }
+                }
+                if (__any_sync(0xffffffffu, !ok) && tid == 0) atomicExch(&S.state[3], 1);
+            }
+            __syncthreads();
+            const int t = d * kThreads + tid;
+            if (t < NP) lap_div_pair<T, true>(M, PL, t, F, vol, rh0, alap);
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&S.state[1], 1) == (int)gridDim.x - 1) {
+            atomicExch(&S.state[0], 0);
+            atomicExch(&S.state[1], 0);
+            __threadfence();
+            atomicAdd(&S.state[2], 1);
+        }
     }
 }
 

@@ -84,6 +84,16 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out);
 // ref.f:99-103): vol of every node, with each group's members replaced by their sum
 std::vector<double> mpg_periodic_volumes(const mpg_mesh_ref *m);
 
+// Order of the fused laplc's work items (gradient items of `per` consecutive nodes, divergence
+// items of `per` level pairs; PL = (L + 1) / 2 pairs per column).  Returns the number of gradient
+// items.  `sched` lists every item once,
+// gradient items in node order, each divergence item (encoded -(d+1)) `lag` gradient items after
+// the last one whose fluxes it reads (or at the end), so that by the time its ticket is drawn the
+// blocks in flight have moved on from its dependencies; dptr/drng give each divergence item's
+// gradient items as merged inclusive ranges.
+int32_t mpg_laplc_schedule(const HostColumnMesh &cm, int per, int lag, std::vector<int32_t> &sched,
+                           std::vector<int32_t> &dptr, std::vector<int2> &drng);
+
 // Static per-node quantities computed on the host at creation (internal order), restating the
 // set-up part of mpsolver: rhprof/thprof, absorbers, beta_timestep_unstr, compute_d_unstr,
 // ambient state, coefw and the vertical-line preconditioner coefficients.

@@ -674,3 +674,47 @@ void mpg_wide_coeffs(const mpg_params *P, const mpg_mesh_ref *m, const HostColum
             }
     }
 }
+
+int32_t mpg_laplc_schedule(const HostColumnMesh &cm, int per, int lag, std::vector<int32_t> &sched,
+                           std::vector<int32_t> &dptr, std::vector<int2> &drng) {
+    const int64_t L = cm.L, PL = (cm.L + 1) / 2, NP = (int64_t)cm.NC * PL;
+    const int32_t NG = (int32_t)((cm.N + per - 1) / per), ND = (int32_t)((NP + per - 1) / per);
+    dptr.assign(1, 0);
+    drng.clear();
+    std::vector<int32_t> last(ND);
+    std::vector<int2> r;
+    for (int32_t d = 0; d < ND; ++d) {
+        const int64_t t0 = (int64_t)d * per, t1 = std::min<int64_t>(NP, t0 + per);
+        const int32_t c0 = (int32_t)(t0 / PL), c1 = (int32_t)((t1 - 1) / PL);
+        r.clear();
+        auto need = [&](int32_t col) {      // every level of column col
+            r.push_back(make_int2((int32_t)(col * L / per), (int32_t)(((int64_t)col * L + L - 1) / per)));
+        };
+        for (int32_t c = c0; c <= c1; ++c) {
+            need(c);
+            for (int32_t j = cm.cptr[c]; j < cm.cptr[c + 1]; ++j)
+                if (cm.cadj[j].x >= 0) need(cm.cadj[j].y);
+        }
+        std::sort(r.begin(), r.end(), [](int2 a, int2 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); });
+        int2 cur = r[0];
+        for (size_t i = 1; i < r.size(); ++i) {
+            if (r[i].x <= cur.y + 1) cur.y = std::max(cur.y, r[i].y);
+            else { drng.push_back(cur); cur = r[i]; }
+        }
+        drng.push_back(cur);
+        last[d] = std::min(NG - 1, cur.y + std::max(lag, 0));
+        dptr.push_back((int32_t)drng.size());
+    }
+    // gradient items in order; each divergence item `lag` gradient items after its last dependency
+    std::vector<int32_t> order(ND);
+    for (int32_t d = 0; d < ND; ++d) order[d] = d;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return last[a] < last[b]; });
+    sched.clear();
+    sched.reserve((size_t)NG + ND);
+    size_t q = 0;
+    for (int32_t g = 0; g < NG; ++g) {
+        sched.push_back(g);
+        while (q < order.size() && last[order[q]] == g) sched.push_back(-(order[q++] + 1));
+    }
+    return NG;
+}

@@ -106,12 +106,20 @@ def test_mixed_precision_duplicate_form(dup):
     the scalar stays non-negative.  On these small meshes the pressure solve stops at the
     iteration limit (8x8x9) or just under eps0, so where it stops moves the small fields: the
     FP64 oracle's own v, w, theta' change by up to 7e-4 when eps0 goes from 1e-8 to 1e-9.  The
-    bound for each small field is therefore three times that change (at least 1e-4).
+    bound for each small field is therefore three times that change (at least 1e-4).  The scalar
+    starts as a periodic bump, equal on the copies of every seam node.
     (The sum of vol*rh0*psi over all nodes is not an invariant of this form: every copy carries
     its group's summed volume and edge sums, so the FP64 reference does not conserve it either.)"""
     rm, _, _ = dup
+    # a periodic bump: both copies of a seam node start with the same value, as the duplicate form
+    # requires (a bump by plain coordinates gives the x = 0 and x = Lx copies different values, and
+    # then the FP64 reference's scalar goes negative at the seam as well)
     x, y, z = rm.coord.T
-    g = np.exp(-((x - 30e3) ** 2 + (y - 60e3) ** 2 + (z - 5e3) ** 2) / (2 * 5e3 ** 2))
+    Lx, Ly = x.max() - x.min(), y.max() - y.min()
+    dx = np.abs(x - 30e3)
+    dy = np.abs(y - 60e3)
+    dx, dy = np.minimum(dx, Lx - dx), np.minimum(dy, Ly - dy)
+    g = np.exp(-(dx ** 2 + dy ** 2 + (z - 5e3) ** 2) / (2 * 5e3 ** 2))
     ref = {}
     for eps0 in (1e-8, 1e-9):
         o = Oracle(RunParams(delt=10.0, nscal=1, eps0=eps0), rm)
