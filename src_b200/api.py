@@ -179,8 +179,13 @@ class Solver:
         a = np.ascontiguousarray(np.broadcast_to(np.asarray(values, np.float64), (self.n,)))
         _check(self.L.mpg_set_field(self.h, fid, a.ctypes.data))
 
-    def get(self, fid: int) -> np.ndarray:
-        out = np.empty(self.n)
+    def get(self, fid: int, out: np.ndarray = None) -> np.ndarray:
+        """Field `fid` in reference node order, into `out` when given (a C-contiguous float64
+        array of npoin values; pass pinned host memory for a full-bandwidth copy)."""
+        if out is None:
+            out = np.empty(self.n)
+        elif out.dtype != np.float64 or out.shape != (self.n,) or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a C-contiguous float64 array of npoin values")
         _check(self.L.mpg_get_field(self.h, fid, out.ctypes.data))
         return out
 

@@ -612,6 +612,17 @@ __global__ void k_div(ColMesh M, const double *__restrict__ ua, const double *__
 }
 
 // ------------------------------------------------------------------------------ line solve
+// The forward-sweep values d are scratch: each is read once, by the lane that wrote it, in the
+// backward sweep.  After a chunk's backward sweep the warp drops the chunk's lines of d from L2
+// (discard.global.L2: no write-back), so the scratch stays off DRAM when its lines are still in
+// L2.  Level k of the warp's 32 columns is one 256-byte segment (line_index), two 128-byte lines.
+__device__ __forceinline__ void discard_line_chunk(double *dbuf, int col0, int k0, int nk, int L, int lane) {
+    for (int i = lane; i < 2 * nk; i += 32) {
+        const double *a = dbuf + line_index(col0, k0 + (i >> 1), L) + 16 * (i & 1);
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(a) : "memory");
+    }
+}
+
 // z = M^{-1} rhs per column (Thomas, FP64, bottom to top), p = (acc ? p : 0) + omega * z.
 // A warp owns 32 consecutive columns.  Their right-hand sides (contiguous in the column layout)
 // pass through a 32 x kLineChunk shared-memory tile, loaded and stored with coalesced accesses;
@@ -688,6 +699,7 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
             }
         }
         __syncwarp();
+        discard_line_chunk(dbuf, col0, k0, nk, L, lane);
         for (int i = lane; i < ncols * nk; i += 32) {
             const int cc = i / nk, kk = i - cc * nk;
             const int64_t g = (int64_t)(col0 + cc) * L + k0 + kk;
@@ -771,6 +783,7 @@ k_wide_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
             }
         }
         __syncwarp();
+        discard_line_chunk(dbuf, col0, k0, nk, L, lane);
         for (int i = lane; i < ncols * nk; i += 32) {
             const int cc = i / nk, kk = i - cc * nk;
             const int64_t g = (int64_t)(col0 + cc) * L + k0 + kk;
