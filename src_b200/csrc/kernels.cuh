@@ -612,28 +612,22 @@ __global__ void k_div(ColMesh M, const double *__restrict__ ua, const double *__
 }
 
 // ------------------------------------------------------------------------------ line solve
-// The forward-sweep values d are scratch: each is read once, by the lane that wrote it, in the
-// backward sweep.  After a chunk's backward sweep the warp drops the chunk's lines of d from L2
-// (discard.global.L2: no write-back), so the scratch stays off DRAM when its lines are still in
-// L2.  Level k of the warp's 32 columns is one 256-byte segment (line_index), two 128-byte lines.
-__device__ __forceinline__ void discard_line_chunk(double *dbuf, int col0, int k0, int nk, int L, int lane) {
-    for (int i = lane; i < 2 * nk; i += 32) {
-        const double *a = dbuf + line_index(col0, k0 + (i >> 1), L) + 16 * (i & 1);
-        asm volatile("discard.global.L2 [%0], 128;" ::"l"(a) : "memory");
-    }
-}
-
 // z = M^{-1} rhs per column (Thomas, FP64, bottom to top), p = (acc ? p : 0) + omega * z.
 // A warp owns 32 consecutive columns.  Their right-hand sides (contiguous in the column layout)
 // pass through a 32 x kLineChunk shared-memory tile, loaded and stored with coalesced accesses;
 // the factorisation (a, 1/m, c') and the forward-sweep values d are stored interleaved
 // (line_index), so lane l reads and writes level k of column col0+l inside one 256-byte segment.
 // With 4 KiB of shared memory per warp the kernel keeps enough warps resident to stream.
+// Measured alternatives at 512x512x81 (FP64, CUDA events), all slower: the largest shared-memory
+// carve-out requested for the kernel (295 against 238 us), chunks of 14 levels with 2-4 levels of
+// coefficients ahead and 7 blocks per SM so that the grid fits one wave (320-367 us), dropping the
+// scratch d from L2 after the backward sweep (no gain).
 constexpr int kLineWarps = 8;
 constexpr int kLineChunk = 16;
 constexpr int kLinePre = 8;
+#define LINE_BOUNDS __launch_bounds__(32 * kLineWarps)
 template <class TO>
-__global__ void __launch_bounds__(32 * kLineWarps)
+__global__ void LINE_BOUNDS
 k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__restrict__ la,
              const double *__restrict__ linv, const double *__restrict__ lcp, double omega, int acc,
              double *__restrict__ dbuf, TO *__restrict__ p) {
@@ -699,7 +693,6 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
             }
         }
         __syncwarp();
-        discard_line_chunk(dbuf, col0, k0, nk, L, lane);
         for (int i = lane; i < ncols * nk; i += 32) {
             const int cc = i / nk, kk = i - cc * nk;
             const int64_t g = (int64_t)(col0 + cc) * L + k0 + kk;
@@ -714,7 +707,7 @@ k_line_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
 // same sweeps as k_line_solve with the recurrences reaching two levels back / ahead, both parity
 // chains advanced together level by level.  Staging, prefetch and indexing are k_line_solve's.
 template <class TO>
-__global__ void __launch_bounds__(32 * kLineWarps)
+__global__ void LINE_BOUNDS
 k_wide_solve(int NC, int L, const double *__restrict__ rhs, const double *__restrict__ la,
              const double *__restrict__ linv, const double *__restrict__ lcp, double omega, int acc,
              double *__restrict__ dbuf, TO *__restrict__ p) {
@@ -783,7 +776,6 @@ k_wide_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
             }
         }
         __syncwarp();
-        discard_line_chunk(dbuf, col0, k0, nk, L, lane);
         for (int i = lane; i < ncols * nk; i += 32) {
             const int cc = i / nk, kk = i - cc * nk;
             const int64_t g = (int64_t)(col0 + cc) * L + k0 + kk;

@@ -97,7 +97,6 @@ int mpg_build_column_mesh(const mpg_mesh_ref *m, HostColumnMesh *out) {
     for (int c = 0; c < NC; ++c)
         if (csize[c] != L)
             return mpg_fail(MPG_ERR_MESH, "not a prism-column mesh: columns have different numbers of levels");
-    if (L < 2) return mpg_fail(MPG_ERR_MESH, "not a prism-column mesh: fewer than 2 levels");
     if ((int64_t)NC * L != npoin) return mpg_fail(MPG_ERR_MESH, "column count mismatch");
 
     // ---- 2. levels: sort each column by z
