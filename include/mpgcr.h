@@ -187,7 +187,9 @@ typedef struct mpg_solver *mpg_handle;
 /* Uploads the mesh once, detects the prism-column structure (columns of equal (x,y), the same
  * number of levels everywhere, horizontal edges between equal levels), packs it column-major
  * (level fastest) and allocates every field on `device`.  Replaces the mesh part of `input`
- * (ref.f:2343-2641) and the static COMMON storage. */
+ * (ref.f:2343-2641) and the static COMMON storage.  With the environment variable
+ * MPG_LAPLC_FUSED=1 set at this call, laplc runs as one persistent launch instead of two
+ * (bit-identical results; slower on the 21.2M-node workload measured; not with copy lists). */
 int mpg_create(const mpg_params *prm, const mpg_mesh_ref *mesh, int device, mpg_handle *out);
 int mpg_destroy(mpg_handle h);
 /* Host-only check of a mesh: runs the prism-column detection of mpg_create without touching a
