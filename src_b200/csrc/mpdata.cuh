@@ -135,8 +135,12 @@ __global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, const do
                                  T *__restrict__ gx, T *__restrict__ gy, T *__restrict__ gz,
                                  double *__restrict__ mx, double *__restrict__ mn) {
     NODE_BEGIN
+    // in mixed precision the bounds come from the FP64 first-pass field; in FP64 that field is
+    // psi1 itself (decided at compile time: a pointer test per face cost the FP64 kernel a block
+    // per SM in registers)
+    constexpr bool BD = std::is_same<T, float>::value;
     const T pn = psi1[n];
-    const double bn = psi1d ? psi1d[n] : (double)pn;       // the bounds come from the FP64 field
+    const double bn = BD ? psi1d[n] : (double)pn;
     T ax = 0., ay = 0., az = 0.;
     double hi = -1.e15, lo = 1.e15;
     for_faces(M, c, k, n,
@@ -152,7 +156,7 @@ __global__ void k_mp_grad_bounds(ColMesh M, const T *__restrict__ psi1, const do
             const T tx = v.a * u, ty = v.b * u, tz = v.c * u;
             if (f.sub) { ax = ax - tx; ay = ay - ty; az = az - tz; }
             else       { ax = ax + tx; ay = ay + ty; az = az + tz; }
-            const double bj = psi1d ? psi1d[f.j] : (double)pj;
+            const double bj = BD ? psi1d[f.j] : (double)pj;
             hi = hi > bn ? hi : bn;
             hi = hi > bj ? hi : bj;
             lo = lo < bn ? lo : bn;
