@@ -27,6 +27,11 @@ constexpr int kThreads = 256;
 constexpr int kRedBlocks = MPG_RED_BLOCKS;   // 4 x 148 SMs
 constexpr int kRedThreads = 256;
 constexpr int kMaxQ = 24;                // quantities per reduction
+// nodes whose operands a reduction thread loads before finishing any: as many as fit the
+// 64 registers that keep 4 blocks of 256 threads per SM (the grid is 4 blocks per SM)
+template <class Loaded> struct RedDepth {
+    static constexpr int value = sizeof(Loaded) <= 32 ? 4 : sizeof(Loaded) <= 48 ? 3 : 2;
+};
 
 __device__ __forceinline__ double amax(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double amin(double a, double b) { return a < b ? a : b; }
@@ -790,8 +795,8 @@ k_wide_solve(int NC, int L, const double *__restrict__ rhs, const double *__rest
 enum RedKind { RSUM = 0, RMAX = 1 };
 
 // A reduction functor may split its work per node into load(n) -> Loaded and finish(n, Loaded,
-// vals) (it then defines a nested type Loaded).  k_reduce then loads two nodes of its
-// grid-stride sequence before finishing either, which the compiler cannot arrange by itself
+// vals) (it then defines a nested type Loaded).  k_reduce then loads RedDepth nodes of its
+// grid-stride sequence before finishing any, which the compiler cannot arrange by itself
 // when finish stores to arrays that might alias the next node's operands.  The order in which a
 // thread accumulates its nodes is the same, so the results are bit-identical.
 template <class P, class = void> struct SplitProd { static constexpr bool value = false; };
@@ -815,13 +820,17 @@ k_reduce(int N, unsigned kinds, Prod prod, Fin fin, double *__restrict__ part,
     };
     int n = blockIdx.x * blockDim.x + threadIdx.x;
     if constexpr (SplitProd<Prod>::value) {
-        for (; n + stride < N; n += 2 * stride) {
-            const typename Prod::Loaded a = prod.load(n), b = prod.load(n + stride);
-            double v[NQ];
-            prod.finish(n, a, v);
-            add(v);
-            prod.finish(n + stride, b, v);
-            add(v);
+        constexpr int D = RedDepth<typename Prod::Loaded>::value;
+        for (; n + (D - 1) * stride < N; n += D * stride) {
+            typename Prod::Loaded a[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) a[d] = prod.load(n + d * stride);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                double v[NQ];
+                prod.finish(n + d * stride, a[d], v);
+                add(v);
+            }
         }
         for (; n < N; n += stride) {
             double v[NQ];
