@@ -185,7 +185,7 @@ typedef struct mpg_solver *mpg_handle;
 
 /* ---------------------------------------------------------------- lifecycle */
 /* Uploads the mesh once, detects the prism-column structure (columns of equal (x,y), the same
- * number of levels everywhere, horizontal edges between equal levels), packs it column-major
+ * number of levels everywhere, 1 to 128 of them, horizontal edges between equal levels), packs it column-major
  * (level fastest) and allocates every field on `device`.  Replaces the mesh part of `input`
  * (ref.f:2343-2641) and the static COMMON storage.  With the environment variable
  * MPG_LAPLC_FUSED=1 set at this call, laplc runs as one persistent launch instead of two
