@@ -438,7 +438,7 @@ k_lap_div2(ColMesh M, int PL, const Flux<T> F, const T *__restrict__ vol, const 
 // state[3] and the item goes ahead (the host reports the error).  Each node's arithmetic is
 // k_lap_grad's and k_lap_div2's, so the result is bit-identical to the two-launch form.
 // Measured at 512x512x81 (FP64): 2.00 ms per laplc against 1.71 ms for the two launches, although
-// DRAM traffic falls by 43% (L2 hit rate 65%).  The gathers are latency-bound, and the kernel's
+// DRAM traffic falls by about 40% (L2 hit rate 65%).  The gathers are latency-bound, and the kernel's
 // 64 registers (the divergence's) hold the gradient items to 32 warps per SM where k_lap_grad
 // runs 48.  The library therefore launches the two halves unless MPG_LAPLC_FUSED=1 at creation.
 //
