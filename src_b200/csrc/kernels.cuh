@@ -306,8 +306,17 @@ __device__ __forceinline__ void lap_grad_node(const ColMesh &M, int n, const T *
     F.store(n, dx * r, dy * r, dz * r);
 }
 
+// laplc's first half keeps 6 blocks per SM in FP64 (40 registers); the FP32 instantiation fits
+// 32 registers without spilling, so it takes 8 (every warp slot of the SM)
+#ifndef MPG_GATHER_MINB_F32
+#define MPG_GATHER_MINB_F32 8
+#endif
+template <class T> struct LapGradMinB { static constexpr int value = MPG_GATHER_MINB; };
+template <> struct LapGradMinB<float> { static constexpr int value = MPG_GATHER_MINB_F32; };
+
 template <class T>
-__global__ void GATHER_BOUNDS k_lap_grad(ColMesh M, const T *__restrict__ p, const T *__restrict__ vol,
+__global__ void __launch_bounds__(kThreads, LapGradMinB<T>::value)
+k_lap_grad(ColMesh M, const T *__restrict__ p, const T *__restrict__ vol,
                                          const T *__restrict__ rh0, const T *__restrict__ coefw,
                                          const double *__restrict__ ue, T dt, int impfl, Flux<T> F) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
