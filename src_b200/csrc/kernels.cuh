@@ -307,7 +307,8 @@ __device__ __forceinline__ void lap_grad_node(const ColMesh &M, int n, const T *
 }
 
 // laplc's first half keeps 6 blocks per SM in FP64 (40 registers); the FP32 instantiation fits
-// 32 registers without spilling, so it takes 8 (every warp slot of the SM)
+// 32 registers without spilling, so it takes 8 (every warp slot of the SM): 563 against 676 us
+// on the 512x512x81 workload
 #ifndef MPG_GATHER_MINB_F32
 #define MPG_GATHER_MINB_F32 8
 #endif
@@ -425,8 +426,16 @@ __device__ __forceinline__ void lap_div_pair(const ColMesh &M, int PL, int t, co
     }
 }
 
+// FP32 (mixed precision) level pairs at 6 blocks per SM, 40 registers: measured 494 us against
+// 520 at 5 blocks (48 registers) and 590 at 4 (64) on the 512x512x81 workload
+#ifndef MPG_DIV2_MINB_F32
+#define MPG_DIV2_MINB_F32 6
+#endif
+template <class T> struct LapDiv2MinB { static constexpr int value = kLapPairMinBlocks; };
+template <> struct LapDiv2MinB<float> { static constexpr int value = MPG_DIV2_MINB_F32; };
+
 template <class T>
-__global__ void __launch_bounds__(kThreads, kLapPairMinBlocks)
+__global__ void __launch_bounds__(kThreads, LapDiv2MinB<T>::value)
 k_lap_div2(ColMesh M, int PL, const Flux<T> F, const T *__restrict__ vol, const T *__restrict__ rh0,
            T *__restrict__ alap) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
