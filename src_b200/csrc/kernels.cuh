@@ -309,11 +309,11 @@ __device__ __forceinline__ void lap_grad_node(const ColMesh &M, int n, const T *
 // laplc's first half keeps 6 blocks per SM in FP64 (40 registers); the FP32 instantiation fits
 // 32 registers without spilling, so it takes 8 (every warp slot of the SM): 563 against 676 us
 // on the 512x512x81 workload
-#ifndef MPG_GATHER_MINB_F32
-#define MPG_GATHER_MINB_F32 8
+#ifndef MPG_LAPGRAD_MINB_F32
+#define MPG_LAPGRAD_MINB_F32 8
 #endif
 template <class T> struct LapGradMinB { static constexpr int value = MPG_GATHER_MINB; };
-template <> struct LapGradMinB<float> { static constexpr int value = MPG_GATHER_MINB_F32; };
+template <> struct LapGradMinB<float> { static constexpr int value = MPG_LAPGRAD_MINB_F32; };
 
 template <class T>
 __global__ void __launch_bounds__(kThreads, LapGradMinB<T>::value)
